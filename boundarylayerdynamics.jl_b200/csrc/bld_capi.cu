@@ -1,0 +1,1267 @@
+// Host side of the engine: the C ABI declared in include/bld.h, set-up of the
+// discretisation tables (the reference's init_process methods), device buffers,
+// kernel launch schedules per RK stage and CUDA-graph replay of whole steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "bld.h"
+#include "bld_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? BLD_ERR_OUT_OF_MEMORY : BLD_ERR_CUDA, \
+                        "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__);  \
+    } while (0)
+
+#define BLD_TRY(expr)          \
+    do {                       \
+        int s_ = (expr);       \
+        if (s_ != BLD_OK) return s_; \
+    } while (0)
+
+// ---------------------------------------------------------------- FFT sizes and plans
+bool smooth23(int n) {
+    if (n < 2) return false;
+    while (n % 2 == 0) n /= 2;
+    while (n % 3 == 0) n /= 3;
+    return n == 1;
+}
+
+int next_even_smooth(int n) {
+    int m = std::max(n, 2);
+    while (!(m % 2 == 0 && smooth23(m))) ++m;
+    return m;
+}
+
+FftPlan make_plan(int n) {
+    FftPlan p{};
+    p.n = n;
+    int m = n, s = 0;
+    while (m % 4 == 0) {
+        p.radix[s++] = 4;
+        m /= 4;
+    }
+    while (m % 2 == 0) {
+        p.radix[s++] = 2;
+        m /= 2;
+    }
+    while (m % 3 == 0) {
+        p.radix[s++] = 3;
+        m /= 3;
+    }
+    p.nst = s;
+    return p;
+}
+
+// quadratic-dealiasing size of the reference (src/physical_space.jl:49-56)
+int pdsize_quadratic(int kmax) {
+    const double l = std::log2(1.0 + kmax);
+    if (l == std::floor(l)) return 3 * kmax + 3;
+    return 3 * kmax + ((kmax % 2 == 1) ? 1 : 2);
+}
+
+struct DevTw {
+    void* d64 = nullptr;
+    void* d32 = nullptr;
+};
+
+struct Space {
+    bool on = false;
+    int P1 = 0, P2 = 0, ref_P1 = 0, ref_P2 = 0;
+    FftPlan plan1{}, plan2{};
+    int ntin = 0, ntout = 0;
+    void* min = nullptr;
+    void* mout = nullptr;
+    long long min_ms = 0, mout_ms = 0;  // elements per member
+    int YT = 1, PPT = 1, zchunk = 1, nchunks = 1;
+    int NLy = 8, MAXO = 8;
+};
+
+}  // namespace
+
+struct bld_handle {
+    bld_config cfg{};
+    int device = 0;
+    int B = 1;
+    Geo g{};
+    bool fp32 = false;
+    cudaStream_t stream = nullptr;
+    // state and integrator buffers [member][vel1|vel2|vel3]
+    double2* u = nullptr;
+    double2* t = nullptr;
+    double2* du = nullptr;
+    double2* dp = nullptr;
+    double2* io = nullptr;     // staging for host-buffer calls
+    double2* io2 = nullptr;
+    double2* pscr = nullptr;
+    double* gamma = nullptr;
+    // tables
+    double *d1 = nullptr, *d2 = nullptr, *DD1 = nullptr, *DD2 = nullptr;
+    double *alpha_c = nullptr, *alpha_i = nullptr, *alpha_ext = nullptr, *mean_w = nullptr;
+    double *lc2 = nullptr, *li2 = nullptr, *wall = nullptr, *src = nullptr, *mean_val = nullptr;
+    int* flag = nullptr;
+    int* flag_host = nullptr;
+    std::map<int, DevTw> tw;
+    Space adv, sgs;
+    // physical-domain transforms at the default size
+    int Pd1 = 0, Pd2 = 0;
+    void* pd_buf = nullptr;     // double [nz][Pd2][Pd1]
+    void* pd_mixed = nullptr;   // double2 [nz][Pd2][K1]
+    // host-side copies used by launches
+    double w_lo = 0, w_hi = 0;
+    int dyn_lo = 0, dyn_hi = 0;
+    Linear lin{};
+    bool slope_valid = false;
+    bool ab2_started = false;
+    double ab2_dt = 0;
+    std::map<std::pair<int, double>, cudaGraphExec_t> graphs;
+    size_t bytes = 0;
+};
+
+namespace {
+
+int dalloc(bld_handle* h, void** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return fail(BLD_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    h->bytes += bytes;
+    return BLD_OK;
+}
+
+template <typename T>
+int upload(bld_handle* h, T** dst, const std::vector<T>& v) {
+    BLD_TRY(dalloc(h, (void**)dst, v.size() * sizeof(T)));
+    if (!v.empty()) CUDA_TRY(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return BLD_OK;
+}
+
+int twiddles(bld_handle* h, int n) {
+    if (h->tw.count(n)) return BLD_OK;
+    std::vector<double2> w64(n);
+    std::vector<float2> w32(n);
+    for (int m = 0; m < n; ++m) {
+        const long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
+        const long double c = cosl(ang), s = sinl(ang);
+        w64[m] = make_double2((double)c, (double)s);
+        w32[m] = make_float2((float)c, (float)s);
+    }
+    DevTw t;
+    BLD_TRY(dalloc(h, &t.d64, n * sizeof(double2)));
+    BLD_TRY(dalloc(h, &t.d32, n * sizeof(float2)));
+    CUDA_TRY(cudaMemcpy(t.d64, w64.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(t.d32, w32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    h->tw[n] = t;
+    return BLD_OK;
+}
+
+const void* twp(const bld_handle* h, int n, bool fp32) {
+    const DevTw& t = h->tw.at(n);
+    return fp32 ? t.d32 : t.d64;
+}
+
+size_t csize(bool fp32) { return fp32 ? sizeof(float2) : sizeof(double2); }
+
+// y-pass lines per block: shared memory <= ~100 KB and outputs per thread <= 16
+void pick_y(const Geo& g, int P2, bool fp32, int& NL, int& MAXO) {
+    const size_t cs = csize(fp32);
+    NL = fp32 ? 16 : 8;
+    while (NL > 2 && (size_t)(P2 + 2 * P2 * NL) * cs > 100 * 1024) NL /= 2;
+    while (g.K2 * NL > 256 * 16 && NL > 2) NL /= 2;
+    MAXO = (g.K2 * NL <= 256 * 8) ? 8 : 16;
+}
+
+// choose tiles for a physical-domain space
+void tile_space(const bld_handle* h, Space& s) {
+    const size_t cs = csize(h->fp32);
+    // y rows per block: largest of 4, 2, 1 dividing P2 with YT*P1 <= 512
+    s.YT = 1;
+    for (int yt : {4, 2}) {
+        if (s.P2 % yt == 0 && yt * s.P1 <= 512) {
+            s.YT = yt;
+            break;
+        }
+    }
+    s.PPT = (s.YT * s.P1 + 511) / 512;
+    while ((s.YT * s.P1) % s.PPT) ++s.PPT;
+    const int n3 = h->g.n3;
+    const long long blocks_per_chunk = (long long)(s.P2 / s.YT) * h->B;
+    int want = (int)std::max<long long>(1, (600 + blocks_per_chunk - 1) / blocks_per_chunk);
+    want = std::min(want, std::max(1, n3 / 4));
+    s.zchunk = (n3 + want - 1) / want;
+    s.nchunks = (n3 + s.zchunk - 1) / s.zchunk;
+    pick_y(h->g, s.P2, h->fp32, s.NLy, s.MAXO);
+    (void)cs;
+}
+
+size_t smem_y(int P2, int NL, bool fp32) { return (size_t)(P2 + 2 * P2 * NL) * csize(fp32); }
+size_t smem_adv(const Space& s, bool fp32) {
+    const int nin = 3 * s.YT, nout = s.YT + (s.YT + 1) / 2;
+    return (size_t)(s.P1 + 3 * std::max(nin, nout) * s.P1) * csize(fp32);
+}
+size_t smem_sgs(const Space& s, bool fp32) { return (size_t)(s.P1 + 3 * 5 * s.YT * s.P1) * csize(fp32); }
+
+// ------------------------------------------------------------------ kernel dispatch
+template <typename R>
+int launch_inv_y(bld_handle* h, const Space& s, const InvYArgs& a, int nm) {
+    dim3 grid((h->g.K1 + s.NLy - 1) / s.NLy, h->g.n3, a.nterms * nm);
+    const size_t sm = smem_y(s.P2, s.NLy, sizeof(R) == 4);
+    switch (s.NLy) {
+        case 16: k_inv_y<R, 16><<<grid, 256, sm, h->stream>>>(a); break;
+        case 8: k_inv_y<R, 8><<<grid, 256, sm, h->stream>>>(a); break;
+        case 4: k_inv_y<R, 4><<<grid, 256, sm, h->stream>>>(a); break;
+        default: k_inv_y<R, 2><<<grid, 256, sm, h->stream>>>(a); break;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+template <typename R>
+int launch_fwd_y(bld_handle* h, const Space& s, const FwdYArgs& a, int nm) {
+    dim3 grid((h->g.K1 + s.NLy - 1) / s.NLy, h->g.n3, a.fields * nm);
+    const size_t sm = smem_y(s.P2, s.NLy, sizeof(R) == 4);
+#define BLD_FWD(NL, MO) k_fwd_y<R, NL, MO><<<grid, 256, sm, h->stream>>>(a)
+    if (s.MAXO == 8) {
+        switch (s.NLy) {
+            case 16: BLD_FWD(16, 8); break;
+            case 8: BLD_FWD(8, 8); break;
+            case 4: BLD_FWD(4, 8); break;
+            default: BLD_FWD(2, 8); break;
+        }
+    } else {
+        switch (s.NLy) {
+            case 16: BLD_FWD(16, 16); break;
+            case 8: BLD_FWD(8, 16); break;
+            case 4: BLD_FWD(4, 16); break;
+            default: BLD_FWD(2, 16); break;
+        }
+    }
+#undef BLD_FWD
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+template <typename R>
+int launch_adv_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    dim3 grid(s.P2 / s.YT, s.nchunks, nm);
+    const int thr = s.YT * s.P1 / s.PPT;
+    const size_t sm = smem_adv(s, sizeof(R) == 4);
+    switch (s.PPT) {
+        case 1: k_adv_x<R, 1><<<grid, thr, sm, h->stream>>>(a); break;
+        case 2: k_adv_x<R, 2><<<grid, thr, sm, h->stream>>>(a); break;
+        case 3: k_adv_x<R, 3><<<grid, thr, sm, h->stream>>>(a); break;
+        default: k_adv_x<R, 4><<<grid, thr, sm, h->stream>>>(a); break;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+template <typename R>
+int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    dim3 grid(s.P2 / s.YT, s.nchunks, nm);
+    const int thr = s.YT * s.P1 / s.PPT;
+    const size_t sm = smem_sgs(s, sizeof(R) == 4);
+    switch (s.PPT) {
+        case 1: k_sgs_x<R, 1><<<grid, thr, sm, h->stream>>>(a); break;
+        case 2: k_sgs_x<R, 2><<<grid, thr, sm, h->stream>>>(a); break;
+        case 3: k_sgs_x<R, 3><<<grid, thr, sm, h->stream>>>(a); break;
+        default: k_sgs_x<R, 4><<<grid, thr, sm, h->stream>>>(a); break;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+template <typename R>
+int set_smem_limits_R() {
+    const int lim = 200 * 1024;
+#define BLD_SET(K) CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, lim))
+    BLD_SET((k_inv_y<R, 16>));
+    BLD_SET((k_inv_y<R, 8>));
+    BLD_SET((k_inv_y<R, 4>));
+    BLD_SET((k_inv_y<R, 2>));
+    BLD_SET((k_fwd_y<R, 16, 8>));
+    BLD_SET((k_fwd_y<R, 8, 8>));
+    BLD_SET((k_fwd_y<R, 4, 8>));
+    BLD_SET((k_fwd_y<R, 2, 8>));
+    BLD_SET((k_fwd_y<R, 16, 16>));
+    BLD_SET((k_fwd_y<R, 8, 16>));
+    BLD_SET((k_fwd_y<R, 4, 16>));
+    BLD_SET((k_fwd_y<R, 2, 16>));
+    BLD_SET((k_adv_x<R, 1>));
+    BLD_SET((k_adv_x<R, 2>));
+    BLD_SET((k_adv_x<R, 3>));
+    BLD_SET((k_adv_x<R, 4>));
+    BLD_SET((k_sgs_x<R, 1>));
+    BLD_SET((k_sgs_x<R, 2>));
+    BLD_SET((k_sgs_x<R, 3>));
+    BLD_SET((k_sgs_x<R, 4>));
+#undef BLD_SET
+    return BLD_OK;
+}
+
+int set_smem_limits() {
+    static int done = 0;
+    if (done) return BLD_OK;
+    BLD_TRY(set_smem_limits_R<double>());
+    BLD_TRY(set_smem_limits_R<float>());
+    CUDA_TRY(cudaFuncSetAttribute(k_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    done = 1;
+    return BLD_OK;
+}
+
+// ------------------------------------------------------------------ schedules
+template <typename R>
+int enqueue_inv_y_R(bld_handle* h, int sp, const double2* state, int m0, int nm) {
+    Space& s = sp == 0 ? h->adv : h->sgs;
+    InvYArgs ia{};
+    ia.g = h->g;
+    ia.P2 = s.P2;
+    ia.m0 = m0;
+    ia.state = state;
+    ia.mixed = s.min;
+    ia.mixed_mstride = s.min_ms;
+    ia.d1 = h->d1;
+    ia.d2 = h->d2;
+    ia.alpha_i = h->alpha_i;
+    ia.plan = s.plan2;
+    ia.tw = twp(h, s.P2, sizeof(R) == 4);
+    if (sp == 0) {  // u, v, w, vort1, vort2, vort3 (src/processes/momentum_advection.jl:40-41)
+        const int op[6] = {T_DIRECT, T_DIRECT, T_DIRECT, T_VORT1, T_VORT2, T_VORT3};
+        const int fl[6] = {0, 1, 2, 0, 0, 0};
+        const int isI[6] = {0, 0, 1, 1, 1, 0};
+        ia.nterms = 6;
+        for (int i = 0; i < 6; ++i) {
+            ia.op[i] = op[i];
+            ia.fld[i] = fl[i];
+            ia.isI[i] = isI[i];
+        }
+    } else {  // u, v, w, u_1, u_2, v_1, v_2, w_1, w_2 (src/processes/static_smagorinsky.jl:39-42)
+        const int op[9] = {T_DIRECT, T_DIRECT, T_DIRECT, T_D1, T_D2, T_D1, T_D2, T_D1, T_D2};
+        const int fl[9] = {0, 1, 2, 0, 0, 1, 1, 2, 2};
+        const int isI[9] = {0, 0, 1, 0, 0, 0, 0, 1, 1};
+        ia.nterms = 9;
+        for (int i = 0; i < 9; ++i) {
+            ia.op[i] = op[i];
+            ia.fld[i] = fl[i];
+            ia.isI[i] = isI[i];
+        }
+    }
+    return launch_inv_y<R>(h, s, ia, nm);
+}
+
+template <typename R>
+int enqueue_x_R(bld_handle* h, int sp, int m0, int nm) {
+    Space& s = sp == 0 ? h->adv : h->sgs;
+    XArgs xa{};
+    xa.g = h->g;
+    xa.P1 = s.P1;
+    xa.P2 = s.P2;
+    xa.YT = s.YT;
+    xa.zchunk = s.zchunk;
+    xa.m0 = m0;
+    xa.min = s.min;
+    xa.mout = s.mout;
+    xa.min_mstride = s.min_ms;
+    xa.mout_mstride = s.mout_ms;
+    xa.plan = s.plan1;
+    xa.tw = twp(h, s.P1, sizeof(R) == 4);
+    xa.alpha_c = h->alpha_c;
+    xa.alpha_i = h->alpha_i;
+    xa.lc = h->lc2;
+    xa.li = h->li2;
+    xa.wall = h->wall;
+    xa.dyn_lo = h->dyn_lo;
+    xa.dyn_hi = h->dyn_hi;
+    xa.w_lo = h->w_lo;
+    xa.w_hi = h->w_hi;
+    return sp == 0 ? launch_adv_x<R>(h, s, xa, nm) : launch_sgs_x<R>(h, s, xa, nm);
+}
+
+template <typename R>
+int enqueue_fwd_y_R(bld_handle* h, int sp, bool first, bool last, const double2* state, double2* du, int m0, int nm) {
+    Space& s = sp == 0 ? h->adv : h->sgs;
+    FwdYArgs fa{};
+    fa.g = h->g;
+    fa.P1 = s.P1;
+    fa.P2 = s.P2;
+    fa.mout = s.mout;
+    fa.mout_mstride = s.mout_ms;
+    if (sp == 0) {  // adv1 -> vel1, adv2 -> vel2, adv3 -> vel3
+        for (int f = 0; f < 3; ++f) {
+            fa.ncontrib[f] = 1;
+            fa.c[f][0] = FwdContrib{f, 0};
+        }
+    } else {  // rate order of add_rates! (src/physical_space.jl:191-204)
+        fa.ncontrib[0] = 3;
+        fa.c[0][0] = FwdContrib{3, 0};
+        fa.c[0][1] = FwdContrib{0, 1};
+        fa.c[0][2] = FwdContrib{1, 2};
+        fa.ncontrib[1] = 3;
+        fa.c[1][0] = FwdContrib{4, 0};
+        fa.c[1][1] = FwdContrib{1, 1};
+        fa.c[1][2] = FwdContrib{2, 2};
+        fa.ncontrib[2] = 3;
+        fa.c[2][0] = FwdContrib{5, 0};
+        fa.c[2][1] = FwdContrib{6, 1};
+        fa.c[2][2] = FwdContrib{7, 2};
+    }
+    fa.mode = first ? 1 : 0;
+    fa.check = last ? 1 : 0;
+    fa.du = du;
+    fa.du_mstride = h->g.mstride;
+    fa.state = state;
+    fa.lin = h->lin;
+    fa.d1 = h->d1;
+    fa.d2 = h->d2;
+    fa.inv_n = 1.0 / ((double)s.P1 * (double)s.P2);
+    fa.flag = h->flag;
+    fa.fields = 3;
+    fa.field0 = 0;
+    fa.m0 = m0;
+    fa.plan = s.plan2;
+    fa.tw = twp(h, s.P2, sizeof(R) == 4);
+    return launch_fwd_y<R>(h, s, fa, nm);
+}
+
+int enqueue_linear(bld_handle* h, const double2* state, double2* du, int m0, int nm) {
+    FwdYArgs fa{};
+    fa.g = h->g;
+    fa.mode = 1;
+    fa.check = 1;
+    fa.du = du;
+    fa.du_mstride = h->g.mstride;
+    fa.state = state;
+    fa.lin = h->lin;
+    fa.flag = h->flag;
+    fa.m0 = m0;
+    dim3 grid((h->g.F + 255) / 256, h->g.n3, 3 * nm);
+    k_linear<<<grid, 256, 0, h->stream>>>(fa);
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+int enqueue_inv_y(bld_handle* h, int sp, const double2* st, int m0, int nm) {
+    return h->fp32 ? enqueue_inv_y_R<float>(h, sp, st, m0, nm) : enqueue_inv_y_R<double>(h, sp, st, m0, nm);
+}
+int enqueue_x(bld_handle* h, int sp, int m0, int nm) {
+    return h->fp32 ? enqueue_x_R<float>(h, sp, m0, nm) : enqueue_x_R<double>(h, sp, m0, nm);
+}
+int enqueue_fwd_y(bld_handle* h, int sp, bool first, bool last, const double2* st, double2* du, int m0, int nm) {
+    return h->fp32 ? enqueue_fwd_y_R<float>(h, sp, first, last, st, du, m0, nm)
+                   : enqueue_fwd_y_R<double>(h, sp, first, last, st, du, m0, nm);
+}
+
+// compute_rates! (src/Processes.jl:39-62): nonlinear processes in the reference's
+// process order (advection, then SGS), each rate written once with the linear terms
+int enqueue_rates_impl(bld_handle* h, const double2* state, double2* du, int m0, int nm) {
+    for (int sp = 0; sp < 2; ++sp) {
+        if (!(sp == 0 ? h->adv.on : h->sgs.on)) continue;
+        BLD_TRY(enqueue_inv_y(h, sp, state, m0, nm));
+        BLD_TRY(enqueue_x(h, sp, m0, nm));
+    }
+    bool first = true;
+    for (int sp = 0; sp < 2; ++sp) {
+        if (!(sp == 0 ? h->adv.on : h->sgs.on)) continue;
+        const bool last = (sp == 1) || !h->sgs.on;
+        BLD_TRY(enqueue_fwd_y(h, sp, first, last, state, du, m0, nm));
+        first = false;
+    }
+    if (first) BLD_TRY(enqueue_linear(h, state, du, m0, nm));
+    return BLD_OK;
+}
+
+int enqueue_rates(bld_handle* h, const double2* state, double2* du, int m0, int nm) {
+    return enqueue_rates_impl(h, state, du, m0, nm);
+}
+
+int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const double2* t, const double2* du,
+                    const double2* dp, double2* out, int m0, int nm) {
+    ProjArgs a{};
+    a.g = h->g;
+    a.m0 = m0;
+    a.u = u;
+    a.t = t;
+    a.du = du;
+    a.dp = dp;
+    a.out = out;
+    a.kind = kind;
+    a.dt = dt;
+    a.pressure = h->cfg.pressure;
+    a.pscr = h->pscr;
+    a.gamma = h->gamma;
+    a.alpha_c = h->alpha_c;
+    a.alpha_i = h->alpha_i;
+    a.d1 = h->d1;
+    a.d2 = h->d2;
+    a.w_lo = h->w_lo;
+    a.w_hi = h->w_hi;
+    for (int f = 0; f < 3; ++f) a.mean_on[f] = h->cfg.mean[f];
+    a.mean_w = h->mean_w;
+    a.mean_val = h->mean_val;
+    const bool any_mean = h->cfg.mean[0] || h->cfg.mean[1];
+    if (!a.pressure && !any_mean && kind == S_NONE && out == u) return BLD_OK;
+    dim3 grid((h->g.F + 127) / 128, nm);
+    k_project<<<grid, 128, 0, h->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+// one time step of `method` (perform_step! + the trailing rate!, src/ODEMethods.jl:217-234)
+int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first) {
+    const int B = h->B;
+    switch (method) {
+        case BLD_EULER:
+            BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->u, 0, B));
+            BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
+            break;
+        case BLD_SSPRK22:
+            BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->t, 0, B));
+            BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
+            BLD_TRY(enqueue_project(h, S_RK22_2, dt, h->u, h->t, h->du, nullptr, h->u, 0, B));
+            BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
+            break;
+        case BLD_SSPRK33:
+            BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->t, 0, B));
+            BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
+            BLD_TRY(enqueue_project(h, S_RK33_2, dt, h->u, h->t, h->du, nullptr, h->t, 0, B));
+            BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
+            BLD_TRY(enqueue_project(h, S_RK33_3, dt, h->u, h->t, h->du, nullptr, h->u, 0, B));
+            BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
+            break;
+        case BLD_AB2: {
+            const size_t bytes = (size_t)B * h->g.mstride * sizeof(double2);
+            if (ab2_first) {
+                BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->u, 0, B));
+                CUDA_TRY(cudaMemcpyAsync(h->dp, h->du, bytes, cudaMemcpyDeviceToDevice, h->stream));
+                BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
+                BLD_TRY(enqueue_project(h, S_AB2_1, dt, h->u, nullptr, h->du, h->dp, h->u, 0, B));
+            } else {
+                BLD_TRY(enqueue_project(h, S_AB2, dt, h->u, nullptr, h->du, h->dp, h->u, 0, B));
+                CUDA_TRY(cudaMemcpyAsync(h->dp, h->du, bytes, cudaMemcpyDeviceToDevice, h->stream));
+            }
+            BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
+            break;
+        }
+        default:
+            return fail(BLD_ERR_ARGUMENT, "unknown method %d", method);
+    }
+    return BLD_OK;
+}
+
+int check_flag(bld_handle* h) {
+    CUDA_TRY(cudaMemcpyAsync(h->flag_host, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (*h->flag_host) {
+        *h->flag_host = 0;
+        CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        return fail(BLD_ERR_DIVERGED, "The simulation has diverged.");
+    }
+    return BLD_OK;
+}
+
+int validate(const bld_config* c) {
+    if (c->n3 < 3) return fail(BLD_ERR_INVALID_CONFIG, "Due to boundary stencils, the grid needs at least 3 vertical layers");
+    if (c->n1 < 1 || c->n2 < 1) return fail(BLD_ERR_INVALID_CONFIG, "invalid horizontal resolution");
+    if (c->members < 1) return fail(BLD_ERR_INVALID_CONFIG, "members must be >= 1");
+    if (!c->dx3_c || !c->dx3_i || !c->x3_c || !c->x3_i) return fail(BLD_ERR_ARGUMENT, "vertical mapping tables missing");
+    if (c->pressure) {
+        if (c->bc_kind[2][0] != BLD_BC_DIRICHLET || c->bc_kind[2][1] != BLD_BC_DIRICHLET)
+            return fail(BLD_ERR_UNSUPPORTED_BC, "The pressure solver only supports Dirichlet BCs");
+        if (c->bc_value[2][0] != c->bc_value[2][1])
+            return fail(BLD_ERR_UNSUPPORTED_BC, "The mean flow must be equal at both vertical boundaries.");
+    }
+    if (c->advection || c->sgs) {
+        if (c->bc_kind[2][0] != BLD_BC_DIRICHLET || c->bc_kind[2][1] != BLD_BC_DIRICHLET)
+            return fail(BLD_ERR_UNSUPPORTED_BC, "physical-domain processes need Dirichlet boundaries for vel3");
+    }
+    if (c->advection && (c->bc_value[2][0] != 0.0 || c->bc_value[2][1] != 0.0))
+        return fail(BLD_ERR_UNSUPPORTED_BC, "Advection for non-zero w at boundary not implemented");
+    if (c->sgs) {
+        for (int s = 0; s < 2; ++s)
+            if (c->wall_kind[s] != BLD_WALL_ROUGH && c->wall_kind[s] != BLD_WALL_FREESLIP)
+                return fail(BLD_ERR_UNSUPPORTED_BC, "SGS model only supports rough-wall and free-slip boundaries");
+    }
+    if (c->diffusion[2] && (c->bc_kind[2][0] != BLD_BC_DIRICHLET || c->bc_kind[2][1] != BLD_BC_DIRICHLET))
+        return fail(BLD_ERR_UNSUPPORTED_BC, "diffusion of vel3 needs Dirichlet boundaries");
+    if (c->mean[2]) return fail(BLD_ERR_INVALID_CONFIG, "The constant-mean source currently does not handle I-nodes correctly");
+    return BLD_OK;
+}
+
+int setup_space(bld_handle* h, Space& s, int dealias, int e1, int e2, bool is_adv) {
+    const int k1 = h->g.k1max, k2 = h->g.k2max;
+    int r1, r2;
+    if (dealias == BLD_DEALIAS_QUADRATIC) {
+        r1 = pdsize_quadratic(k1);
+        r2 = pdsize_quadratic(k2);
+        s.P1 = next_even_smooth(r1);
+        s.P2 = next_even_smooth(r2);
+    } else if (dealias == BLD_DEALIAS_NONE) {
+        r1 = 2 * k1 + 2;
+        r2 = 2 * k2 + 2;
+        s.P1 = r1;
+        s.P2 = r2;
+    } else {
+        r1 = e1;
+        r2 = e2;
+        s.P1 = e1;
+        s.P2 = e2;
+    }
+    s.ref_P1 = r1;
+    s.ref_P2 = r2;
+    for (int P : {s.P1, s.P2})
+        if (!(P % 2 == 0 && smooth23(P)))
+            return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size %d is not an even 2^a*3^b (kernels support radix 2/3 only)", P);
+    if (s.P1 < 2 * k1 + 2 || s.P2 < 2 * k2 + 2)
+        return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size (%d, %d) smaller than the resolved modes", s.P1, s.P2);
+    if (s.P1 > 2048 || s.P2 > 2048) return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size above 2048");
+    s.plan1 = make_plan(s.P1);
+    s.plan2 = make_plan(s.P2);
+    BLD_TRY(twiddles(h, s.P1));
+    BLD_TRY(twiddles(h, s.P2));
+    s.ntin = is_adv ? 6 : 9;
+    s.ntout = is_adv ? 3 : 8;
+    tile_space(h, s);
+    const size_t cs = csize(h->fp32);
+    const long long layer = (long long)s.P2 * h->g.K1;
+    s.min_ms = (long long)s.ntin * h->g.n3 * layer;
+    s.mout_ms = (long long)s.ntout * h->g.n3 * layer;
+    BLD_TRY(dalloc(h, &s.min, (size_t)s.min_ms * h->B * cs));
+    BLD_TRY(dalloc(h, &s.mout, (size_t)s.mout_ms * h->B * cs));
+    CUDA_TRY(cudaMemset(s.mout, 0, (size_t)s.mout_ms * h->B * cs));
+    const size_t sm = is_adv ? smem_adv(s, h->fp32) : smem_sgs(s, h->fp32);
+    if (sm > 200 * 1024 || smem_y(s.P2, s.NLy, h->fp32) > 200 * 1024)
+        return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size (%d, %d) needs too much shared memory", s.P1, s.P2);
+    s.on = true;
+    return BLD_OK;
+}
+
+void free_handle(bld_handle* h) {
+    if (!h) return;
+    for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    void* ptrs[] = {h->u, h->t, h->du, h->dp, h->io, h->io2, h->pscr, h->gamma, h->d1, h->d2, h->DD1, h->DD2,
+                    h->alpha_c, h->alpha_i, h->alpha_ext, h->mean_w, h->lc2, h->li2, h->wall, h->src,
+                    h->mean_val, h->flag, h->adv.min, h->adv.mout, h->sgs.min, h->sgs.mout, h->pd_buf, h->pd_mixed};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto& kv : h->tw) {
+        cudaFree(kv.second.d64);
+        cudaFree(kv.second.d32);
+    }
+    if (h->flag_host) cudaFreeHost(h->flag_host);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // namespace
+
+// ======================================================================== C ABI
+extern "C" {
+
+int32_t bld_abi_version(void) { return BLD_ABI_VERSION; }
+
+const char* bld_status_string(int32_t s) {
+    switch (s) {
+        case BLD_OK: return "ok";
+        case BLD_ERR_INVALID_CONFIG: return "invalid configuration";
+        case BLD_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case BLD_ERR_DIVERGED: return "The simulation has diverged.";
+        case BLD_ERR_UNSUPPORTED_BC: return "unsupported boundary condition";
+        case BLD_ERR_CUDA: return "CUDA error";
+        case BLD_ERR_TIMEOUT: return "device wait timed out";
+        case BLD_ERR_ARGUMENT: return "invalid argument";
+        case BLD_ERR_NO_DEVICE: return "no usable CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int32_t bld_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return BLD_ERR_ARGUMENT;
+    snprintf(buf, len, "%s", g_last_error.c_str());
+    return BLD_OK;
+}
+
+int32_t bld_create(const bld_config* cfg, bld_handle** out) {
+    if (!cfg || !out) return fail(BLD_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    BLD_TRY(validate(cfg));
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || cfg->device >= ndev)
+        return fail(BLD_ERR_NO_DEVICE, "no CUDA device %d available", cfg->device);
+    CUDA_TRY(cudaSetDevice(cfg->device));
+    BLD_TRY(set_smem_limits());
+    bld_handle* h = new bld_handle();
+    h->cfg = *cfg;
+    h->device = cfg->device;
+    h->B = cfg->members;
+    h->fp32 = (cfg->precision == BLD_MIXED);
+    Geo& g = h->g;
+    g.k1max = (cfg->n1 - 1) / 2;
+    g.k2max = (cfg->n2 - 1) / 2;
+    g.K1 = g.k1max + 1;
+    g.K2 = 2 * g.k2max + 1;
+    g.n3 = cfg->n3;
+    g.F = g.K1 * g.K2;
+    g.mstride = (long long)(3 * g.n3 - 1) * g.F;
+    const int n3 = g.n3, K1 = g.K1, K2 = g.K2, B = h->B;
+    auto bail = [&](int code) {
+        free_handle(h);
+        return code;
+    };
+#define H_TRY(expr)                   \
+    do {                              \
+        int s_ = (expr);              \
+        if (s_ != BLD_OK) return bail(s_); \
+    } while (0)
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(BLD_ERR_CUDA, "cudaStreamCreate failed"));
+    const size_t sbytes = (size_t)B * g.mstride * sizeof(double2);
+    H_TRY(dalloc(h, (void**)&h->u, sbytes));
+    H_TRY(dalloc(h, (void**)&h->t, sbytes));
+    H_TRY(dalloc(h, (void**)&h->du, sbytes));
+    H_TRY(dalloc(h, (void**)&h->dp, sbytes));
+    H_TRY(dalloc(h, (void**)&h->io, sbytes));
+    H_TRY(dalloc(h, (void**)&h->io2, sbytes));
+    for (void* p : {(void*)h->u, (void*)h->t, (void*)h->du, (void*)h->dp, (void*)h->io, (void*)h->io2})
+        if (cudaMemset(p, 0, sbytes) != cudaSuccess) return bail(fail(BLD_ERR_CUDA, "cudaMemset failed"));
+    if (cfg->pressure) H_TRY(dalloc(h, (void**)&h->pscr, (size_t)B * n3 * g.F * sizeof(double2)));
+    H_TRY(dalloc(h, (void**)&h->flag, sizeof(int)));
+    if (cudaMemset(h->flag, 0, sizeof(int)) != cudaSuccess) return bail(fail(BLD_ERR_CUDA, "cudaMemset failed"));
+    if (cudaMallocHost(&h->flag_host, sizeof(int)) != cudaSuccess) return bail(fail(BLD_ERR_CUDA, "cudaMallocHost failed"));
+    *h->flag_host = 0;
+
+    // ---- wavenumber factors (src/Domains.jl:285-288, src/derivatives.jl:21-27)
+    const double TWO_PI = 2.0 * M_PI;
+    std::vector<double> d1(K1), d2(K2), DD1(K1), DD2(K2);
+    const double c1 = TWO_PI / cfg->l1, c2 = TWO_PI / cfg->l2;
+    for (int k = 0; k < K1; ++k) {
+        d1[k] = (double)k * c1;
+        DD1[k] = (double)(-(long long)k * k) * (c1 * c1);
+    }
+    for (int j = 0; j < K2; ++j) {
+        const long long k2 = (j <= g.k2max) ? j : j - K2;
+        d2[j] = (double)k2 * c2;
+        DD2[j] = (double)(-k2 * k2) * (c2 * c2);
+    }
+    // ---- vertical factors alpha = N3 / (dx3/dzeta) (src/derivatives.jl:10-19)
+    std::vector<double> ac(n3), ai(n3 - 1), aext(n3 + 1), mw(n3);
+    for (int i = 0; i < n3; ++i) ac[i] = (double)n3 / cfg->dx3_c[i];
+    for (int i = 0; i <= n3; ++i) aext[i] = (double)n3 / cfg->dx3_i[i];
+    for (int i = 0; i < n3 - 1; ++i) ai[i] = aext[i + 1];
+    const double L3 = cfg->x3_max - cfg->x3_min;
+    for (int i = 0; i < n3; ++i) mw[i] = 1.0 / ac[i] / L3;  // ConstantMean weight (src/processes/sources.jl:62)
+    H_TRY(upload(h, &h->d1, d1));
+    H_TRY(upload(h, &h->d2, d2));
+    H_TRY(upload(h, &h->DD1, DD1));
+    H_TRY(upload(h, &h->DD2, DD2));
+    H_TRY(upload(h, &h->alpha_c, ac));
+    H_TRY(upload(h, &h->alpha_i, ai));
+    H_TRY(upload(h, &h->alpha_ext, aext));
+    H_TRY(upload(h, &h->mean_w, mw));
+
+    // ---- pressure: d3g3 diagonal and LDL^T factor (src/processes/pressure.jl:231-296,85-95)
+    if (cfg->pressure) {
+        std::vector<double> d3g3(n3, 0.0);
+        for (int i = 1; i < n3; ++i) d3g3[i] -= aext[i];
+        for (int i = 0; i < n3 - 1; ++i) d3g3[i] -= aext[i + 1];
+        const double s1 = 1.0 / cfg->l1, s2 = 1.0 / cfg->l2;
+        const double fourpi2 = 4.0 * (M_PI * M_PI);
+        std::vector<double> gam((size_t)n3 * g.F);
+        std::vector<double> dv(n3);
+        for (int j = 0; j < K2; ++j) {
+            const long long k2 = (j <= g.k2max) ? j : j - K2;
+            for (int k = 0; k < K1; ++k) {
+                const int c = j * K1 + k;
+                if (k == 0 && k2 == 0) {
+                    for (int z = 0; z < n3; ++z) dv[z] = d3g3[z];
+                    dv[n3 - 1] = -3.0 * aext[n3 - 1];
+                } else {
+                    const double kk = (double)((long long)k * k) * (s1 * s1) + (double)(k2 * k2) * (s2 * s2);
+                    for (int z = 0; z < n3; ++z) dv[z] = d3g3[z] - fourpi2 * kk / ac[z];
+                }
+                double gp = 1.0 / dv[0];
+                gam[c] = gp;
+                for (int z = 1; z < n3; ++z) {
+                    const double be = ai[z - 1];
+                    gp = 1.0 / (dv[z] - gp * (be * be));
+                    gam[(size_t)z * g.F + c] = gp;
+                }
+            }
+        }
+        H_TRY(upload(h, &h->gamma, gam));
+    }
+
+    // ---- boundary conditions and the linear processes
+    h->w_lo = cfg->bc_value[2][0];
+    h->w_hi = cfg->bc_value[2][1];
+    Linear& L = h->lin;
+    for (int f = 0; f < 3; ++f) {
+        L.diff_on[f] = cfg->diffusion[f];
+        L.nu[f] = cfg->diffusivity[f];
+        L.src_on[f] = cfg->source[f];
+        for (int s = 0; s < 2; ++s) {
+            L.bc_kind[f][s] = cfg->bc_kind[f][s];
+            L.bc_val[f][s] = cfg->bc_value[f][s];
+            // ConstantGradient.difference = gradient * Dvmap(zeta_wall) / N3 (src/boundary_conditions.jl:299-320)
+            L.bc_diff[f][s] = cfg->bc_value[f][s] * (cfg->dx3_i[s == 0 ? 0 : n3] / (double)n3);
+        }
+    }
+    std::vector<double> src((size_t)3 * B), mval((size_t)3 * B);
+    for (int m = 0; m < B; ++m)
+        for (int f = 0; f < 3; ++f) {
+            src[3 * m + f] = cfg->source_strength[f];
+            if (f == 0 && cfg->member_source1) src[3 * m + f] = cfg->member_source1[m];
+            mval[3 * m + f] = cfg->mean_value[f];
+        }
+    H_TRY(upload(h, &h->src, src));
+    H_TRY(upload(h, &h->mean_val, mval));
+    L.DD1 = h->DD1;
+    L.DD2 = h->DD2;
+    L.alpha_c = h->alpha_c;
+    L.alpha_i = h->alpha_i;
+    L.alpha_ext = h->alpha_ext;
+    L.src = h->src;
+
+    // ---- SGS length scales and wall model (src/processes/static_smagorinsky.jl:44-123)
+    std::vector<double> lc2((size_t)B * n3, 0.0), li2((size_t)B * (n3 - 1), 0.0), wall((size_t)4 * B, 0.0);
+    if (cfg->sgs) {
+        const double D1 = cfg->l1 / (2.0 * g.k1max + 2.0), D2 = cfg->l2 / (2.0 * g.k2max + 2.0);
+        h->dyn_lo = cfg->wall_kind[0] == BLD_WALL_ROUGH;
+        h->dyn_hi = cfg->wall_kind[1] == BLD_WALL_ROUGH;
+        for (int m = 0; m < B; ++m) {
+            const double cs = cfg->member_cs ? cfg->member_cs[m] : cfg->sgs_cs;
+            const double z0lo = (cfg->member_z0_lower) ? cfg->member_z0_lower[m] : cfg->wall_z0[0];
+            auto ml = [&](double x3) {
+                double lo = INFINITY, hi = INFINITY;
+                if (cfg->wall_kind[0] == BLD_WALL_ROUGH) lo = (x3 - cfg->x3_min) * cfg->wall_kappa[0];
+                if (cfg->wall_kind[1] == BLD_WALL_ROUGH) hi = (cfg->x3_max - x3) * cfg->wall_kappa[1];
+                return std::min(lo, hi);
+            };
+            const double N = cfg->sgs_wall_damping_exponent;
+            for (int i = 0; i < n3; ++i) {
+                double l = cs * std::cbrt(D1 * D2 * (cfg->dx3_c[i] / n3));
+                if (cfg->sgs_wall_damping) l = std::pow(std::pow(l, -N) + std::pow(ml(cfg->x3_c[i]), -N), -1.0 / N);
+                lc2[(size_t)m * n3 + i] = l * l;
+            }
+            for (int i = 0; i < n3 - 1; ++i) {
+                double l = cs * std::cbrt(D1 * D2 * (cfg->dx3_i[i + 1] / n3));
+                if (cfg->sgs_wall_damping) l = std::pow(std::pow(l, -N) + std::pow(ml(cfg->x3_i[i]), -N), -1.0 / N);
+                li2[(size_t)m * (n3 - 1) + i] = l * l;
+            }
+            const double dxb = cfg->x3_c[0] - cfg->x3_min, dxa = cfg->x3_max - cfg->x3_c[n3 - 1];
+            double fs[2] = {0, 0}, ft[2] = {0, 0};
+            for (int s = 0; s < 2; ++s) {
+                if (cfg->wall_kind[s] != BLD_WALL_ROUGH) continue;
+                const double dx = s == 0 ? dxb : dxa;
+                const double z0 = s == 0 ? z0lo : cfg->wall_z0[1];
+                const double lg = std::log(dx / z0);
+                fs[s] = 1.0 / (2.0 * dx * lg);
+                ft[s] = -(cfg->wall_kappa[s] * cfg->wall_kappa[s]) / (lg * lg);
+            }
+            wall[4 * m + 0] = fs[0];
+            wall[4 * m + 1] = -fs[1];
+            wall[4 * m + 2] = ft[0];
+            wall[4 * m + 3] = -ft[1];
+        }
+    }
+    H_TRY(upload(h, &h->lc2, lc2));
+    H_TRY(upload(h, &h->li2, li2));
+    H_TRY(upload(h, &h->wall, wall));
+
+    // ---- physical-domain spaces
+    if (cfg->advection) H_TRY(setup_space(h, h->adv, cfg->adv_dealias, cfg->adv_p1, cfg->adv_p2, true));
+    if (cfg->sgs) H_TRY(setup_space(h, h->sgs, cfg->sgs_dealias, cfg->sgs_p1, cfg->sgs_p2, false));
+    // default-size transform for initialize!/getindex (src/physical_space.jl:44)
+    h->Pd1 = 2 * g.k1max + 2;
+    h->Pd2 = 2 * g.k2max + 2;
+    if (smooth23(h->Pd1) && smooth23(h->Pd2)) {
+        H_TRY(twiddles(h, h->Pd1));
+        H_TRY(twiddles(h, h->Pd2));
+        H_TRY(dalloc(h, &h->pd_buf, (size_t)n3 * h->Pd2 * h->Pd1 * sizeof(double)));
+        H_TRY(dalloc(h, &h->pd_mixed, (size_t)n3 * h->Pd2 * K1 * sizeof(double2)));
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(BLD_ERR_CUDA, "set-up failed"));
+#undef H_TRY
+    *out = h;
+    return BLD_OK;
+}
+
+void bld_destroy(bld_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_handle(h);
+}
+
+int32_t bld_get_info(const bld_handle* h, bld_info* info) {
+    if (!h || !info) return fail(BLD_ERR_ARGUMENT, "null argument");
+    memset(info, 0, sizeof *info);
+    info->k1max = h->g.k1max;
+    info->k2max = h->g.k2max;
+    info->n3 = h->g.n3;
+    info->members = h->B;
+    info->modes_per_layer = h->g.F;
+    info->state_doubles = 2 * h->g.mstride;
+    if (h->adv.on) {
+        info->adv_p1 = h->adv.P1;
+        info->adv_p2 = h->adv.P2;
+        info->adv_ref_p1 = h->adv.ref_P1;
+        info->adv_ref_p2 = h->adv.ref_P2;
+    }
+    if (h->sgs.on) {
+        info->sgs_p1 = h->sgs.P1;
+        info->sgs_p2 = h->sgs.P2;
+    }
+    info->device_bytes = (int64_t)h->bytes;
+    info->precision = h->cfg.precision;
+    return BLD_OK;
+}
+
+static int member_ok(const bld_handle* h, int m) { return h && m >= 0 && m < h->B; }
+
+static int copy_fields_h2d(bld_handle* h, double2* base, int m, const double* v1, const double* v2, const double* v3) {
+    const Geo& g = h->g;
+    double2* dst = base + (size_t)m * g.mstride;
+    const size_t nc = (size_t)g.n3 * g.F, ni = (size_t)(g.n3 - 1) * g.F;
+    CUDA_TRY(cudaMemcpyAsync(dst, v1, nc * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(dst + nc, v2, nc * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(dst + 2 * nc, v3, ni * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    return BLD_OK;
+}
+
+static int copy_fields_d2h(bld_handle* h, const double2* base, int m, double* v1, double* v2, double* v3) {
+    const Geo& g = h->g;
+    const double2* src = base + (size_t)m * g.mstride;
+    const size_t nc = (size_t)g.n3 * g.F, ni = (size_t)(g.n3 - 1) * g.F;
+    CUDA_TRY(cudaMemcpyAsync(v1, src, nc * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(v2, src + nc, nc * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(v3, src + 2 * nc, ni * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
+}
+
+int32_t bld_set_state(bld_handle* h, int32_t m, const double* v1, const double* v2, const double* v3) {
+    if (!member_ok(h, m) || !v1 || !v2 || !v3) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    BLD_TRY(copy_fields_h2d(h, h->u, m, v1, v2, v3));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->slope_valid = false;
+    h->ab2_started = false;
+    return BLD_OK;
+}
+
+int32_t bld_get_state(bld_handle* h, int32_t m, double* v1, double* v2, double* v3) {
+    if (!member_ok(h, m) || !v1 || !v2 || !v3) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    return copy_fields_d2h(h, h->u, m, v1, v2, v3);
+}
+
+int32_t bld_compute_rates(bld_handle* h, int32_t m, const double* v1, const double* v2, const double* v3,
+                          double* r1, double* r2, double* r3) {
+    if (!member_ok(h, m) || !v1 || !v2 || !v3 || !r1 || !r2 || !r3) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    BLD_TRY(copy_fields_h2d(h, h->io, m, v1, v2, v3));
+    BLD_TRY(enqueue_rates(h, h->io, h->io2, m, 1));
+    BLD_TRY(copy_fields_d2h(h, h->io2, m, r1, r2, r3));
+    return check_flag(h);
+}
+
+int32_t bld_apply_projections(bld_handle* h, int32_t m, double* v1, double* v2, double* v3) {
+    if (!member_ok(h, m) || !v1 || !v2 || !v3) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    BLD_TRY(copy_fields_h2d(h, h->io, m, v1, v2, v3));
+    BLD_TRY(enqueue_project(h, S_NONE, 0.0, h->io, nullptr, nullptr, nullptr, h->io, m, 1));
+    return copy_fields_d2h(h, h->io, m, v1, v2, v3);
+}
+
+int32_t bld_prepare(bld_handle* h) {
+    if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    BLD_TRY(enqueue_project(h, S_NONE, 0.0, h->u, nullptr, nullptr, nullptr, h->u, 0, h->B));
+    BLD_TRY(enqueue_rates(h, h->u, h->du, 0, h->B));
+    h->slope_valid = true;
+    h->ab2_started = false;
+    return check_flag(h);
+}
+
+static int step_impl(bld_handle* h, int64_t nsteps, double dt, int32_t method);
+
+int32_t bld_step(bld_handle* h, int64_t nsteps, double dt, int32_t method) {
+    BLD_TRY(step_impl(h, nsteps, dt, method));
+    return check_flag(h);
+}
+
+int32_t bld_step_async(bld_handle* h, int64_t nsteps, double dt, int32_t method) {
+    return step_impl(h, nsteps, dt, method);
+}
+
+static int step_impl(bld_handle* h, int64_t nsteps, double dt, int32_t method) {
+    if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
+    if (method < BLD_EULER || method > BLD_SSPRK33) return fail(BLD_ERR_ARGUMENT, "unknown method %d", method);
+    if (!h->slope_valid) return fail(BLD_ERR_ARGUMENT, "bld_prepare or bld_evolve must run before bld_step");
+    if (nsteps <= 0) return BLD_OK;
+    CUDA_TRY(cudaSetDevice(h->device));
+    int64_t done = 0;
+    if (method == BLD_AB2) {
+        if (h->ab2_started && h->ab2_dt != dt) return fail(BLD_ERR_ARGUMENT, "Cannot change time step for multi-step methods");
+        if (!h->ab2_started) {
+            BLD_TRY(enqueue_step(h, method, dt, true));
+            h->ab2_started = true;
+            h->ab2_dt = dt;
+            done = 1;
+        }
+    }
+    if (done < nsteps) {
+        const auto key = std::make_pair((int)method, dt);
+        auto it = h->graphs.find(key);
+        if (it == h->graphs.end()) {
+            cudaGraph_t graph;
+            CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            int st = enqueue_step(h, method, dt, false);
+            cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+            if (st != BLD_OK) {
+                if (ce == cudaSuccess) cudaGraphDestroy(graph);
+                return st;
+            }
+            CUDA_TRY(ce);
+            cudaGraphExec_t exec;
+            cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            CUDA_TRY(ie);
+            it = h->graphs.emplace(key, exec).first;
+        }
+        for (; done < nsteps; ++done) CUDA_TRY(cudaGraphLaunch(it->second, h->stream));
+    }
+    return BLD_OK;
+}
+
+int32_t bld_get_stream(bld_handle* h, void** stream) {
+    if (!h || !stream) return fail(BLD_ERR_ARGUMENT, "null argument");
+    *stream = (void*)h->stream;
+    return BLD_OK;
+}
+
+static int launches_per_rhs(const bld_handle* h) {
+    int n = 0;
+    if (h->adv.on) n += 3;
+    if (h->sgs.on) n += 3;
+    return n ? n : 1;
+}
+
+int32_t bld_time_phases(bld_handle* h, int32_t iters, int32_t method, bld_phase_times* out) {
+    if (!h || !out || iters < 1) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    memset(out, 0, sizeof *out);
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    auto timeit = [&](auto&& fn, double* ms) -> int {
+        BLD_TRY(fn());  // warm-up launch
+        CUDA_TRY(cudaEventRecord(e0, h->stream));
+        for (int i = 0; i < iters; ++i) BLD_TRY(fn());
+        CUDA_TRY(cudaEventRecord(e1, h->stream));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float t = 0;
+        CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+        *ms = (double)t / iters;
+        return BLD_OK;
+    };
+    int st = BLD_OK;
+    const int B = h->B;
+    for (int sp = 0; sp < 2 && st == BLD_OK; ++sp) {
+        if (!(sp == 0 ? h->adv.on : h->sgs.on)) continue;
+        st = timeit([&] { return enqueue_inv_y(h, sp, h->u, 0, B); }, &out->inv_y_ms[sp]);
+        if (st == BLD_OK) st = timeit([&] { return enqueue_x(h, sp, 0, B); }, &out->x_ms[sp]);
+        if (st == BLD_OK)
+            st = timeit([&] { return enqueue_fwd_y(h, sp, true, false, h->u, h->io2, 0, B); }, &out->fwd_y_ms[sp]);
+    }
+    if (st == BLD_OK && !h->adv.on && !h->sgs.on)
+        st = timeit([&] { return enqueue_linear(h, h->u, h->io2, 0, B); }, &out->linear_ms);
+    if (st == BLD_OK)
+        st = timeit([&] { return enqueue_project(h, S_NONE, 0.0, h->u, nullptr, nullptr, nullptr, h->io, 0, B); },
+                    &out->project_ms);
+    const int stages = method == BLD_SSPRK33 ? 3 : method == BLD_SSPRK22 ? 2 : 1;
+    const bool proj = h->cfg.pressure || h->cfg.mean[0] || h->cfg.mean[1];
+    out->launches_per_step = stages * (launches_per_rhs(h) + (proj || stages > 1 ? 1 : 1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st == BLD_OK) CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    return st;
+}
+
+int32_t bld_evolve(bld_handle* h, double t1, double t2, double dt, int32_t method) {
+    if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
+    if (t1 > t2) return fail(BLD_ERR_ARGUMENT, "Integration start time is larger than end time");
+    BLD_TRY(bld_prepare(h));
+    if (t2 > t1) {
+        const double r = (t2 - t1) / dt;
+        const double ri = std::round(r);
+        if (std::fabs(r - ri) > std::sqrt(2.220446049250313e-16) * std::max(std::fabs(r), std::fabs(ri)))
+            return fail(BLD_ERR_ARGUMENT, "Division has a non-integer result");
+        BLD_TRY(bld_step(h, (int64_t)ri, dt, method));
+    }
+    return BLD_OK;
+}
+
+int32_t bld_compute_rates_device(bld_handle* h, const void* state, void* rates, void* stream) {
+    if (!h || !state || !rates) return fail(BLD_ERR_ARGUMENT, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t keep = h->stream;
+    if (stream) h->stream = (cudaStream_t)stream;
+    int s = enqueue_rates(h, (const double2*)state, (double2*)rates, 0, h->B);
+    h->stream = keep;
+    return s;
+}
+
+int32_t bld_apply_projections_device(bld_handle* h, void* state, void* stream) {
+    if (!h || !state) return fail(BLD_ERR_ARGUMENT, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t keep = h->stream;
+    if (stream) h->stream = (cudaStream_t)stream;
+    int s = enqueue_project(h, S_NONE, 0.0, (const double2*)state, nullptr, nullptr, nullptr, (double2*)state, 0, h->B);
+    h->stream = keep;
+    return s;
+}
+
+int32_t bld_state_device_ptr(bld_handle* h, void** state) {
+    if (!h || !state) return fail(BLD_ERR_ARGUMENT, "null argument");
+    *state = h->u;
+    return BLD_OK;
+}
+
+int32_t bld_sync(bld_handle* h) {
+    if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    return check_flag(h);
+}
+
+int32_t bld_set_field_physical(bld_handle* h, int32_t m, int32_t field, const double* values) {
+    if (!member_ok(h, m) || field < 0 || field > 2 || !values) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    if (!h->pd_buf) return fail(BLD_ERR_INVALID_CONFIG, "default physical size is not an even 2^a*3^b");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const Geo& g = h->g;
+    const int nz = field == 2 ? g.n3 - 1 : g.n3;
+    const int P1 = h->Pd1, P2 = h->Pd2;
+    CUDA_TRY(cudaMemcpyAsync(h->pd_buf, values, (size_t)nz * P2 * P1 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    XPlainArgs xa{};
+    xa.P1 = P1;
+    xa.P2 = P2;
+    xa.K1 = g.K1;
+    xa.k1max = g.k1max;
+    xa.nz = nz;
+    xa.pd = (const double*)h->pd_buf;
+    xa.mixed_out = (double2*)h->pd_mixed;
+    xa.plan = make_plan(P1);
+    xa.tw = (const double2*)twp(h, P1, false);
+    const long long rows = (long long)nz * P2;
+    k_x_r2c<<<(unsigned)((rows + 1) / 2), 256, (size_t)3 * P1 * sizeof(double2), h->stream>>>(xa);
+    CUDA_TRY(cudaGetLastError());
+    // forward y pass, assigning the truncated modes (set_field!, src/physical_space.jl:253-256)
+    Space s{};
+    s.P1 = P1;
+    s.P2 = P2;
+    pick_y(g, P2, false, s.NLy, s.MAXO);
+    FwdYArgs fa{};
+    fa.g = g;
+    fa.P1 = P1;
+    fa.P2 = P2;
+    fa.mout = h->pd_mixed;
+    fa.mout_mstride = 0;
+    fa.ncontrib[0] = 1;
+    fa.c[0][0] = FwdContrib{0, 0};
+    fa.mode = 2;
+    fa.check = 0;
+    fa.du = h->u + (size_t)m * g.mstride;
+    fa.du_mstride = 0;
+    fa.inv_n = 1.0 / ((double)P1 * (double)P2);
+    fa.flag = h->flag;
+    fa.fields = 1;
+    fa.field0 = field;
+    fa.m0 = 0;
+    fa.plan = make_plan(P2);
+    fa.tw = twp(h, P2, false);
+    BLD_TRY(launch_fwd_y<double>(h, s, fa, 1));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->slope_valid = false;
+    return BLD_OK;
+}
+
+int32_t bld_get_field_physical(bld_handle* h, int32_t m, int32_t field, double* values) {
+    if (!member_ok(h, m) || field < 0 || field > 2 || !values) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    if (!h->pd_buf) return fail(BLD_ERR_INVALID_CONFIG, "default physical size is not an even 2^a*3^b");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const Geo& g = h->g;
+    const int nz = field == 2 ? g.n3 - 1 : g.n3;
+    const int P1 = h->Pd1, P2 = h->Pd2;
+    Space s{};
+    s.P1 = P1;
+    s.P2 = P2;
+    pick_y(g, P2, false, s.NLy, s.MAXO);
+    InvYArgs ia{};
+    ia.g = g;
+    ia.P2 = P2;
+    ia.nterms = 1;
+    ia.op[0] = T_DIRECT;
+    ia.fld[0] = field;
+    ia.isI[0] = field == 2;
+    ia.m0 = m;
+    ia.state = h->u;
+    ia.mixed = h->pd_mixed;
+    ia.mixed_mstride = 0;
+    ia.d1 = h->d1;
+    ia.d2 = h->d2;
+    ia.alpha_i = h->alpha_i;
+    ia.plan = make_plan(P2);
+    ia.tw = twp(h, P2, false);
+    BLD_TRY(launch_inv_y<double>(h, s, ia, 1));
+    XPlainArgs xa{};
+    xa.P1 = P1;
+    xa.P2 = P2;
+    xa.K1 = g.K1;
+    xa.k1max = g.k1max;
+    xa.nz = nz;
+    xa.pd_out = (double*)h->pd_buf;
+    xa.mixed_in = (const double2*)h->pd_mixed;
+    xa.plan = make_plan(P1);
+    xa.tw = (const double2*)twp(h, P1, false);
+    const long long rows = (long long)nz * P2;
+    k_x_c2r<<<(unsigned)((rows + 1) / 2), 256, (size_t)3 * P1 * sizeof(double2), h->stream>>>(xa);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(values, h->pd_buf, (size_t)nz * P2 * P1 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
+}
+
+int32_t bld_ldlt_solve_device(const double* gamma, const double* beta, void* rhs, int64_t nsys, int32_t n, void* stream) {
+    if (!gamma || !beta || !rhs || nsys <= 0 || n < 1) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    const unsigned blocks = (unsigned)((nsys + 127) / 128);
+    k_ldlt_solve<<<blocks, 128, 0, (cudaStream_t)stream>>>(gamma, beta, (double2*)rhs, nsys, n);
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+}  // extern "C"

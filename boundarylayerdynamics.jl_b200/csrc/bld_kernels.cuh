@@ -1,0 +1,1001 @@
+// Device kernels of the right-hand side, the pressure projection and the
+// SSP-RK stage update.  R is the arithmetic type of the physical-domain path
+// (double for the plain form, float for the mixed form); the spectral state,
+// the linear terms and the pressure solve are always double.
+//
+// Data flow of one nonlinear process (physical-domain size P1 x P2):
+//   k_inv_y  : spectral terms (per z layer, per k1 line) -> complex IFFT along y
+//              -> "mixed" array M[term][z][y][k1]                 (get_layer! part 1)
+//   k_adv_x / k_sgs_x : per y row, streaming upward in z: c2r along x of two
+//              terms packed in one complex FFT, the physical-domain products with
+//              their z neighbours, r2c along x of the rates      (get_layer! part 2,
+//              the process's add_rates!, add_layer! part 1)
+//   k_fwd_y  : complex FFT along y of every rate term, truncation, 1/(P1 P2),
+//              D1/D2 prefactors, summed with the linear terms into du
+//                                                               (add_layer! part 2)
+#pragma once
+
+#include "bld_fft.cuh"
+
+#define BLD_MAXT 10
+#define BLD_MAXC 4
+
+struct Geo {
+    int K1, K2, k1max, k2max, n3, F;  // F = K1*K2 modes per layer
+    long long mstride;                // complex values per member state (3*n3-1)*F
+};
+
+__device__ __forceinline__ long long fld_off(const Geo& g, int f) { return (long long)f * g.n3 * g.F; }
+
+// ------------------------------------------------------------------ inverse y pass
+enum TermOp { T_DIRECT = 0, T_D1 = 1, T_D2 = 2, T_VORT1 = 3, T_VORT2 = 4, T_VORT3 = 5 };
+
+struct InvYArgs {
+    Geo g;
+    int P2;
+    int nterms;
+    int op[BLD_MAXT];
+    int fld[BLD_MAXT];
+    int isI[BLD_MAXT];
+    int m0;                      // first member
+    const double2* state;
+    void* mixed;
+    long long mixed_mstride;     // elements per member
+    const double* d1;            // [K1] k1 * 2pi/L1
+    const double* d2;            // [K2] k2 * 2pi/L2
+    const double* alpha_i;       // [n3-1]
+    FftPlan plan;
+    const void* tw;
+};
+
+// value of spectral term `op` at (z, j, k1); D1 = i*d1, D2 = i*d2
+// (src/derivatives.jl:67-80,228-230; src/Domains.jl:285-288)
+__device__ __forceinline__ double2 inv_term_value(const InvYArgs& a, const double2* __restrict__ S, int op, int f,
+                                                  int z, int j, int k1) {
+    const Geo& g = a.g;
+    const long long mo = (long long)j * g.K1 + k1;
+    switch (op) {
+        case T_DIRECT:
+            return S[fld_off(g, f) + (long long)z * g.F + mo];
+        case T_D1: {
+            const double2 s = S[fld_off(g, f) + (long long)z * g.F + mo];
+            const double d = a.d1[k1];
+            return make_double2(-d * s.y, d * s.x);
+        }
+        case T_D2: {
+            const double2 s = S[fld_off(g, f) + (long long)z * g.F + mo];
+            const double d = a.d2[j];
+            return make_double2(-d * s.y, d * s.x);
+        }
+        case T_VORT1: {  // D2*w - (-a*v(z) + a*v(z+1))
+            const double2 w = S[fld_off(g, 2) + (long long)z * g.F + mo];
+            const double2 v0 = S[fld_off(g, 1) + (long long)z * g.F + mo];
+            const double2 v1 = S[fld_off(g, 1) + (long long)(z + 1) * g.F + mo];
+            const double al = a.alpha_i[z], d = a.d2[j];
+            const double dzx = -al * v0.x + al * v1.x, dzy = -al * v0.y + al * v1.y;
+            return make_double2(-d * w.y - dzx, d * w.x - dzy);
+        }
+        case T_VORT2: {  // (-a*u(z) + a*u(z+1)) - D1*w
+            const double2 w = S[fld_off(g, 2) + (long long)z * g.F + mo];
+            const double2 u0 = S[fld_off(g, 0) + (long long)z * g.F + mo];
+            const double2 u1 = S[fld_off(g, 0) + (long long)(z + 1) * g.F + mo];
+            const double al = a.alpha_i[z], d = a.d1[k1];
+            const double dzx = -al * u0.x + al * u1.x, dzy = -al * u0.y + al * u1.y;
+            return make_double2(dzx - (-d * w.y), dzy - d * w.x);
+        }
+        default: {  // T_VORT3: D1*v - D2*u
+            const double2 v = S[fld_off(g, 1) + (long long)z * g.F + mo];
+            const double2 u = S[fld_off(g, 0) + (long long)z * g.F + mo];
+            const double e1 = a.d1[k1], e2 = a.d2[j];
+            return make_double2(-e1 * v.y - (-e2 * u.y), e1 * v.x - e2 * u.x);
+        }
+    }
+}
+
+// grid (ceil(K1/NL), n3, nterms*members); smem: tw[P2] + 2*P2*NL complex
+template <typename R, int NL>
+__global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* b0 = tw + a.P2;
+    C* b1 = b0 + a.P2 * NL;
+    const int t = blockIdx.z % a.nterms, m = a.m0 + blockIdx.z / a.nterms;
+    const int z = blockIdx.y;
+    const int nz = a.isI[t] ? a.g.n3 - 1 : a.g.n3;
+    if (z >= nz) return;
+    const int op = a.op[t], f = a.fld[t];
+    const int K1 = a.g.K1, K2 = a.g.K2, k2max = a.g.k2max, P2 = a.P2;
+    const int k10 = blockIdx.x * NL;
+    const C* twg = reinterpret_cast<const C*>(a.tw);
+    for (int i = threadIdx.x; i < P2; i += blockDim.x) tw[i] = twg[i];
+    const double2* S = a.state + (long long)m * a.g.mstride;
+    for (int i = threadIdx.x; i < P2 * NL; i += blockDim.x) {
+        const int p = i / NL, l = i - p * NL;
+        const int k1 = k10 + l;
+        int j = -1;
+        if (p <= k2max)
+            j = p;
+        else if (p >= P2 - k2max)
+            j = K2 - (P2 - p);
+        double2 v = make_double2(0.0, 0.0);
+        if (j >= 0 && k1 < K1) v = inv_term_value(a, S, op, f, z, j, k1);
+        b0[i] = mk<R>((R)v.x, (R)v.y);
+    }
+    __syncthreads();
+    C* res = fft_run<R, +1>(b0, b1, NL, 1, NL, false, a.plan, tw);
+    C* out = reinterpret_cast<C*>(a.mixed) + (long long)m * a.mixed_mstride + (long long)(t * a.g.n3 + z) * P2 * K1;
+    for (int i = threadIdx.x; i < P2 * NL; i += blockDim.x) {
+        const int y = i / NL, l = i - y * NL, k1 = k10 + l;
+        if (k1 < K1) out[(long long)y * K1 + k1] = res[i];
+    }
+}
+
+// ----------------------------------------------------------- physical x kernels
+struct XArgs {
+    Geo g;
+    int P1, P2, YT, zchunk;
+    int m0;
+    const void* min;
+    void* mout;
+    long long min_mstride, mout_mstride;  // elements per member
+    FftPlan plan;
+    const void* tw;
+    // SGS only
+    const double* alpha_c;   // [n3]
+    const double* alpha_i;   // [n3-1]
+    const double* lc;        // [members][n3]   Smagorinsky length^2 at C nodes
+    const double* li;        // [members][n3-1] ... at I nodes
+    const double* wall;      // [members][4]: strain factor lo, hi; stress factor lo, hi
+    int dyn_lo, dyn_hi;      // rough wall (dynamic wall-model values) below / above
+    double w_lo, w_hi;       // Dirichlet values of vel3
+};
+
+template <typename C>
+__device__ __forceinline__ const C* mrow(const C* M, const XArgs& a, int t, int z, int y) {
+    return M + ((long long)(t * a.g.n3 + z) * a.P2 + y) * a.g.K1;
+}
+template <typename C>
+__device__ __forceinline__ C* mrow_w(C* M, const XArgs& a, int t, int z, int y) {
+    return M + ((long long)(t * a.g.n3 + z) * a.P2 + y) * a.g.K1;
+}
+
+// Build packed line Z[k] = A[k] + i B[k] (Hermitian-extended, DC imaginary parts
+// dropped as in FFTW's c2r) from mixed rows A (term ta) and B (term tb).
+template <typename R>
+__device__ __forceinline__ void build_packed(cplx<R>* line, const cplx<R>* rowA, const cplx<R>* rowB, int k, int P1) {
+    using C = cplx<R>;
+    C A = rowA ? rowA[k] : mk<R>(0, 0);
+    C B = rowB ? rowB[k] : mk<R>(0, 0);
+    if (k == 0) {
+        line[0] = mk<R>(A.x, B.x);
+    } else {
+        line[k] = mk<R>(A.x - B.y, A.y + B.x);          // A + iB
+        line[P1 - k] = mk<R>(A.x + B.y, -A.y + B.x);    // conj(A) + i conj(B)
+    }
+}
+
+// Unpack forward FFT Z of a + ib: A[k] = (Z[k] + conj(Z[-k]))/2, B[k] = (Z[k] - conj(Z[-k]))/(2i)
+template <typename R>
+__device__ __forceinline__ void unpack_pair(const cplx<R>* line, int k, int P1, cplx<R>& A, cplx<R>& B) {
+    const cplx<R> Zk = line[k];
+    const cplx<R> Zr = line[k == 0 ? 0 : P1 - k];
+    A = mk<R>((Zk.x + Zr.x) * R(0.5), (Zk.y - Zr.y) * R(0.5));
+    const R dx = Zk.x - Zr.x, dy = Zk.y + Zr.y;
+    B = mk<R>(dy * R(0.5), -dx * R(0.5));
+}
+
+// Rotation-form advection (src/processes/momentum_advection.jl:44-206).
+// Inputs: terms 0 u, 1 v, 5 vort3 (C); 2 w, 3 vort1, 4 vort2 (I).
+// Outputs: 0 adv1, 1 adv2 (C); 2 adv3 (I).
+// grid (P2/YT, nchunks, members), block YT*P1/PPT threads.
+template <typename R, int PPT>
+__global__ void __launch_bounds__(512) k_adv_x(XArgs a) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int P1 = a.P1, YT = a.YT, n3 = a.g.n3, k1max = a.g.k1max;
+    const int NLin = 3 * YT, NLout = YT + (YT + 1) / 2;
+    const int NLmax = NLin > NLout ? NLin : NLout;
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* cur = tw + P1;
+    C* scr = cur + NLmax * P1;
+    C* outb = scr + NLmax * P1;
+    const int y0 = blockIdx.x * YT;
+    const int m = a.m0 + blockIdx.z;
+    const int z0 = blockIdx.y * a.zchunk;
+    const int z1 = min(n3, z0 + a.zchunk);
+    const int nthr = blockDim.x;
+    const C* twg = reinterpret_cast<const C*>(a.tw);
+    for (int i = threadIdx.x; i < P1; i += nthr) tw[i] = twg[i];
+    const C* Min = reinterpret_cast<const C*>(a.min) + (long long)m * a.min_mstride;
+    C* Mout = reinterpret_cast<C*>(a.mout) + (long long)m * a.mout_mstride;
+
+    R pu[PPT], pv[PPT], pw[PPT], po1[PPT], po2[PPT];
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) pu[i] = pv[i] = pw[i] = po1[i] = po2[i] = R(0);
+
+    for (int j = max(0, z0 - 1); j < z1; ++j) {
+        const bool hasI = (j < n3 - 1);
+        // ---- build packed input lines: (u, v), (vort3, w), (vort1, vort2) per y
+        for (int i = threadIdx.x; i < NLin * P1; i += nthr) {
+            const int line = i / P1, k = i - line * P1;
+            if (k > k1max && k < P1 - k1max) {
+                cur[i] = mk<R>(0, 0);
+                continue;
+            }
+            if (k > k1max) continue;  // mirrored half written by the owner of P1-k
+            const int yl = line / 3, q = line - yl * 3, y = y0 + yl;
+            const C *ra, *rb;
+            if (q == 0) {
+                ra = mrow(Min, a, 0, j, y);
+                rb = mrow(Min, a, 1, j, y);
+            } else if (q == 1) {
+                ra = mrow(Min, a, 5, j, y);
+                rb = hasI ? mrow(Min, a, 2, j, y) : nullptr;
+            } else {
+                ra = hasI ? mrow(Min, a, 3, j, y) : nullptr;
+                rb = hasI ? mrow(Min, a, 4, j, y) : nullptr;
+            }
+            build_packed<R>(cur + line * P1, ra, rb, k, P1);
+        }
+        __syncthreads();
+        C* res = fft_run<R, +1>(cur, scr, NLin, P1, 1, true, a.plan, tw);
+        if (res != cur) {
+            scr = cur;
+            cur = res;
+        }
+        const bool emitC = (j >= z0);
+        const bool emitI = (j >= z0) && (j >= 1);
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) {
+            const int p = threadIdx.x + i * nthr;
+            const int yl = p / P1, x = p - yl * P1;
+            const C c0 = cur[(yl * 3 + 0) * P1 + x];
+            const C c1 = cur[(yl * 3 + 1) * P1 + x];
+            const C c2 = cur[(yl * 3 + 2) * P1 + x];
+            const R u = c0.x, v = c0.y, o3 = c1.x;
+            const R w = hasI ? c1.y : R(0);
+            const R o1 = hasI ? c2.x : R(0);
+            const R o2 = hasI ? c2.y : R(0);
+            if (emitC) {
+                R adv1, adv2;
+                if (j == 0) {  // w below is the (zero) boundary value (:181-184,:194-197)
+                    adv1 = o3 * v - R(0.5) * (o2 * w);
+                    adv2 = R(0.5) * (o1 * w) - o3 * u;
+                } else if (j == n3 - 1) {  // w above is the boundary value (:185-188,:198-201)
+                    adv1 = o3 * v - R(0.5) * (po2[i] * pw[i]);
+                    adv2 = R(0.5) * (po1[i] * pw[i]) - o3 * u;
+                } else {  // (:180,:193)
+                    adv1 = o3 * v - R(0.5) * (po2[i] * pw[i] + o2 * w);
+                    adv2 = R(0.5) * (po1[i] * pw[i] + o1 * w) - o3 * u;
+                }
+                outb[yl * P1 + x] = mk<R>(adv1, adv2);
+            }
+            if (emitI) {  // adv3 on I layer j-1 (:206)
+                const R adv3 = po2[i] * R(0.5) * (pu[i] + u) - po1[i] * R(0.5) * (pv[i] + v);
+                C* o = outb + (YT + yl / 2) * P1 + x;
+                if (yl & 1) {
+                    o->y = adv3;
+                } else {
+                    o->x = adv3;
+                    if (yl + 1 >= YT) o->y = R(0);
+                }
+            }
+            pu[i] = u;
+            pv[i] = v;
+            pw[i] = w;
+            po1[i] = o1;
+            po2[i] = o2;
+        }
+        if (emitC) {
+            __syncthreads();
+            C* r2 = fft_run<R, -1>(outb, scr, NLout, P1, 1, true, a.plan, tw);
+            const int nk = k1max + 1;
+            for (int i = threadIdx.x; i < NLout * nk; i += nthr) {
+                const int line = i / nk, k = i - line * nk;
+                C A, B;
+                unpack_pair<R>(r2 + line * P1, k, P1, A, B);
+                if (line < YT) {
+                    const int y = y0 + line;
+                    mrow_w(Mout, a, 0, j, y)[k] = A;
+                    mrow_w(Mout, a, 1, j, y)[k] = B;
+                } else if (emitI) {
+                    const int q = line - YT;
+                    const int ya = y0 + 2 * q, yb = ya + 1;
+                    mrow_w(Mout, a, 2, j - 1, ya)[k] = A;
+                    if (2 * q + 1 < YT) mrow_w(Mout, a, 2, j - 1, yb)[k] = B;
+                }
+            }
+            // restore outb as the output staging buffer for the next layer
+            if (r2 != outb) {
+                scr = outb;
+                outb = r2;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Static Smagorinsky model with the rough-wall model
+// (src/processes/static_smagorinsky.jl:129-249, src/derivatives.jl:104-138,235-241).
+// Inputs: 0 u, 1 v, 3 u_1, 4 u_2, 5 v_1, 6 v_2 (C); 2 w, 7 w_1, 8 w_2 (I).
+// Outputs (physical-domain rates, i.e. minus the SGS stress terms):
+//   0 -tau11 (C, D1 -> vel1)   1 -tau12 (C, D2 -> vel1 and D1 -> vel2)
+//   2 -tau22 (C, D2 -> vel2)   3 -d3 tau13 (C -> vel1)   4 -d3 tau23 (C -> vel2)
+//   5 -d3 tau33 (I -> vel3)    6 -tau13 (I, D1 -> vel3)   7 -tau23 (I, D2 -> vel3)
+// Streaming in z with a two-layer lag: step j loads C layer j and I layer j and
+// completes C layer j-1, I layer j-1 and the d3 tau33 of I layer j-2.
+template <typename R, int PPT>
+__global__ void __launch_bounds__(512) k_sgs_x(XArgs a) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int P1 = a.P1, YT = a.YT, n3 = a.g.n3, k1max = a.g.k1max;
+    const int NLin = 5 * YT, NLout = 4 * YT;
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* cur = tw + P1;
+    C* scr = cur + NLin * P1;
+    C* outb = scr + NLin * P1;
+    const int y0 = blockIdx.x * YT;
+    const int m = a.m0 + blockIdx.z;
+    const int z0 = blockIdx.y * a.zchunk;
+    const int z1 = min(n3, z0 + a.zchunk);
+    const int nthr = blockDim.x;
+    const C* twg = reinterpret_cast<const C*>(a.tw);
+    for (int i = threadIdx.x; i < P1; i += nthr) tw[i] = twg[i];
+    const C* Min = reinterpret_cast<const C*>(a.min) + (long long)m * a.min_mstride;
+    C* Mout = reinterpret_cast<C*>(a.mout) + (long long)m * a.mout_mstride;
+    const double* lcm = a.lc + (long long)m * n3;
+    const double* lim = a.li + (long long)m * (n3 - 1);
+    const R fs_lo = (R)a.wall[4 * m + 0], fs_hi = (R)a.wall[4 * m + 1];
+    const R ft_lo = (R)a.wall[4 * m + 2], ft_hi = (R)a.wall[4 * m + 3];
+    const R wlo = (R)a.w_lo, whi = (R)a.w_hi;
+
+    R pu[PPT], pv[PPT], pw[PPT], pw1[PPT], pw2[PPT];
+    R ps11[PPT], ps22[PPT], ps33[PPT], ps12[PPT], psc[PPT];
+    R s13pp[PPT], s23pp[PPT], t13pp[PPT], t23pp[PPT], t33pp[PPT];
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) {
+        pu[i] = pv[i] = pw[i] = pw1[i] = pw2[i] = R(0);
+        ps11[i] = ps22[i] = ps33[i] = ps12[i] = psc[i] = R(0);
+        s13pp[i] = s23pp[i] = t13pp[i] = t23pp[i] = t33pp[i] = R(0);
+    }
+
+    const int jend = min(n3, z1 + 1);
+    for (int j = max(0, z0 - 2); j <= jend; ++j) {
+        const bool hasC = (j <= n3 - 1), hasI = (j <= n3 - 2);
+        if (hasC) {
+            for (int i = threadIdx.x; i < NLin * P1; i += nthr) {
+                const int line = i / P1, k = i - line * P1;
+                if (k > k1max && k < P1 - k1max) {
+                    cur[i] = mk<R>(0, 0);
+                    continue;
+                }
+                if (k > k1max) continue;
+                const int yl = line / 5, q = line - yl * 5, y = y0 + yl;
+                const C *ra, *rb;
+                switch (q) {
+                    case 0: ra = mrow(Min, a, 0, j, y); rb = mrow(Min, a, 1, j, y); break;
+                    case 1: ra = mrow(Min, a, 3, j, y); rb = mrow(Min, a, 4, j, y); break;
+                    case 2: ra = mrow(Min, a, 5, j, y); rb = mrow(Min, a, 6, j, y); break;
+                    case 3: ra = hasI ? mrow(Min, a, 2, j, y) : nullptr; rb = hasI ? mrow(Min, a, 7, j, y) : nullptr; break;
+                    default: ra = hasI ? mrow(Min, a, 8, j, y) : nullptr; rb = nullptr; break;
+                }
+                build_packed<R>(cur + line * P1, ra, rb, k, P1);
+            }
+            __syncthreads();
+            C* res = fft_run<R, +1>(cur, scr, NLin, P1, 1, true, a.plan, tw);
+            if (res != cur) {
+                scr = cur;
+                cur = res;
+            }
+        }
+        const int c = j - 1;                                   // C layer completed at this step
+        const bool doC = (j >= 1) && (c >= z0) && (c < z1);
+        const bool do67 = (j >= 1) && (j <= n3 - 1) && (c >= z0) && (c < z1);
+        const bool do5 = (j >= 2) && (j - 2 >= z0) && (j - 2 < z1) && (j - 2 <= n3 - 2);
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) {
+            const int p = threadIdx.x + i * nthr;
+            const int yl = p / P1, x = p - yl * P1;
+            R u = 0, v = 0, u1 = 0, u2 = 0, v1 = 0, v2 = 0, w = whi, w1 = 0, w2 = 0;
+            if (hasC) {
+                const C c0 = cur[(yl * 5 + 0) * P1 + x], c1 = cur[(yl * 5 + 1) * P1 + x];
+                const C c2 = cur[(yl * 5 + 2) * P1 + x];
+                u = c0.x; v = c0.y; u1 = c1.x; u2 = c1.y; v1 = c2.x; v2 = c2.y;
+                if (hasI) {
+                    const C c3 = cur[(yl * 5 + 3) * P1 + x], c4 = cur[(yl * 5 + 4) * P1 + x];
+                    w = c3.x; w1 = c3.y; w2 = c4.x;
+                }
+            }
+            // (a) strain on C layer j (vel3_3 by dx3_i2c with Dirichlet w, :202-216)
+            R s11 = 0, s22 = 0, s33 = 0, s12 = 0, sc = 0;
+            if (hasC) {
+                const R ac = (R)a.alpha_c[j];
+                const R wb = (j == 0) ? wlo : pw[i];
+                s33 = -ac * wb + ac * w;
+                s11 = u1;
+                s22 = v2;
+                s12 = (u2 + v1) / R(2);
+                sc = s11 * s11 + s22 * s22 + s33 * s33 + R(2) * (s12 * s12);
+            }
+            // (b) I layer j-1: S13, S23, eddy viscosity, tau13, tau23
+            R s13 = 0, s23 = 0, sg13 = 0, sg23 = 0;
+            if (j >= 1 && j <= n3 - 1) {
+                const R ai = (R)a.alpha_i[j - 1];
+                s13 = ((-ai * pu[i] + ai * u) + pw1[i]) / R(2);
+                s23 = ((-ai * pv[i] + ai * v) + pw2[i]) / R(2);
+                R si = R(2) * (s13 * s13) + R(2) * (s23 * s23);
+                R t;
+                t = ps11[i] + s11; si += t * t / R(4);
+                t = ps22[i] + s22; si += t * t / R(4);
+                t = ps33[i] + s33; si += t * t / R(4);
+                t = ps12[i] + s12; si += R(2) * (t * t) / R(4);
+                const R l2 = (R)lim[j - 1];
+                const R evi = sqrt(R(2) * si) * l2;
+                sg13 = R(-2) * evi * s13;
+                sg23 = R(-2) * evi * s23;
+            }
+            R o[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) o[q] = 0;
+            R sg33 = 0;
+            if (j >= 1) {
+                // (c) C layer c = j-1
+                R scc = psc[i];
+                // S13 (:232-233); dynamic values are not interpolated (:245-249)
+                if (c == 0) {
+                    if (a.dyn_lo) { const R d = pu[i] * fs_lo; scc += R(2) * (d * d); }
+                    else { const R d = R(0) + s13; scc += R(2) * (d * d) / R(4); }
+                } else if (c == n3 - 1) {
+                    if (a.dyn_hi) { const R d = pu[i] * fs_hi; scc += R(2) * (d * d); }
+                    else { const R d = s13pp[i] + R(0); scc += R(2) * (d * d) / R(4); }
+                } else {
+                    const R d = s13pp[i] + s13; scc += R(2) * (d * d) / R(4);
+                }
+                if (c == 0) {
+                    if (a.dyn_lo) { const R d = pv[i] * fs_lo; scc += R(2) * (d * d); }
+                    else { const R d = R(0) + s23; scc += R(2) * (d * d) / R(4); }
+                } else if (c == n3 - 1) {
+                    if (a.dyn_hi) { const R d = pv[i] * fs_hi; scc += R(2) * (d * d); }
+                    else { const R d = s23pp[i] + R(0); scc += R(2) * (d * d) / R(4); }
+                } else {
+                    const R d = s23pp[i] + s23; scc += R(2) * (d * d) / R(4);
+                }
+                const R evc = sqrt(R(2) * scc) * (R)lcm[c];
+                o[0] = -(R(-2) * evc * ps11[i]);
+                o[2] = -(R(-2) * evc * ps22[i]);
+                sg33 = R(-2) * evc * ps33[i];
+                o[1] = -(R(-2) * evc * ps12[i]);
+                // wall stress (stress_bc, :195-200) from the wall-adjacent C layer
+                const R uh = sqrt(pu[i] * pu[i] + pv[i] * pv[i]);
+                const R b13lo = a.dyn_lo ? ft_lo * pu[i] * uh : R(0);
+                const R b23lo = a.dyn_lo ? ft_lo * pv[i] * uh : R(0);
+                const R b13hi = a.dyn_hi ? ft_hi * pu[i] * uh : R(0);
+                const R b23hi = a.dyn_hi ? ft_hi * pv[i] * uh : R(0);
+                const R below13 = (c == 0) ? b13lo : t13pp[i];
+                const R below23 = (c == 0) ? b23lo : t23pp[i];
+                const R above13 = (c == n3 - 1) ? b13hi : sg13;
+                const R above23 = (c == n3 - 1) ? b23hi : sg23;
+                const R ac = (R)a.alpha_c[c];
+                o[3] = -(-ac * below13 + ac * above13);
+                o[4] = -(-ac * below23 + ac * above23);
+                if (c >= 1) {  // d3 tau33 on I layer c-1 (dx3_c2i!, :363)
+                    const R ai = (R)a.alpha_i[c - 1];
+                    o[5] = -(-ai * t33pp[i] + ai * sg33);
+                }
+                o[6] = -sg13;
+                o[7] = -sg23;
+            }
+            if (doC || do5) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) outb[(yl * 4 + q) * P1 + x] = mk<R>(o[2 * q], o[2 * q + 1]);
+            }
+            // (d) carry
+            if (j >= 1 && j <= n3 - 1) {
+                s13pp[i] = s13;
+                s23pp[i] = s23;
+                t13pp[i] = sg13;
+                t23pp[i] = sg23;
+            }
+            if (j >= 1) t33pp[i] = sg33;
+            if (hasC) {
+                ps11[i] = s11; ps22[i] = s22; ps33[i] = s33; ps12[i] = s12; psc[i] = sc;
+                pu[i] = u; pv[i] = v; pw[i] = w; pw1[i] = w1; pw2[i] = w2;
+            }
+        }
+        if (doC || do5) {
+            __syncthreads();
+            C* r2 = fft_run<R, -1>(outb, scr, NLout, P1, 1, true, a.plan, tw);
+            const int nk = k1max + 1;
+            for (int i = threadIdx.x; i < NLout * nk; i += nthr) {
+                const int line = i / nk, k = i - line * nk;
+                const int yl = line / 4, q = line - yl * 4, y = y0 + yl;
+                C A, B;
+                unpack_pair<R>(r2 + line * P1, k, P1, A, B);
+                // pairs (0,1) (2,3) (4,5) (6,7)
+                const int ta = 2 * q, tb = 2 * q + 1;
+                if (ta <= 4) {
+                    if (doC) mrow_w(Mout, a, ta, c, y)[k] = A;
+                } else if (do67) {
+                    mrow_w(Mout, a, ta, c, y)[k] = A;
+                }
+                if (tb <= 4) {
+                    if (doC) mrow_w(Mout, a, tb, c, y)[k] = B;
+                } else if (tb == 5) {
+                    if (do5) mrow_w(Mout, a, 5, j - 2, y)[k] = B;
+                } else if (do67) {
+                    mrow_w(Mout, a, tb, c, y)[k] = B;
+                }
+            }
+            if (r2 != outb) {
+                scr = outb;
+                outb = r2;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ forward y pass
+struct FwdContrib {
+    int term;  // mixed output term index
+    int pref;  // 0 none, 1 D1, 2 D2
+};
+
+struct Linear {
+    int diff_on[3];
+    double nu[3];
+    const double* DD1;        // [K1]
+    const double* DD2;        // [K2]
+    const double* alpha_c;    // [n3]
+    const double* alpha_i;    // [n3-1]
+    const double* alpha_ext;  // [n3+1] alpha at I positions incl. boundaries
+    int bc_kind[3][2];
+    double bc_val[3][2];      // Dirichlet value
+    double bc_diff[3][2];     // Neumann gradient * dx3 (ConstantGradient.difference)
+    int src_on[3];
+    const double* src;        // [members][3]
+};
+
+struct FwdYArgs {
+    Geo g;
+    int P1, P2;
+    const void* mout;
+    long long mout_mstride;
+    int ncontrib[3];
+    FwdContrib c[3][BLD_MAXC];
+    int mode;                  // 0: du += acc; 1: du = linear + acc; 2: du = acc (transform only)
+    int check;                 // set *flag on a non-finite result
+    double2* du;               // member stride g.mstride
+    long long du_mstride;
+    const double2* state;
+    Linear lin;
+    const double* d1;
+    const double* d2;
+    double inv_n;              // 1/(P1*P2)
+    int* flag;
+    int fields;                // number of target fields (3 for rates, 1 for transforms)
+    int field0;                // first target field
+    int m0;                    // first member
+    FftPlan plan;
+    const void* tw;
+};
+
+// Frequency-domain Laplacian with ghost layers (src/processes/molecular_diffusion.jl:57-72,
+// src/boundary_conditions.jl:506-602) and the constant source (src/processes/sources.jl:30-35).
+__device__ __forceinline__ double2 linear_terms(const Geo& g, const Linear& L, const double2* __restrict__ S, int f,
+                                                int z, int j, int k1, int m) {
+    double2 val = make_double2(0.0, 0.0);
+    const long long mo = (long long)j * g.K1 + k1;
+    const bool mean_mode = (j == 0 && k1 == 0);
+    if (L.diff_on[f]) {
+        const double2* Sf = S + fld_off(g, f);
+        const int n = (f == 2) ? g.n3 - 1 : g.n3;
+        const double2 q0 = Sf[(long long)z * g.F + mo];
+        double2 qm, qp;
+        double A, B, Cc;
+        if (f != 2) {
+            A = L.alpha_ext[z];
+            B = L.alpha_c[z];
+            Cc = L.alpha_ext[z + 1];
+            if (z == 0) {
+                const double2 l1 = Sf[mo], l2 = Sf[g.F + mo], l3 = Sf[2LL * g.F + mo];
+                if (L.bc_kind[f][0] == 0) {
+                    qm.x = (-15.0 * l1.x + 5.0 * l2.x - l3.x) / 5.0;
+                    qm.y = (-15.0 * l1.y + 5.0 * l2.y - l3.y) / 5.0;
+                    if (mean_mode) qm.x += 16.0 * L.bc_val[f][0] / 5.0;
+                } else {
+                    qm.x = (21.0 * l1.x + 3.0 * l2.x - l3.x) / 23.0;
+                    qm.y = (21.0 * l1.y + 3.0 * l2.y - l3.y) / 23.0;
+                    if (mean_mode) qm.x -= 24.0 * L.bc_diff[f][0] / 23.0;
+                }
+            } else {
+                qm = Sf[(long long)(z - 1) * g.F + mo];
+            }
+            if (z == n - 1) {
+                const double2 l1 = Sf[(long long)(n - 1) * g.F + mo], l2 = Sf[(long long)(n - 2) * g.F + mo],
+                              l3 = Sf[(long long)(n - 3) * g.F + mo];
+                if (L.bc_kind[f][1] == 0) {
+                    qp.x = (-15.0 * l1.x + 5.0 * l2.x - l3.x) / 5.0;
+                    qp.y = (-15.0 * l1.y + 5.0 * l2.y - l3.y) / 5.0;
+                    if (mean_mode) qp.x += 16.0 * L.bc_val[f][1] / 5.0;
+                } else {
+                    qp.x = (21.0 * l1.x + 3.0 * l2.x - l3.x) / 23.0;
+                    qp.y = (21.0 * l1.y + 3.0 * l2.y - l3.y) / 23.0;
+                    if (mean_mode) qp.x -= 24.0 * (-L.bc_diff[f][1]) / 23.0;
+                }
+            } else {
+                qp = Sf[(long long)(z + 1) * g.F + mo];
+            }
+        } else {
+            A = L.alpha_c[z];
+            B = L.alpha_i[z];
+            Cc = L.alpha_c[z + 1];
+            // Dirichlet values enter every mode (src/boundary_conditions.jl:506-517)
+            qm = (z == 0) ? make_double2(L.bc_val[2][0], 0.0) : Sf[(long long)(z - 1) * g.F + mo];
+            qp = (z == n - 1) ? make_double2(L.bc_val[2][1], 0.0) : Sf[(long long)(z + 1) * g.F + mo];
+        }
+        const double ab = A * B, bc = B * Cc;
+        const double coef = ((L.DD1[k1] + L.DD2[j]) - ab) - bc;
+        const double nu = L.nu[f];
+        val.x = nu * ((ab * qm.x + coef * q0.x) + bc * qp.x);
+        val.y = nu * ((ab * qm.y + coef * q0.y) + bc * qp.y);
+    }
+    if (L.src_on[f] && mean_mode) val.x += L.src[3 * m + f];
+    return val;
+}
+
+// grid (ceil(K1/NL), n3, fields*members); smem tw[P2] + 2*P2*NL complex
+template <typename R, int NL, int MAXO>
+__global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* b0 = tw + a.P2;
+    C* b1 = b0 + a.P2 * NL;
+    const int fi = blockIdx.z % a.fields, m = a.m0 + blockIdx.z / a.fields;
+    const int f = a.field0 + fi;
+    const int z = blockIdx.y;
+    const Geo& g = a.g;
+    const int nz = (f == 2) ? g.n3 - 1 : g.n3;
+    if (z >= nz) return;
+    const int K1 = g.K1, K2 = g.K2, k2max = g.k2max, P2 = a.P2;
+    const int k10 = blockIdx.x * NL;
+    const C* twg = reinterpret_cast<const C*>(a.tw);
+    for (int i = threadIdx.x; i < P2; i += blockDim.x) tw[i] = twg[i];
+    double2 acc[MAXO];
+#pragma unroll
+    for (int r = 0; r < MAXO; ++r) acc[r] = make_double2(0.0, 0.0);
+    const int nout = K2 * NL;
+    const int nc = a.ncontrib[fi];
+    for (int ci = 0; ci < nc; ++ci) {
+        const FwdContrib cb = a.c[fi][ci];
+        const C* src = reinterpret_cast<const C*>(a.mout) + (long long)m * a.mout_mstride +
+                       (long long)(cb.term * g.n3 + z) * P2 * K1;
+        for (int i = threadIdx.x; i < P2 * NL; i += blockDim.x) {
+            const int y = i / NL, l = i - y * NL, k1 = k10 + l;
+            b0[i] = (k1 < K1) ? src[(long long)y * K1 + k1] : mk<R>(0, 0);
+        }
+        __syncthreads();
+        const C* res = fft_run<R, -1>(b0, b1, NL, 1, NL, false, a.plan, tw);
+#pragma unroll
+        for (int r = 0; r < MAXO; ++r) {
+            const int o = threadIdx.x + r * blockDim.x;
+            if (o < nout) {
+                const int j = o / NL, l = o - j * NL;
+                const int pos = (j <= k2max) ? j : P2 - (K2 - j);
+                const C X = res[pos * NL + l];
+                double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
+                if (cb.pref == 1) {
+                    const int k1 = min(k10 + l, K1 - 1);
+                    const double d = a.d1[k1];
+                    const double tx = -d * vy;
+                    vy = d * vx;
+                    vx = tx;
+                } else if (cb.pref == 2) {
+                    const double d = a.d2[j];
+                    const double tx = -d * vy;
+                    vy = d * vx;
+                    vx = tx;
+                }
+                acc[r].x += vx;
+                acc[r].y += vy;
+            }
+        }
+        __syncthreads();
+    }
+    double2* du = a.du + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F;
+    const double2* S = a.state ? a.state + (long long)m * g.mstride : nullptr;
+    bool bad = false;
+#pragma unroll
+    for (int r = 0; r < MAXO; ++r) {
+        const int o = threadIdx.x + r * blockDim.x;
+        if (o < nout) {
+            const int j = o / NL, l = o - j * NL, k1 = k10 + l;
+            if (k1 < K1) {
+                const long long idx = (long long)j * K1 + k1;
+                double2 v;
+                if (a.mode == 1) {
+                    const double2 lin = linear_terms(g, a.lin, S, f, z, j, k1, m);
+                    v = make_double2(lin.x + acc[r].x, lin.y + acc[r].y);
+                } else if (a.mode == 2) {
+                    v = acc[r];
+                } else {
+                    const double2 o0 = du[idx];
+                    v = make_double2(o0.x + acc[r].x, o0.y + acc[r].y);
+                }
+                du[idx] = v;
+                if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
+            }
+        }
+    }
+    if (a.check && bad) atomicOr(a.flag, 1);
+}
+
+// Linear terms only (no physical-domain process): grid (ceil(F/256), n3, 3*members)
+__global__ void __launch_bounds__(256) k_linear(FwdYArgs a) {
+    const Geo& g = a.g;
+    const int f = blockIdx.z % 3, m = a.m0 + blockIdx.z / 3;
+    const int z = blockIdx.y;
+    const int nz = (f == 2) ? g.n3 - 1 : g.n3;
+    const int mo = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z >= nz || mo >= g.F) return;
+    const int j = mo / g.K1, k1 = mo - j * g.K1;
+    const double2* S = a.state + (long long)m * g.mstride;
+    const double2 v = linear_terms(g, a.lin, S, f, z, j, k1, m);
+    a.du[(long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F + mo] = v;
+    if (a.check && !(isfinite(v.x) && isfinite(v.y))) atomicOr(a.flag, 1);
+}
+
+// --------------------------------------------------- stage update + projection
+enum StageKind {
+    S_NONE = 0,     // out = u (projection only)
+    S_EULER = 1,    // u + dt du                       (src/ODEMethods.jl:101,137,150)
+    S_RK22_2 = 2,   // (u + t + dt du) / 2             (:143)
+    S_RK33_2 = 3,   // (3u + t + dt du) / 4            (:157)
+    S_RK33_3 = 4,   // (u + 2t + 2 dt du) / 3          (:164)
+    S_AB2_1 = 5,    // u + dt (du - dp) / 2            (:120)
+    S_AB2 = 6       // u + dt/2 (3 du - dp)            (:127)
+};
+
+struct ProjArgs {
+    Geo g;
+    int m0;
+    const double2* u;
+    const double2* t;
+    const double2* du;
+    const double2* dp;
+    double2* out;
+    int kind;
+    double dt;
+    int pressure;
+    double2* pscr;           // [members][n3][F] forward-sweep scratch
+    const double* gamma;     // [n3][F]
+    const double* alpha_c;   // [n3]
+    const double* alpha_i;   // [n3-1]  (off-diagonal beta)
+    const double* d1;
+    const double* d2;
+    double w_lo, w_hi;
+    int mean_on[3];
+    const double* mean_w;    // [n3] weights (dx3/dzeta)/(n3 L3)
+    const double* mean_val;  // [members][3]
+};
+
+__device__ __forceinline__ double2 stage_value(const ProjArgs& a, long long idx) {
+    const double2 u = a.u[idx];
+    const double dt = a.dt;
+    switch (a.kind) {
+        case S_NONE:
+            return u;
+        case S_EULER: {
+            const double2 d = a.du[idx];
+            return make_double2(u.x + dt * d.x, u.y + dt * d.y);
+        }
+        case S_RK22_2: {
+            const double2 t = a.t[idx], d = a.du[idx];
+            return make_double2((u.x + t.x + dt * d.x) / 2.0, (u.y + t.y + dt * d.y) / 2.0);
+        }
+        case S_RK33_2: {
+            const double2 t = a.t[idx], d = a.du[idx];
+            return make_double2((3.0 * u.x + t.x + dt * d.x) / 4.0, (3.0 * u.y + t.y + dt * d.y) / 4.0);
+        }
+        case S_RK33_3: {
+            const double2 t = a.t[idx], d = a.du[idx];
+            const double dt2 = 2.0 * dt;
+            return make_double2((u.x + 2.0 * t.x + dt2 * d.x) / 3.0, (u.y + 2.0 * t.y + dt2 * d.y) / 3.0);
+        }
+        case S_AB2_1: {
+            const double2 d = a.du[idx], p = a.dp[idx];
+            return make_double2(u.x + dt * (d.x - p.x) / 2.0, u.y + dt * (d.y - p.y) / 2.0);
+        }
+        default: {  // S_AB2
+            const double2 d = a.du[idx], p = a.dp[idx];
+            const double h = dt / 2.0;
+            return make_double2(u.x + h * (3.0 * d.x - p.x), u.y + h * (3.0 * d.y - p.y));
+        }
+    }
+}
+
+// One thread per (k1, k2) column: stage update, divergence (div!, src/processes/pressure.jl:368-378),
+// forward/backward Thomas (:106-165), gradient (add_gradient!, :405-426), then ConstantMean
+// (src/processes/sources.jl:69-77) on the (0,0) column.  grid (ceil(F/128), members)
+__global__ void __launch_bounds__(128) k_project(ProjArgs a) {
+    const Geo& g = a.g;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = a.m0 + blockIdx.y;
+    if (c >= g.F) return;
+    const long long mb = (long long)m * g.mstride;
+    const long long F = g.F;
+    const int n = g.n3;
+    const long long o1 = mb, o2 = mb + (long long)n * F, o3 = mb + 2LL * n * F;
+    if (a.pressure) {
+        const int j = c / g.K1, k1 = c - j * g.K1;
+        const bool mean_mode = (c == 0);
+        const double e1 = a.d1[k1], e2 = a.d2[j];
+        double2* P = a.pscr + (long long)m * n * F + c;
+        double2 wprev = make_double2(0.0, 0.0);
+        double2 b = make_double2(0.0, 0.0);
+        for (int z = 0; z < n; ++z) {
+            const double2 uz = stage_value(a, o1 + z * F + c);
+            const double2 vz = stage_value(a, o2 + z * F + c);
+            a.out[o1 + z * F + c] = uz;
+            a.out[o2 + z * F + c] = vz;
+            double2 wz = make_double2(0.0, 0.0);
+            if (z < n - 1) {
+                wz = stage_value(a, o3 + z * F + c);
+                a.out[o3 + z * F + c] = wz;
+            }
+            const double h = 1.0 / a.alpha_c[z];
+            double2 val;
+            val.x = (-e1 * uz.y) * h + (-e2 * vz.y) * h;
+            val.y = (e1 * uz.x) * h + (e2 * vz.x) * h;
+            if (z == 0) {
+                val.x += wz.x;
+                val.y += wz.y;
+                if (mean_mode) val.x -= a.w_lo;
+            } else if (z == n - 1) {
+                val.x -= wprev.x;
+                val.y -= wprev.y;
+                if (mean_mode) val.x += a.w_hi;
+            } else {
+                val.x = val.x - wprev.x + wz.x;
+                val.y = val.y - wprev.y + wz.y;
+            }
+            if (mean_mode && z == n - 1) val = make_double2(0.0, 0.0);  // adjust_pressure_rhs! (:396)
+            const double gm = a.gamma[(long long)z * F + c];
+            if (z == 0) {
+                b = make_double2(gm * val.x, gm * val.y);
+            } else {
+                const double be = a.alpha_i[z - 1];
+                b = make_double2(gm * (val.x - be * b.x), gm * (val.y - be * b.y));
+            }
+            P[(long long)z * F] = b;
+            wprev = wz;
+        }
+        // backward sweep and gradient, top to bottom
+        double2 pn = b;  // p at z = n-1
+        {
+            const int z = n - 1;
+            double2 u = a.out[o1 + z * F + c], v = a.out[o2 + z * F + c];
+            u.x += e1 * pn.y; u.y += -e1 * pn.x;
+            v.x += e2 * pn.y; v.y += -e2 * pn.x;
+            a.out[o1 + z * F + c] = u;
+            a.out[o2 + z * F + c] = v;
+        }
+        for (int z = n - 2; z >= 0; --z) {
+            const double2 bz = P[(long long)z * F];
+            const double gb = a.gamma[(long long)z * F + c] * a.alpha_i[z];
+            const double2 pz = make_double2(bz.x - gb * pn.x, bz.y - gb * pn.y);
+            double2 u = a.out[o1 + z * F + c], v = a.out[o2 + z * F + c], w = a.out[o3 + z * F + c];
+            u.x += e1 * pz.y; u.y += -e1 * pz.x;
+            v.x += e2 * pz.y; v.y += -e2 * pz.x;
+            const double ai = a.alpha_i[z];
+            w.x += -1.0 * (-ai * pz.x + ai * pn.x);
+            w.y += -1.0 * (-ai * pz.y + ai * pn.y);
+            a.out[o1 + z * F + c] = u;
+            a.out[o2 + z * F + c] = v;
+            a.out[o3 + z * F + c] = w;
+            pn = pz;
+        }
+    } else if (a.kind != S_NONE || a.out != a.u) {
+        for (int z = 0; z < n; ++z) {
+            a.out[o1 + z * F + c] = stage_value(a, o1 + z * F + c);
+            a.out[o2 + z * F + c] = stage_value(a, o2 + z * F + c);
+            if (z < n - 1) a.out[o3 + z * F + c] = stage_value(a, o3 + z * F + c);
+        }
+    }
+    if (c == 0) {
+        for (int f = 0; f < 2; ++f) {
+            if (!a.mean_on[f]) continue;
+            const long long of = (f == 0) ? o1 : o2;
+            double s = 0.0;
+            for (int z = 0; z < n; ++z) s += a.out[of + z * F].x * a.mean_w[z];
+            const double add = a.mean_val[3 * m + f] - s;
+            for (int z = 0; z < n; ++z) a.out[of + z * F].x += add;
+        }
+    }
+}
+
+// Standalone batched LDL^T solve, one thread per system (ldiv!, src/processes/pressure.jl:167-201)
+__global__ void __launch_bounds__(128) k_ldlt_solve(const double* __restrict__ gamma, const double* __restrict__ beta,
+                                                    double2* rhs, long long nsys, int n) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nsys) return;
+    double2 b = rhs[c];
+    double gm = gamma[c];
+    b.x *= gm;
+    b.y *= gm;
+    rhs[c] = b;
+    for (int z = 1; z < n; ++z) {
+        const long long idx = (long long)z * nsys + c;
+        const double2 r = rhs[idx];
+        const double be = beta[z - 1];
+        gm = gamma[idx];
+        b = make_double2(gm * (r.x - be * b.x), gm * (r.y - be * b.y));
+        rhs[idx] = b;
+    }
+    for (int z = n - 2; z >= 0; --z) {
+        const long long idx = (long long)z * nsys + c;
+        const double2 r = rhs[idx];
+        const double gb = gamma[idx] * beta[z];
+        b = make_double2(r.x - gb * b.x, r.y - gb * b.y);
+        rhs[idx] = b;
+    }
+}
+
+// ------------------------------------------- plain x transforms (initialize!/getindex)
+struct XPlainArgs {
+    int P1, P2, K1, k1max, nz;
+    const double* pd;     // [nz][P2][P1]
+    double* pd_out;
+    const double2* mixed_in;  // [nz][P2][K1]
+    double2* mixed_out;
+    FftPlan plan;
+    const double2* tw;
+};
+
+// r2c along x of two physical rows per block -> mixed rows; grid ceil(nz*P2/2)
+__global__ void __launch_bounds__(256) k_x_r2c(XPlainArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* tw = reinterpret_cast<double2*>(smem_raw);
+    double2* b0 = tw + a.P1;
+    double2* b1 = b0 + a.P1;
+    const long long rows = (long long)a.nz * a.P2;
+    const long long r0 = 2LL * blockIdx.x, r1 = r0 + 1;
+    for (int i = threadIdx.x; i < a.P1; i += blockDim.x) tw[i] = a.tw[i];
+    for (int x = threadIdx.x; x < a.P1; x += blockDim.x) {
+        const double va = a.pd[r0 * a.P1 + x];
+        const double vb = (r1 < rows) ? a.pd[r1 * a.P1 + x] : 0.0;
+        b0[x] = make_double2(va, vb);
+    }
+    __syncthreads();
+    double2* res = fft_run<double, -1>(b0, b1, 1, a.P1, 1, true, a.plan, tw);
+    for (int k = threadIdx.x; k <= a.k1max; k += blockDim.x) {
+        double2 A, B;
+        unpack_pair<double>(res, k, a.P1, A, B);
+        a.mixed_out[r0 * a.K1 + k] = A;
+        if (r1 < rows) a.mixed_out[r1 * a.K1 + k] = B;
+    }
+}
+
+// c2r along x of two mixed rows per block -> physical rows; grid ceil(nz*P2/2)
+__global__ void __launch_bounds__(256) k_x_c2r(XPlainArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* tw = reinterpret_cast<double2*>(smem_raw);
+    double2* b0 = tw + a.P1;
+    double2* b1 = b0 + a.P1;
+    const long long rows = (long long)a.nz * a.P2;
+    const long long r0 = 2LL * blockIdx.x, r1 = r0 + 1;
+    for (int i = threadIdx.x; i < a.P1; i += blockDim.x) tw[i] = a.tw[i];
+    for (int k = threadIdx.x; k < a.P1; k += blockDim.x) {
+        if (k > a.k1max && k < a.P1 - a.k1max) b0[k] = make_double2(0.0, 0.0);
+        if (k <= a.k1max)
+            build_packed<double>(b0, a.mixed_in + r0 * a.K1, (r1 < rows) ? a.mixed_in + r1 * a.K1 : nullptr, k, a.P1);
+    }
+    __syncthreads();
+    double2* res = fft_run<double, +1>(b0, b1, 1, a.P1, 1, true, a.plan, tw);
+    for (int x = threadIdx.x; x < a.P1; x += blockDim.x) {
+        a.pd_out[r0 * a.P1 + x] = res[x].x;
+        if (r1 < rows) a.pd_out[r1 * a.P1 + x] = res[x].y;
+    }
+}

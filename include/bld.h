@@ -1,0 +1,210 @@
+/*
+ * bld.h -- C ABI of the B200-native time-step engine for BoundaryLayerDynamics.jl.
+ *
+ * The engine replaces the reference's per-stage Julia closures
+ *   rate!(du, u, t)        -> compute_rates!   (src/BoundaryLayerDynamics.jl:149-158,
+ *                                               src/Processes.jl:39-62)
+ *   projection!(u)         -> apply_projections! (src/BoundaryLayerDynamics.jl:161-165,
+ *                                               src/Processes.jl:67-75)
+ *   perform_step!/step_to! -> the explicit integrators (src/ODEMethods.jl:100-166,217-234)
+ * with hand-written sm_100a kernels.  All entry points are plain C: pointers,
+ * sizes and POD structs, no exceptions; every function returns a bld_status.
+ *
+ * Field layout (host and device): a spectral field is interleaved complex
+ * double, column-major (k1, k2, z) exactly like the reference's
+ * Array{Complex{Float64},3} of size (k1max+1, 2*k2max+1, n3) with k2 ordered
+ * 0..k2max, -k2max..-1 (src/Grids.jl:74-83,91-93).  vel1 and vel2 live on the
+ * n3 C nodes, vel3 on the n3-1 I nodes (src/Grids.jl:97-99).
+ */
+#ifndef BLD_H
+#define BLD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BLD_ABI_VERSION 1
+
+/* status codes (no exception crosses the ABI) */
+typedef enum {
+    BLD_OK = 0,
+    BLD_ERR_INVALID_CONFIG = -1,  /* bad sizes / unsupported physical-domain size          */
+    BLD_ERR_OUT_OF_MEMORY = -2,   /* cudaMalloc failed                                       */
+    BLD_ERR_DIVERGED = -3,        /* a rate was not finite: "The simulation has diverged."
+                                     (src/BoundaryLayerDynamics.jl:155-157)                  */
+    BLD_ERR_UNSUPPORTED_BC = -4,  /* pressure needs Dirichlet w with equal values
+                                     (src/processes/pressure.jl:338-339,357); advection
+                                     needs w = 0 (src/processes/momentum_advection.jl:182);
+                                     SGS needs rough-wall / free-slip walls
+                                     (src/processes/static_smagorinsky.jl:298-304)           */
+    BLD_ERR_CUDA = -5,            /* a CUDA runtime call failed (see bld_last_error)         */
+    BLD_ERR_TIMEOUT = -6,         /* a bounded device wait expired                           */
+    BLD_ERR_ARGUMENT = -7,        /* null pointer / out-of-range argument                    */
+    BLD_ERR_NO_DEVICE = -8        /* no CUDA device or the library was not built for it      */
+} bld_status;
+
+typedef enum { BLD_BC_DIRICHLET = 0, BLD_BC_NEUMANN = 1 } bld_bc_kind;
+
+/* wall types used by the SGS wall model (src/Domains.jl:322-343) */
+typedef enum { BLD_WALL_OTHER = 0, BLD_WALL_ROUGH = 1, BLD_WALL_FREESLIP = 2 } bld_wall_kind;
+
+typedef enum { BLD_FP64 = 0, BLD_MIXED = 1 } bld_precision;
+
+/* src/ODEMethods.jl:21-50 */
+typedef enum { BLD_EULER = 0, BLD_AB2 = 1, BLD_SSPRK22 = 2, BLD_SSPRK33 = 3 } bld_method;
+
+/* dealiasing modes of MomentumAdvection / StaticSmagorinskyModel (src/physical_space.jl:42-56) */
+typedef enum { BLD_DEALIAS_NONE = 0, BLD_DEALIAS_QUADRATIC = 1, BLD_DEALIAS_EXPLICIT = 2 } bld_dealias;
+
+/*
+ * Model description (Model(resolution, domain, processes), src/BoundaryLayerDynamics.jl:72-97).
+ * The vertical mapping is passed as tables the caller evaluates from its Domain
+ * (src/Domains.jl:240-278): dx3/dzeta at the C nodes and at the n3+1 I
+ * positions zeta = 0, 1/n3, ..., 1, and x3 at the C and interior I nodes.
+ * Arrays are copied by bld_create; the caller keeps ownership.
+ */
+typedef struct {
+    int32_t n1, n2, n3;            /* resolution (modes x1, modes x2, layers x3), n3 >= 3  */
+    int32_t members;               /* independent ensemble members of this size (>= 1)     */
+    double l1, l2;                 /* horizontal domain size                               */
+    double x3_min, x3_max;         /* vmap(0), vmap(1)                                     */
+    const double* dx3_c;           /* [n3]    Dvmap at C nodes                             */
+    const double* dx3_i;           /* [n3+1]  Dvmap at I positions incl. both boundaries   */
+    const double* x3_c;            /* [n3]    vmap at C nodes                              */
+    const double* x3_i;            /* [n3-1]  vmap at interior I nodes                     */
+    /* boundary conditions per field (vel1, vel2, vel3) and side (lower, upper);
+       for Neumann the value is the gradient d/dx3 (src/boundary_conditions.jl:296-302) */
+    int32_t bc_kind[3][2];
+    double bc_value[3][2];
+    int32_t wall_kind[2];          /* lower/upper wall type for the SGS wall model         */
+    double wall_z0[2];             /* roughness length (RoughWall)                         */
+    double wall_kappa[2];          /* von Karman constant (RoughWall)                      */
+    /* processes */
+    int32_t advection;             /* MomentumAdvection present                            */
+    int32_t adv_dealias;           /* bld_dealias                                          */
+    int32_t adv_p1, adv_p2;        /* explicit physical size when adv_dealias==EXPLICIT    */
+    int32_t diffusion[3];          /* MolecularDiffusion(vel_i, nu_i) present              */
+    double diffusivity[3];
+    int32_t pressure;              /* Pressure()                                           */
+    int32_t source[3];             /* ConstantSource(vel_i, S_i) present                   */
+    double source_strength[3];
+    int32_t mean[3];               /* ConstantMean(vel_i, Q_i) present (C-node fields)     */
+    double mean_value[3];
+    int32_t sgs;                   /* StaticSmagorinskyModel present                       */
+    int32_t sgs_dealias;           /* bld_dealias                                          */
+    int32_t sgs_p1, sgs_p2;
+    double sgs_cs;                 /* Cs                                                   */
+    int32_t sgs_wall_damping;      /* wall_damping                                         */
+    double sgs_wall_damping_exponent;
+    int32_t precision;             /* bld_precision                                        */
+    int32_t device;                /* CUDA device ordinal                                  */
+    /* optional per-member overrides (arrays of length `members`, or NULL) */
+    const double* member_cs;           /* Cs of each member                                */
+    const double* member_z0_lower;     /* roughness length of the lower rough wall         */
+    const double* member_source1;      /* ConstantSource strength for vel1                 */
+} bld_config;
+
+typedef struct {
+    int32_t k1max, k2max, n3, members;
+    int64_t modes_per_layer;       /* (k1max+1)*(2*k2max+1)                                */
+    int64_t state_doubles;         /* doubles of one member's (vel1, vel2, vel3) state     */
+    int32_t adv_p1, adv_p2;        /* physical size the kernels use for advection (0: off) */
+    int32_t adv_ref_p1, adv_ref_p2;/* the reference's pdsize for the same process          */
+    int32_t sgs_p1, sgs_p2;        /* physical size used by the SGS kernels (0: off)       */
+    int64_t device_bytes;          /* device memory held by the handle                     */
+    int32_t precision;
+} bld_info;
+
+typedef struct bld_handle bld_handle;
+
+/* library */
+int32_t bld_abi_version(void);
+const char* bld_status_string(int32_t status);
+/* copies the last error message of the calling thread into buf (NUL-terminated) */
+int32_t bld_last_error(char* buf, size_t len);
+
+/* Model(resolution, domain, processes) (src/BoundaryLayerDynamics.jl:79-96):
+   validates the process set, factorises the pressure matrices
+   (src/processes/pressure.jl:231-264) and allocates all device buffers. */
+int32_t bld_create(const bld_config* cfg, bld_handle** out);
+void bld_destroy(bld_handle* h);
+int32_t bld_get_info(const bld_handle* h, bld_info* info);
+
+/* model.state <-> host arrays (interleaved complex, reference layout), one member */
+int32_t bld_set_state(bld_handle* h, int32_t member, const double* vel1, const double* vel2, const double* vel3);
+int32_t bld_get_state(bld_handle* h, int32_t member, double* vel1, double* vel2, double* vel3);
+
+/* compute_rates!(rates, state, t, processes, ...) + the isfinite scan of rate!
+   on host arrays of one member (src/Processes.jl:39-62, src/BoundaryLayerDynamics.jl:149-158).
+   Returns BLD_ERR_DIVERGED if any rate is not finite (the rates are still written). */
+int32_t bld_compute_rates(bld_handle* h, int32_t member,
+                          const double* vel1, const double* vel2, const double* vel3,
+                          double* rate1, double* rate2, double* rate3);
+
+/* apply_projections!(state, processes) in place on host arrays of one member
+   (src/Processes.jl:67-75: Pressure, then ConstantMean). */
+int32_t bld_apply_projections(bld_handle* h, int32_t member, double* vel1, double* vel2, double* vel3);
+
+/* evolve!(model, (t1, t2); dt, method) on the device-resident state of all members
+   (src/BoundaryLayerDynamics.jl:190-219): one projection and one rate evaluation,
+   then round((t2-t1)/dt) steps, each followed by a rate evaluation. */
+int32_t bld_evolve(bld_handle* h, double t1, double t2, double dt, int32_t method);
+
+/* The inner loop of evolve!: `nsteps` steps from the current state and slope,
+   replayed from a CUDA graph.  bld_evolve (or bld_prepare) must have run once. */
+int32_t bld_prepare(bld_handle* h);                       /* projection + rates  */
+int32_t bld_step(bld_handle* h, int64_t nsteps, double dt, int32_t method);
+
+/* Device-pointer variants, stream-ordered on `stream` (a cudaStream_t, or NULL for
+   the handle's stream).  Pointers address all members' fields packed as
+   [member][vel1 | vel2 | vel3].  They neither synchronise nor check divergence;
+   bld_sync reports a non-finite rate seen since the last check. */
+int32_t bld_compute_rates_device(bld_handle* h, const void* state, void* rates, void* stream);
+int32_t bld_apply_projections_device(bld_handle* h, void* state, void* stream);
+int32_t bld_state_device_ptr(bld_handle* h, void** state);
+int32_t bld_sync(bld_handle* h);
+
+/* The handle's CUDA stream (cudaStream_t) on which every launch of the handle is
+   ordered, so callers can record CUDA events around engine work. */
+int32_t bld_get_stream(bld_handle* h, void** stream);
+
+/* bld_step without the trailing synchronisation and divergence check: enqueues
+   `nsteps` graph launches and returns; bld_sync reports the outcome. */
+int32_t bld_step_async(bld_handle* h, int64_t nsteps, double dt, int32_t method);
+
+/* Average device time of each launch kind of one right-hand side, measured with
+   CUDA events on the handle's stream over `iters` back-to-back launches of that
+   kind on the resident state (index 0: advection space, 1: SGS space). */
+typedef struct {
+    double inv_y_ms[2];            /* inverse y pass                              */
+    double x_ms[2];                /* x transforms + physical-domain products     */
+    double fwd_y_ms[2];            /* forward y pass + linear terms               */
+    double project_ms;             /* stage update + pressure projection          */
+    double linear_ms;              /* linear-only rates (no nonlinear process)    */
+    int32_t launches_per_step;     /* kernel launches of one step of the method   */
+} bld_phase_times;
+int32_t bld_time_phases(bld_handle* h, int32_t iters, int32_t method, bld_phase_times* out);
+
+/* Physical-domain fields at the default size (2*k1max+2, 2*k2max+2) of one member:
+   initialize!(model; vel = values) (src/State.jl:11-31, set_field! src/physical_space.jl:253-275)
+   and model[:vel] (src/State.jl:81-85, get_field src/physical_space.jl:315-319).
+   `values` is float64 (P1, P2, nz) column-major (x fastest). field: 0, 1, 2. */
+int32_t bld_set_field_physical(bld_handle* h, int32_t member, int32_t field, const double* values);
+int32_t bld_get_field_physical(bld_handle* h, int32_t member, int32_t field, double* values);
+
+/* Standalone batched symmetric tridiagonal solve (the kernel of
+   ldiv!(::DistributedBatchLDLt, b), src/processes/pressure.jl:106-201):
+   `nsys` systems of size `n`, factor `gamma` [n][nsys] and off-diagonal `beta`
+   [n-1] shared by all systems, complex right-hand sides `rhs` [n][nsys] solved in
+   place.  Device pointers, stream-ordered. */
+int32_t bld_ldlt_solve_device(const double* gamma, const double* beta, void* rhs,
+                              int64_t nsys, int32_t n, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BLD_H */
