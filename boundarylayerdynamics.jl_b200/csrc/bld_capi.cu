@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1265,3 +1266,66 @@ int32_t bld_ldlt_solve_device(const double* gamma, const double* beta, void* rhs
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- no-alloc projection
+// Scratch of bld_project_noalloc: one fixed array per device, looked up once per
+// device with cudaGetSymbolAddress (host code may not use the symbol as an address).
+static __device__ __align__(256) double2 g_noalloc_scratch[BLD_NOALLOC_MAX_VALUES];
+
+namespace {
+std::mutex g_noalloc_mutex;
+std::map<int, void*> g_noalloc_ptr;  // device ordinal -> device address of g_noalloc_scratch
+
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    auto it = g_noalloc_ptr.find(dev);
+    if (it == g_noalloc_ptr.end()) {
+        void* ptr = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        it = g_noalloc_ptr.emplace(dev, ptr).first;
+    }
+    *out = it->second;
+    return BLD_OK;
+}
+}  // namespace
+
+extern "C" int32_t bld_project_noalloc(int32_t k1max, int32_t k2max, int32_t n3, const double* gamma,
+                                       const double* alpha_c, const double* alpha_i, const double* d1,
+                                       const double* d2, double w_lo, double w_hi, void* state, void* stream) {
+    if (!gamma || !alpha_c || !alpha_i || !d1 || !d2 || !state) return fail(BLD_ERR_ARGUMENT, "null argument");
+    if (k1max < 0 || k2max < 0 || n3 < 3) return fail(BLD_ERR_INVALID_CONFIG, "invalid grid size");
+    const long long F = (long long)(k1max + 1) * (2 * k2max + 1);
+    if ((long long)n3 * F > (long long)BLD_NOALLOC_MAX_VALUES)
+        return fail(BLD_ERR_INVALID_CONFIG,
+                    "bld_project_noalloc: n3*(k1max+1)*(2*k2max+1) = %lld exceeds the fixed scratch of %d values",
+                    (long long)n3 * F, BLD_NOALLOC_MAX_VALUES);
+    void* scratch = nullptr;
+    BLD_TRY(noalloc_scratch(&scratch));
+    ProjArgs a{};
+    a.g.k1max = k1max;
+    a.g.k2max = k2max;
+    a.g.K1 = k1max + 1;
+    a.g.K2 = 2 * k2max + 1;
+    a.g.n3 = n3;
+    a.g.F = (int)F;
+    a.g.mstride = (long long)(3 * n3 - 1) * F;
+    a.m0 = 0;
+    a.u = (const double2*)state;
+    a.out = (double2*)state;
+    a.kind = S_NONE;
+    a.pressure = 1;
+    a.pscr = (double2*)scratch;
+    a.gamma = gamma;
+    a.alpha_c = alpha_c;
+    a.alpha_i = alpha_i;
+    a.d1 = d1;
+    a.d2 = d2;
+    a.w_lo = w_lo;
+    a.w_hi = w_hi;
+    dim3 grid((unsigned)((F + 127) / 128), 1);
+    k_project<<<grid, 128, 0, (cudaStream_t)stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}

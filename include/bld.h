@@ -203,6 +203,30 @@ int32_t bld_get_field_physical(bld_handle* h, int32_t member, int32_t field, dou
 int32_t bld_ldlt_solve_device(const double* gamma, const double* beta, void* rhs,
                               int64_t nsys, int32_t n, void* stream);
 
+/* Pressure projection that allocates nothing.  No counterpart in the reference:
+   it exists for callers that cannot call cudaMalloc -- code whose device memory
+   is owned by a host framework's pool (a Julia CuArray pool, an embedding
+   application with a fixed memory budget) and that must not have a library
+   allocate behind its back.  Such a caller passes every buffer: the velocity
+   fields `state` (device, vel1|vel2|vel3 in the reference layout, projected in
+   place) and the tables of the Pressure process on the device: `gamma` [n3][F]
+   (the LDL^T factor, DistributedBatchLDLt.γ transposed to z-major), `alpha_c`
+   [n3] and `alpha_i` [n3-1] (N3/(dx3/dzeta) at C and I nodes), `d1` [k1max+1]
+   and `d2` [2*k2max+1] (k*2pi/L).  The forward-sweep scratch of the solve lives
+   in one fixed device array inside the library of BLD_NOALLOC_MAX_VALUES
+   complex doubles (16 MiB), which every GPU that loads the library holds until
+   the process exits; n3 * (k1max+1) * (2*k2max+1) above that limit is rejected
+   with BLD_ERR_INVALID_CONFIG.  The first call on a device looks up the array's
+   device address and should come before any stream capture.  All calls share
+   the array: calls that overlap on the GPU (other streams, other threads) race,
+   so serialise them.  The solve writes every scratch value before reading it,
+   so no clearing is needed between calls. */
+#define BLD_NOALLOC_MAX_VALUES (1 << 20)
+int32_t bld_project_noalloc(int32_t k1max, int32_t k2max, int32_t n3,
+                            const double* gamma, const double* alpha_c, const double* alpha_i,
+                            const double* d1, const double* d2, double w_lo, double w_hi,
+                            void* state, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
