@@ -9,7 +9,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libbld.so")
+LIB_PATH = os.environ.get("BLD_LIBRARY") or os.path.join(os.path.dirname(HERE), "lib", "libbld.so")
 
 BLD_OK = 0
 BLD_ERR_INVALID_CONFIG = -1

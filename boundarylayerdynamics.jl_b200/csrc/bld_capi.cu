@@ -16,6 +16,9 @@
 #include "bld.h"
 #include "bld_kernels.cuh"
 
+double2 h_wtab64[BLD_WTAB_SIZE];
+float2 h_wtab32[BLD_WTAB_SIZE];
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -58,24 +61,41 @@ int next_even_smooth(int n) {
     return m;
 }
 
-FftPlan make_plan(int n) {
-    FftPlan p{};
-    p.n = n;
-    int m = n, s = 0;
-    while (m % 4 == 0) {
-        p.radix[s++] = 4;
-        m /= 4;
+// Fewest Stockham stages whose radices are register codelet sizes, then the
+// smallest largest radix (register pressure), capped at BLD_FP64_MAXR for double.
+FftPlan make_plan(int n, bool fp32 = false) {
+    static const int rads[] = {32, 24, 18, 16, 12, 9, 8, 6, 4, 3, 2};
+    const int cap = fp32 ? 32 : BLD_FP64_MAXR;
+    FftPlan best{};
+    best.n = n;
+    int best_st = 99, best_max = 99;
+    int seq[6];
+    // depth-first search over radix sequences (n <= 2048 needs at most 4 stages)
+    auto dfs = [&](auto&& self, int rem, int depth, int mx) -> void {
+        if (depth > 4 || depth > best_st) return;
+        if (rem == 1) {
+            if (depth < best_st || (depth == best_st && mx < best_max)) {
+                best_st = depth;
+                best_max = mx;
+                best.nst = depth;
+                for (int i = 0; i < depth; ++i) best.radix[i] = seq[i];
+            }
+            return;
+        }
+        for (int r : rads) {
+            if (r > cap || rem % r) continue;
+            seq[depth] = r;
+            self(self, rem / r, depth + 1, std::max(mx, r));
+        }
+    };
+    dfs(dfs, n, 0, 0);
+    if (best_st == 99) {  // cannot happen for 2^a 3^b, kept for safety: radix 2/3 chain
+        int m = n, s = 0;
+        while (m % 2 == 0) { best.radix[s++] = 2; m /= 2; }
+        while (m % 3 == 0) { best.radix[s++] = 3; m /= 3; }
+        best.nst = s;
     }
-    while (m % 2 == 0) {
-        p.radix[s++] = 2;
-        m /= 2;
-    }
-    while (m % 3 == 0) {
-        p.radix[s++] = 3;
-        m /= 3;
-    }
-    p.nst = s;
-    return p;
+    return best;
 }
 
 // quadratic-dealiasing size of the reference (src/physical_space.jl:49-56)
@@ -99,7 +119,7 @@ struct Space {
     void* mout = nullptr;
     long long min_ms = 0, mout_ms = 0;  // elements per member
     int YT = 1, PPT = 1, zchunk = 1, nchunks = 1;
-    int NLy = 8, MAXO = 8;
+    int NLy = 8, NLf = 8, fsets = 1;  // y-pass lines per block (inverse, forward), forward line sets
 };
 
 }  // namespace
@@ -187,80 +207,77 @@ const void* twp(const bld_handle* h, int n, bool fp32) {
 size_t csize(bool fp32) { return fp32 ? sizeof(float2) : sizeof(double2); }
 
 // y-pass lines per block: shared memory <= ~100 KB and outputs per thread <= 16
-void pick_y(const Geo& g, int P2, bool fp32, int& NL, int& MAXO) {
+// y-pass lines per block: the largest of 16 (single) / 8, 4, 2 whose two
+// shared line buffers (times `sets`) and twiddles stay within ~110 KB
+int pick_y(int P2, bool fp32, int sets) {
     const size_t cs = csize(fp32);
-    NL = fp32 ? 16 : 8;
-    while (NL > 2 && (size_t)(P2 + 2 * P2 * NL) * cs > 100 * 1024) NL /= 2;
-    while (g.K2 * NL > 256 * 16 && NL > 2) NL /= 2;
-    MAXO = (g.K2 * NL <= 256 * 8) ? 8 : 16;
+    int NL = fp32 ? 16 : 8;
+    while (NL > 2 && (size_t)(P2 + 2 * P2 * sets * NL) * cs > 110 * 1024) NL /= 2;
+    return NL;
 }
 
 // choose tiles for a physical-domain space
-void tile_space(const bld_handle* h, Space& s) {
-    const size_t cs = csize(h->fp32);
-    // y rows per block: largest of 4, 2, 1 dividing P2 with YT*P1 <= 512
+void tile_space(const bld_handle* h, Space& s, bool is_adv) {
+    // (y rows per block, points per thread): blocks of <= 256 threads near 96
+    // (advection, double) / 128 (SGS, double) / 192 (single) threads, so several
+    // blocks stay resident per SM despite the codelet registers; fewer points per
+    // thread (registers) and fewer rows (shared memory) break ties
+    const int target = h->fp32 ? 192 : (is_adv ? 96 : 128);
+    int best = 1 << 30;
     s.YT = 1;
-    for (int yt : {4, 2}) {
-        if (s.P2 % yt == 0 && yt * s.P1 <= 512) {
-            s.YT = yt;
-            break;
+    s.PPT = 0;
+    for (int yt : {1, 2, 4}) {
+        if (s.P2 % yt || yt * s.P1 > 1024) continue;
+        const int pts = yt * s.P1;
+        for (int ppt = 1; ppt <= 4; ++ppt) {
+            if (pts % ppt) continue;
+            const int thr = pts / ppt;
+            if (thr > 256) continue;
+            const int score = std::abs(thr - target) + 24 * (ppt - 1) + 8 * (yt - 1);
+            if (score < best) {
+                best = score;
+                s.YT = yt;
+                s.PPT = ppt;
+            }
         }
     }
-    s.PPT = (s.YT * s.P1 + 511) / 512;
-    while ((s.YT * s.P1) % s.PPT) ++s.PPT;
     const int n3 = h->g.n3;
     const long long blocks_per_chunk = (long long)(s.P2 / s.YT) * h->B;
-    int want = (int)std::max<long long>(1, (600 + blocks_per_chunk - 1) / blocks_per_chunk);
-    want = std::min(want, std::max(1, n3 / 4));
+    int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
+    want = std::min(want, std::max(1, n3 / 8));
     s.zchunk = (n3 + want - 1) / want;
     s.nchunks = (n3 + s.zchunk - 1) / s.zchunk;
-    pick_y(h->g, s.P2, h->fp32, s.NLy, s.MAXO);
-    (void)cs;
 }
 
 size_t smem_y(int P2, int NL, bool fp32) { return (size_t)(P2 + 2 * P2 * NL) * csize(fp32); }
-size_t smem_adv(const Space& s, bool fp32) {
-    const int nin = 3 * s.YT, nout = s.YT + (s.YT + 1) / 2;
-    return (size_t)(s.P1 + 3 * std::max(nin, nout) * s.P1) * csize(fp32);
-}
-size_t smem_sgs(const Space& s, bool fp32) { return (size_t)(s.P1 + 3 * 5 * s.YT * s.P1) * csize(fp32); }
+size_t smem_adv(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 3 * s.YT * s.P1) * csize(fp32); }
+size_t smem_sgs(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 5 * s.YT * s.P1) * csize(fp32); }
 
 // ------------------------------------------------------------------ kernel dispatch
+// threads of a y-pass block: enough for the widest FFT stage of `lines` lines
+int y_threads(const FftPlan& pl, int lines) {
+    int rmin = 64;
+    for (int i = 0; i < pl.nst; ++i) rmin = std::min(rmin, pl.radix[i]);
+    const int tasks = lines * pl.n / rmin;
+    return std::min(256, std::max(64, (tasks + 31) / 32 * 32));
+}
+
 template <typename R>
-int launch_inv_y(bld_handle* h, const Space& s, const InvYArgs& a, int nm) {
-    dim3 grid((h->g.K1 + s.NLy - 1) / s.NLy, h->g.n3, a.nterms * nm);
+int launch_inv_y(bld_handle* h, const Space& s, InvYArgs a, int nm) {
+    a.NL = s.NLy;
+    dim3 grid(a.nterms * nm, (h->g.K1 + s.NLy - 1) / s.NLy, h->g.n3);
     const size_t sm = smem_y(s.P2, s.NLy, sizeof(R) == 4);
-    switch (s.NLy) {
-        case 16: k_inv_y<R, 16><<<grid, 256, sm, h->stream>>>(a); break;
-        case 8: k_inv_y<R, 8><<<grid, 256, sm, h->stream>>>(a); break;
-        case 4: k_inv_y<R, 4><<<grid, 256, sm, h->stream>>>(a); break;
-        default: k_inv_y<R, 2><<<grid, 256, sm, h->stream>>>(a); break;
-    }
+    k_inv_y<R><<<grid, y_threads(a.plan, s.NLy), sm, h->stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
 }
 
 template <typename R>
-int launch_fwd_y(bld_handle* h, const Space& s, const FwdYArgs& a, int nm) {
-    dim3 grid((h->g.K1 + s.NLy - 1) / s.NLy, h->g.n3, a.fields * nm);
-    const size_t sm = smem_y(s.P2, s.NLy, sizeof(R) == 4);
-#define BLD_FWD(NL, MO) k_fwd_y<R, NL, MO><<<grid, 256, sm, h->stream>>>(a)
-    if (s.MAXO == 8) {
-        switch (s.NLy) {
-            case 16: BLD_FWD(16, 8); break;
-            case 8: BLD_FWD(8, 8); break;
-            case 4: BLD_FWD(4, 8); break;
-            default: BLD_FWD(2, 8); break;
-        }
-    } else {
-        switch (s.NLy) {
-            case 16: BLD_FWD(16, 16); break;
-            case 8: BLD_FWD(8, 16); break;
-            case 4: BLD_FWD(4, 16); break;
-            default: BLD_FWD(2, 16); break;
-        }
-    }
-#undef BLD_FWD
+int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
+    a.NL = s.NLf;
+    dim3 grid(a.fields * nm, (h->g.K1 + s.NLf - 1) / s.NLf, h->g.n3);
+    const size_t sm = smem_y(s.P2, s.fsets * s.NLf, sizeof(R) == 4);
+    k_fwd_y<R><<<grid, y_threads(a.plan, s.fsets * s.NLf), sm, h->stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
 }
@@ -298,19 +315,16 @@ int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
 template <typename R>
 int set_smem_limits_R() {
     const int lim = 200 * 1024;
-#define BLD_SET(K) CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, lim))
-    BLD_SET((k_inv_y<R, 16>));
-    BLD_SET((k_inv_y<R, 8>));
-    BLD_SET((k_inv_y<R, 4>));
-    BLD_SET((k_inv_y<R, 2>));
-    BLD_SET((k_fwd_y<R, 16, 8>));
-    BLD_SET((k_fwd_y<R, 8, 8>));
-    BLD_SET((k_fwd_y<R, 4, 8>));
-    BLD_SET((k_fwd_y<R, 2, 8>));
-    BLD_SET((k_fwd_y<R, 16, 16>));
-    BLD_SET((k_fwd_y<R, 8, 16>));
-    BLD_SET((k_fwd_y<R, 4, 16>));
-    BLD_SET((k_fwd_y<R, 2, 16>));
+    // large dynamic shared memory, and the largest shared-memory carveout so the
+    // per-SM block count is set by the kernel's real footprint
+#define BLD_SET(K)                                                                           \
+    do {                                                                                     \
+        CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)); \
+        CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributePreferredSharedMemoryCarveout,     \
+                                      cudaSharedmemCarveoutMaxShared));                      \
+    } while (0)
+    BLD_SET((k_inv_y<R>));
+    BLD_SET((k_fwd_y<R>));
     BLD_SET((k_adv_x<R, 1>));
     BLD_SET((k_adv_x<R, 2>));
     BLD_SET((k_adv_x<R, 3>));
@@ -323,7 +337,29 @@ int set_smem_limits_R() {
     return BLD_OK;
 }
 
+// codelet twiddles W_N^m for N in {6,8,9,12,16,18,24,32}, once per device
+int init_codelet_twiddles() {
+    static std::mutex mu;
+    static std::map<int, bool> done;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return BLD_OK;
+    const int sizes[] = {6, 8, 9, 12, 16, 18, 24, 32};
+    for (int N : sizes)
+        for (int m = 0; m < N; ++m) {
+            const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)N;
+            h_wtab64[woff(N) + m] = make_double2((double)cosl(a), (double)sinl(a));
+            h_wtab32[woff(N) + m] = make_float2((float)cosl(a), (float)sinl(a));
+        }
+    CUDA_TRY(cudaMemcpyToSymbol(c_wtab64, h_wtab64, sizeof(h_wtab64)));
+    CUDA_TRY(cudaMemcpyToSymbol(c_wtab32, h_wtab32, sizeof(h_wtab32)));
+    done[dev] = true;
+    return BLD_OK;
+}
+
 int set_smem_limits() {
+    BLD_TRY(init_codelet_twiddles());
     static int done = 0;
     if (done) return BLD_OK;
     BLD_TRY(set_smem_limits_R<double>());
@@ -525,8 +561,21 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
     a.mean_val = h->mean_val;
     const bool any_mean = h->cfg.mean[0] || h->cfg.mean[1];
     if (!a.pressure && !any_mean && kind == S_NONE && out == u) return BLD_OK;
-    dim3 grid((h->g.F + 127) / 128, nm);
-    k_project<<<grid, 128, 0, h->stream>>>(a);
+    const int n3 = h->g.n3;
+    if (a.pressure && n3 <= 256) {
+        // z-segmented solve: <= 16 segments of <= 8 (n3 <= 128) or <= 16 layers
+        const int lmax = n3 <= 128 ? 8 : 16;
+        const int ns = std::max(1, std::min(16, (n3 + lmax - 1) / lmax));
+        dim3 grid((h->g.F + 31) / 32, nm);
+        dim3 block(32, ns);
+        if (lmax == 8)
+            k_project_seg<8><<<grid, block, 0, h->stream>>>(a);
+        else
+            k_project_seg<16><<<grid, block, 0, h->stream>>>(a);
+    } else {
+        dim3 grid((h->g.F + 127) / 128, nm);
+        k_project<<<grid, 128, 0, h->stream>>>(a);
+    }
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
 }
@@ -639,14 +688,16 @@ int setup_space(bld_handle* h, Space& s, int dealias, int e1, int e2, bool is_ad
             return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size %d is not an even 2^a*3^b (kernels support radix 2/3 only)", P);
     if (s.P1 < 2 * k1 + 2 || s.P2 < 2 * k2 + 2)
         return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size (%d, %d) smaller than the resolved modes", s.P1, s.P2);
-    if (s.P1 > 2048 || s.P2 > 2048) return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size above 2048");
-    s.plan1 = make_plan(s.P1);
-    s.plan2 = make_plan(s.P2);
+    if (s.P1 > 1024 || s.P2 > 1024) return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size above 1024");
+    s.plan1 = make_plan(s.P1, h->fp32);
+    s.plan2 = make_plan(s.P2, h->fp32);
     BLD_TRY(twiddles(h, s.P1));
     BLD_TRY(twiddles(h, s.P2));
     s.ntin = is_adv ? 6 : 9;
     s.ntout = is_adv ? 3 : 8;
-    tile_space(h, s);
+    s.fsets = is_adv ? 1 : 2;
+    tile_space(h, s, is_adv);
+    if (!s.PPT) return fail(BLD_ERR_INVALID_CONFIG, "no thread tiling for physical size %d", s.P1);
     const size_t cs = csize(h->fp32);
     const long long layer = (long long)s.P2 * h->g.K1;
     s.min_ms = (long long)s.ntin * h->g.n3 * layer;
@@ -1185,7 +1236,8 @@ int32_t bld_set_field_physical(bld_handle* h, int32_t m, int32_t field, const do
     Space s{};
     s.P1 = P1;
     s.P2 = P2;
-    pick_y(g, P2, false, s.NLy, s.MAXO);
+    s.NLy = pick_y(P2, false, 1);
+    s.NLf = s.NLy;
     FwdYArgs fa{};
     fa.g = g;
     fa.P1 = P1;
@@ -1221,7 +1273,8 @@ int32_t bld_get_field_physical(bld_handle* h, int32_t m, int32_t field, double* 
     Space s{};
     s.P1 = P1;
     s.P2 = P2;
-    pick_y(g, P2, false, s.NLy, s.MAXO);
+    s.NLy = pick_y(P2, false, 1);
+    s.NLf = s.NLy;
     InvYArgs ia{};
     ia.g = g;
     ia.P2 = P2;

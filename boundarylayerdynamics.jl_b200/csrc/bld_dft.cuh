@@ -1,0 +1,234 @@
+// Register DFT codelets of size N in {2,3,4,6,8,9,12,16,18,24,32}.
+//
+// dft<R, N, DIR>(x) transforms x[0..N) in place (registers, compile-time
+// indices after unrolling): X[k] = sum_n x[n] exp(DIR * 2 pi i n k / N).
+// Composite sizes split N = Rr * M (Rr = 4, 2 or 3; decimation in time): M-point
+// DFTs of the Rr interleaved subsequences, twiddles W_N^(r k'), then Rr-point
+// DFTs.  The twiddles W_N^m of every codelet size live in one small table
+// (constant memory on the device, a host array in host builds) filled from
+// long-double cos/sin on the host.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bld_fft.cuh"
+
+#define BLD_WTAB_SIZE 125
+
+// largest codelet compiled for double precision (register budget); single
+// precision always has all sizes up to 32
+#ifndef BLD_FP64_MAXR
+#define BLD_FP64_MAXR 18
+#endif
+
+// offsets of W_N (m = 0..N-1) in the twiddle table
+__host__ __device__ constexpr int woff(int N) {
+    return N == 6 ? 0 : N == 8 ? 6 : N == 9 ? 14 : N == 12 ? 23 : N == 16 ? 35 : N == 18 ? 51 : N == 24 ? 69
+         : N == 32 ? 93 : -1;
+}
+__host__ __device__ constexpr bool codelet_size(int N) {
+    return N == 2 || N == 3 || N == 4 || N == 6 || N == 8 || N == 9 || N == 12 || N == 16 || N == 18 || N == 24 ||
+           N == 32;
+}
+
+#ifdef __CUDACC__
+__constant__ double2 c_wtab64[BLD_WTAB_SIZE];
+__constant__ float2 c_wtab32[BLD_WTAB_SIZE];
+#endif
+extern double2 h_wtab64[BLD_WTAB_SIZE];
+extern float2 h_wtab32[BLD_WTAB_SIZE];
+
+template <typename R> __host__ __device__ __forceinline__ cplx<R> wtab(int i);
+template <> __host__ __device__ __forceinline__ double2 wtab<double>(int i) {
+#ifdef __CUDA_ARCH__
+    return c_wtab64[i];
+#else
+    return h_wtab64[i];
+#endif
+}
+template <> __host__ __device__ __forceinline__ float2 wtab<float>(int i) {
+#ifdef __CUDA_ARCH__
+    return c_wtab32[i];
+#else
+    return h_wtab32[i];
+#endif
+}
+
+template <typename R> __host__ __device__ __forceinline__ R hsin60() { return R(0.86602540378443864676); }
+
+template <typename C>
+__host__ __device__ __forceinline__ C c_add(C a, C b) {
+    C r;
+    r.x = a.x + b.x;
+    r.y = a.y + b.y;
+    return r;
+}
+template <typename C>
+__host__ __device__ __forceinline__ C c_sub(C a, C b) {
+    C r;
+    r.x = a.x - b.x;
+    r.y = a.y - b.y;
+    return r;
+}
+// x * w for DIR < 0, x * conj(w) for DIR > 0
+template <int DIR, typename C>
+__host__ __device__ __forceinline__ C c_tw(C x, C w) {
+    C r;
+    if (DIR < 0) {
+        r.x = x.x * w.x - x.y * w.y;
+        r.y = x.x * w.y + x.y * w.x;
+    } else {
+        r.x = x.x * w.x + x.y * w.y;
+        r.y = x.y * w.x - x.x * w.y;
+    }
+    return r;
+}
+
+template <typename R, int N, int DIR>
+__host__ __device__ __forceinline__ void dft(cplx<R> (&x)[N]) {
+    using C = cplx<R>;
+    if constexpr (N == 1) {
+        return;
+    } else if constexpr (N == 2) {
+        const C a = x[0], b = x[1];
+        x[0] = c_add(a, b);
+        x[1] = c_sub(a, b);
+    } else if constexpr (N == 3) {
+        const C s = c_add(x[1], x[2]);
+        const C d = c_sub(x[1], x[2]);
+        C m = x[0];
+        m.x -= R(0.5) * s.x;
+        m.y -= R(0.5) * s.y;
+        C t;
+        t.x = -d.y * hsin60<R>();
+        t.y = d.x * hsin60<R>();
+        x[0] = c_add(x[0], s);
+        if (DIR < 0) {
+            x[1] = c_sub(m, t);
+            x[2] = c_add(m, t);
+        } else {
+            x[1] = c_add(m, t);
+            x[2] = c_sub(m, t);
+        }
+    } else if constexpr (N == 4) {
+        const C a0 = c_add(x[0], x[2]), a1 = c_sub(x[0], x[2]);
+        const C a2 = c_add(x[1], x[3]);
+        const C d = c_sub(x[1], x[3]);
+        C a3;
+        a3.x = -d.y;
+        a3.y = d.x;  // i (x1 - x3)
+        x[0] = c_add(a0, a2);
+        x[2] = c_sub(a0, a2);
+        if (DIR < 0) {
+            x[1] = c_sub(a1, a3);
+            x[3] = c_add(a1, a3);
+        } else {
+            x[1] = c_add(a1, a3);
+            x[3] = c_sub(a1, a3);
+        }
+    } else {
+        constexpr int Rr = (N % 4 == 0) ? 4 : (N % 2 == 0) ? 2 : 3;
+        constexpr int M = N / Rr;
+        C sub[Rr][M];
+#pragma unroll
+        for (int r = 0; r < Rr; ++r)
+#pragma unroll
+            for (int m = 0; m < M; ++m) sub[r][m] = x[m * Rr + r];
+#pragma unroll
+        for (int r = 0; r < Rr; ++r) dft<R, M, DIR>(sub[r]);
+#pragma unroll
+        for (int r = 1; r < Rr; ++r)
+#pragma unroll
+            for (int k = 1; k < M; ++k) sub[r][k] = c_tw<DIR>(sub[r][k], wtab<R>(woff(N) + r * k));
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            C t[Rr];
+#pragma unroll
+            for (int r = 0; r < Rr; ++r) t[r] = sub[r][k];
+            dft<R, Rr, DIR>(t);
+#pragma unroll
+            for (int q = 0; q < Rr; ++q) x[k + M * q] = t[q];
+        }
+    }
+}
+
+// One Stockham stage of radix RAD over `nlines` lines of length n (element p of
+// line l at base[l*ls + p*ps]); Ns = product of the radices of earlier stages.
+template <typename R, int DIR, int RAD>
+__device__ __forceinline__ void stockham_stage(const cplx<R>* src, cplx<R>* dst, int n, int Ns, int nlines, int ls,
+                                               int ps, bool pos_fastest, const cplx<R>* __restrict__ tw) {
+    using C = cplx<R>;
+    const int nb = n / RAD;
+    const int total = nb * nlines;
+    const int tws = n / (Ns * RAD);
+    for (int w = threadIdx.x; w < total; w += blockDim.x) {
+        int j, l;
+        if (pos_fastest) {
+            l = w / nb;
+            j = w - l * nb;
+        } else {
+            j = w / nlines;
+            l = w - j * nlines;
+        }
+        const int k = j % Ns;
+        const C* in = src + l * ls;
+        C* out = dst + l * ls;
+        C x[RAD];
+#pragma unroll
+        for (int t = 0; t < RAD; ++t) x[t] = in[(j + t * nb) * ps];
+        if (k) {
+#pragma unroll
+            for (int t = 1; t < RAD; ++t) x[t] = c_tw<DIR>(x[t], tw[k * t * tws]);
+        }
+        dft<R, RAD, DIR>(x);
+        const int od = (j - k) * RAD + k;
+#pragma unroll
+        for (int q = 0; q < RAD; ++q) out[(od + q * Ns) * ps] = x[q];
+    }
+}
+
+// Mixed-radix Stockham FFT with register codelets; same contract as fft_run.
+template <typename R, int DIR>
+__device__ cplx<R>* fft_big(cplx<R>* a, cplx<R>* b, int nlines, int ls, int ps, bool pos_fastest, const FftPlan& pl,
+                            const cplx<R>* __restrict__ tw) {
+    using C = cplx<R>;
+    const int n = pl.n;
+    int Ns = 1;
+    C* src = a;
+    C* dst = b;
+    for (int s = 0; s < pl.nst; ++s) {
+        const int r = pl.radix[s];
+        constexpr int MAXR = sizeof(R) == 4 ? 32 : BLD_FP64_MAXR;
+        switch (r) {
+            case 2: stockham_stage<R, DIR, 2>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 3: stockham_stage<R, DIR, 3>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 4: stockham_stage<R, DIR, 4>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 6: stockham_stage<R, DIR, 6>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 8: stockham_stage<R, DIR, 8>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 9:
+                if constexpr (MAXR >= 9) stockham_stage<R, DIR, 9>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw);
+                break;
+            case 12:
+                if constexpr (MAXR >= 12) stockham_stage<R, DIR, 12>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw);
+                break;
+            case 16:
+                if constexpr (MAXR >= 16) stockham_stage<R, DIR, 16>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw);
+                break;
+            case 18:
+                if constexpr (MAXR >= 18) stockham_stage<R, DIR, 18>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw);
+                break;
+            case 24:
+                if constexpr (MAXR >= 24) stockham_stage<R, DIR, 24>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw);
+                break;
+            default:
+                if constexpr (MAXR >= 32) stockham_stage<R, DIR, 32>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw);
+                break;
+        }
+        __syncthreads();
+        C* t = src;
+        src = dst;
+        dst = t;
+        Ns *= r;
+    }
+    return src;
+}

@@ -16,6 +16,7 @@
 #pragma once
 
 #include "bld_fft.cuh"
+#include "bld_dft.cuh"
 
 #define BLD_MAXT 10
 #define BLD_MAXC 4
@@ -26,6 +27,26 @@ struct Geo {
 };
 
 __device__ __forceinline__ long long fld_off(const Geo& g, int f) { return (long long)f * g.n3 * g.F; }
+
+// Copies n table entries from global to shared memory with up to 8 loads in
+// flight per thread (a load-then-store loop would wait one DRAM latency per entry).
+template <typename C>
+__device__ __forceinline__ void copy_table(C* dst, const C* __restrict__ src, int n) {
+    constexpr int B = 8;
+    for (int i0 = 0; i0 < n; i0 += B * blockDim.x) {
+        C v[B];
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            if (i < n) v[q] = __ldg(src + i);
+        }
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            if (i < n) dst[i] = v[q];
+        }
+    }
+}
 
 // ------------------------------------------------------------------ inverse y pass
 enum TermOp { T_DIRECT = 0, T_D1 = 1, T_D2 = 2, T_VORT1 = 3, T_VORT2 = 4, T_VORT3 = 5 };
@@ -38,6 +59,7 @@ struct InvYArgs {
     int fld[BLD_MAXT];
     int isI[BLD_MAXT];
     int m0;                      // first member
+    int NL;                      // k1 lines per block
     const double2* state;
     void* mixed;
     long long mixed_mstride;     // elements per member
@@ -93,37 +115,57 @@ __device__ __forceinline__ double2 inv_term_value(const InvYArgs& a, const doubl
 }
 
 // grid (ceil(K1/NL), n3, nterms*members); smem: tw[P2] + 2*P2*NL complex
-template <typename R, int NL>
+// grid (nterms*members, ceil(K1/NL), n3): the terms of one (layer, k1 tile) are
+// neighbouring blocks, so their shared state reads (vorticity needs z and z+1)
+// hit L2.  smem: tw[P2] + 2*P2*NL complex.
+template <typename R>
 __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
     using C = cplx<R>;
+    const int NL = a.NL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* b0 = tw + a.P2;
     C* b1 = b0 + a.P2 * NL;
-    const int t = blockIdx.z % a.nterms, m = a.m0 + blockIdx.z / a.nterms;
-    const int z = blockIdx.y;
+    const int t = blockIdx.x % a.nterms, m = a.m0 + blockIdx.x / a.nterms;
+    const int z = blockIdx.z;
     const int nz = a.isI[t] ? a.g.n3 - 1 : a.g.n3;
     if (z >= nz) return;
     const int op = a.op[t], f = a.fld[t];
     const int K1 = a.g.K1, K2 = a.g.K2, k2max = a.g.k2max, P2 = a.P2;
-    const int k10 = blockIdx.x * NL;
+    const int k10 = blockIdx.y * NL;
     const C* twg = reinterpret_cast<const C*>(a.tw);
-    for (int i = threadIdx.x; i < P2; i += blockDim.x) tw[i] = twg[i];
+    copy_table(tw, twg, P2);
     const double2* S = a.state + (long long)m * a.g.mstride;
-    for (int i = threadIdx.x; i < P2 * NL; i += blockDim.x) {
-        const int p = i / NL, l = i - p * NL;
-        const int k1 = k10 + l;
-        int j = -1;
-        if (p <= k2max)
-            j = p;
-        else if (p >= P2 - k2max)
-            j = K2 - (P2 - p);
-        double2 v = make_double2(0.0, 0.0);
-        if (j >= 0 && k1 < K1) v = inv_term_value(a, S, op, f, z, j, k1);
-        b0[i] = mk<R>((R)v.x, (R)v.y);
+    // zero the padding band, then gather the K2*NL modes in batches of 8 per thread
+    for (int i = threadIdx.x; i < (P2 - K2) * NL; i += blockDim.x) {
+        const int p = k2max + 1 + i / NL, l = i % NL;
+        b0[p * NL + l] = mk<R>(0, 0);
+    }
+    constexpr int BATCH = 8;
+    const int nmodes = K2 * NL;
+    for (int i0 = 0; i0 < nmodes; i0 += BATCH * blockDim.x) {
+        double2 v[BATCH];
+#pragma unroll
+        for (int q = 0; q < BATCH; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            v[q] = make_double2(0.0, 0.0);
+            if (i < nmodes) {
+                const int j = i / NL, l = i - j * NL, k1 = k10 + l;
+                if (k1 < K1) v[q] = inv_term_value(a, S, op, f, z, j, k1);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < BATCH; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            if (i < nmodes) {
+                const int j = i / NL, l = i - j * NL;
+                const int p = (j <= k2max) ? j : P2 - (K2 - j);
+                b0[p * NL + l] = mk<R>((R)v[q].x, (R)v[q].y);
+            }
+        }
     }
     __syncthreads();
-    C* res = fft_run<R, +1>(b0, b1, NL, 1, NL, false, a.plan, tw);
+    C* res = fft_big<R, +1>(b0, b1, NL, 1, NL, false, a.plan, tw);
     C* out = reinterpret_cast<C*>(a.mixed) + (long long)m * a.mixed_mstride + (long long)(t * a.g.n3 + z) * P2 * K1;
     for (int i = threadIdx.x; i < P2 * NL; i += blockDim.x) {
         const int y = i / NL, l = i - y * NL, k1 = k10 + l;
@@ -175,6 +217,16 @@ __device__ __forceinline__ void build_packed(cplx<R>* line, const cplx<R>* rowA,
     }
 }
 
+template <typename R>
+__device__ __forceinline__ void put_packed(cplx<R>* line, cplx<R> A, cplx<R> B, int k, int P1) {
+    if (k == 0) {
+        line[0] = mk<R>(A.x, B.x);
+    } else {
+        line[k] = mk<R>(A.x - B.y, A.y + B.x);
+        line[P1 - k] = mk<R>(A.x + B.y, -A.y + B.x);
+    }
+}
+
 // Unpack forward FFT Z of a + ib: A[k] = (Z[k] + conj(Z[-k]))/2, B[k] = (Z[k] - conj(Z[-k]))/(2i)
 template <typename R>
 __device__ __forceinline__ void unpack_pair(const cplx<R>* line, int k, int P1, cplx<R>& A, cplx<R>& B) {
@@ -188,25 +240,24 @@ __device__ __forceinline__ void unpack_pair(const cplx<R>* line, int k, int P1, 
 // Rotation-form advection (src/processes/momentum_advection.jl:44-206).
 // Inputs: terms 0 u, 1 v, 5 vort3 (C); 2 w, 3 vort1, 4 vort2 (I).
 // Outputs: 0 adv1, 1 adv2 (C); 2 adv3 (I).
-// grid (P2/YT, nchunks, members), block YT*P1/PPT threads.
+// grid (P2/YT, nchunks, members), block YT*P1/PPT <= 256 threads.
 template <typename R, int PPT>
-__global__ void __launch_bounds__(512) k_adv_x(XArgs a) {
+__global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P1 = a.P1, YT = a.YT, n3 = a.g.n3, k1max = a.g.k1max;
     const int NLin = 3 * YT, NLout = YT + (YT + 1) / 2;
-    const int NLmax = NLin > NLout ? NLin : NLout;
+    // two line buffers of NLin lines: inputs/physical values and outputs ping-pong between them
     C* tw = reinterpret_cast<C*>(smem_raw);
-    C* cur = tw + P1;
-    C* scr = cur + NLmax * P1;
-    C* outb = scr + NLmax * P1;
+    C* bufA = tw + P1;
+    C* bufB = bufA + NLin * P1;
     const int y0 = blockIdx.x * YT;
     const int m = a.m0 + blockIdx.z;
     const int z0 = blockIdx.y * a.zchunk;
     const int z1 = min(n3, z0 + a.zchunk);
     const int nthr = blockDim.x;
     const C* twg = reinterpret_cast<const C*>(a.tw);
-    for (int i = threadIdx.x; i < P1; i += nthr) tw[i] = twg[i];
+    copy_table(tw, twg, P1);
     const C* Min = reinterpret_cast<const C*>(a.min) + (long long)m * a.min_mstride;
     C* Mout = reinterpret_cast<C*>(a.mout) + (long long)m * a.mout_mstride;
 
@@ -216,43 +267,56 @@ __global__ void __launch_bounds__(512) k_adv_x(XArgs a) {
 
     for (int j = max(0, z0 - 1); j < z1; ++j) {
         const bool hasI = (j < n3 - 1);
-        // ---- build packed input lines: (u, v), (vort3, w), (vort1, vort2) per y
-        for (int i = threadIdx.x; i < NLin * P1; i += nthr) {
-            const int line = i / P1, k = i - line * P1;
-            if (k > k1max && k < P1 - k1max) {
-                cur[i] = mk<R>(0, 0);
-                continue;
+        C* cur = bufA;
+        // ---- build packed input lines: (u, v), (vort3, w), (vort1, vort2) per y;
+        // zero band first, then the resolved modes with 4 rows in flight per thread
+        const int nk = k1max + 1;
+        for (int i = threadIdx.x; i < NLin * (P1 - 2 * k1max - 1); i += nthr) {
+            const int line = i / (P1 - 2 * k1max - 1), k = k1max + 1 + i % (P1 - 2 * k1max - 1);
+            cur[line * P1 + k] = mk<R>(0, 0);
+        }
+        for (int i0 = 0; i0 < NLin * nk; i0 += 4 * nthr) {
+            C va[4], vb[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = i0 + q * nthr + threadIdx.x;
+                va[q] = vb[q] = mk<R>(0, 0);
+                if (i < NLin * nk) {
+                    const int line = i / nk, k = i - line * nk;
+                    const int yl = line / 3, qq = line - yl * 3, y = y0 + yl;
+                    if (qq == 0) {
+                        va[q] = mrow(Min, a, 0, j, y)[k];
+                        vb[q] = mrow(Min, a, 1, j, y)[k];
+                    } else if (qq == 1) {
+                        va[q] = mrow(Min, a, 5, j, y)[k];
+                        if (hasI) vb[q] = mrow(Min, a, 2, j, y)[k];
+                    } else if (hasI) {
+                        va[q] = mrow(Min, a, 3, j, y)[k];
+                        vb[q] = mrow(Min, a, 4, j, y)[k];
+                    }
+                }
             }
-            if (k > k1max) continue;  // mirrored half written by the owner of P1-k
-            const int yl = line / 3, q = line - yl * 3, y = y0 + yl;
-            const C *ra, *rb;
-            if (q == 0) {
-                ra = mrow(Min, a, 0, j, y);
-                rb = mrow(Min, a, 1, j, y);
-            } else if (q == 1) {
-                ra = mrow(Min, a, 5, j, y);
-                rb = hasI ? mrow(Min, a, 2, j, y) : nullptr;
-            } else {
-                ra = hasI ? mrow(Min, a, 3, j, y) : nullptr;
-                rb = hasI ? mrow(Min, a, 4, j, y) : nullptr;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = i0 + q * nthr + threadIdx.x;
+                if (i < NLin * nk) {
+                    const int line = i / nk, k = i - line * nk;
+                    put_packed<R>(cur + line * P1, va[q], vb[q], k, P1);
+                }
             }
-            build_packed<R>(cur + line * P1, ra, rb, k, P1);
         }
         __syncthreads();
-        C* res = fft_run<R, +1>(cur, scr, NLin, P1, 1, true, a.plan, tw);
-        if (res != cur) {
-            scr = cur;
-            cur = res;
-        }
+        C* phys = fft_big<R, +1>(bufA, bufB, NLin, P1, 1, true, a.plan, tw);
+        C* outb = (phys == bufA) ? bufB : bufA;
         const bool emitC = (j >= z0);
         const bool emitI = (j >= z0) && (j >= 1);
 #pragma unroll
         for (int i = 0; i < PPT; ++i) {
             const int p = threadIdx.x + i * nthr;
             const int yl = p / P1, x = p - yl * P1;
-            const C c0 = cur[(yl * 3 + 0) * P1 + x];
-            const C c1 = cur[(yl * 3 + 1) * P1 + x];
-            const C c2 = cur[(yl * 3 + 2) * P1 + x];
+            const C c0 = phys[(yl * 3 + 0) * P1 + x];
+            const C c1 = phys[(yl * 3 + 1) * P1 + x];
+            const C c2 = phys[(yl * 3 + 2) * P1 + x];
             const R u = c0.x, v = c0.y, o3 = c1.x;
             const R w = hasI ? c1.y : R(0);
             const R o1 = hasI ? c2.x : R(0);
@@ -289,7 +353,7 @@ __global__ void __launch_bounds__(512) k_adv_x(XArgs a) {
         }
         if (emitC) {
             __syncthreads();
-            C* r2 = fft_run<R, -1>(outb, scr, NLout, P1, 1, true, a.plan, tw);
+            C* r2 = fft_big<R, -1>(outb, phys, NLout, P1, 1, true, a.plan, tw);
             const int nk = k1max + 1;
             for (int i = threadIdx.x; i < NLout * nk; i += nthr) {
                 const int line = i / nk, k = i - line * nk;
@@ -306,11 +370,6 @@ __global__ void __launch_bounds__(512) k_adv_x(XArgs a) {
                     if (2 * q + 1 < YT) mrow_w(Mout, a, 2, j - 1, yb)[k] = B;
                 }
             }
-            // restore outb as the output staging buffer for the next layer
-            if (r2 != outb) {
-                scr = outb;
-                outb = r2;
-            }
         }
         __syncthreads();
     }
@@ -326,22 +385,21 @@ __global__ void __launch_bounds__(512) k_adv_x(XArgs a) {
 // Streaming in z with a two-layer lag: step j loads C layer j and I layer j and
 // completes C layer j-1, I layer j-1 and the d3 tau33 of I layer j-2.
 template <typename R, int PPT>
-__global__ void __launch_bounds__(512) k_sgs_x(XArgs a) {
+__global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P1 = a.P1, YT = a.YT, n3 = a.g.n3, k1max = a.g.k1max;
     const int NLin = 5 * YT, NLout = 4 * YT;
     C* tw = reinterpret_cast<C*>(smem_raw);
-    C* cur = tw + P1;
-    C* scr = cur + NLin * P1;
-    C* outb = scr + NLin * P1;
+    C* bufA = tw + P1;
+    C* bufB = bufA + NLin * P1;
     const int y0 = blockIdx.x * YT;
     const int m = a.m0 + blockIdx.z;
     const int z0 = blockIdx.y * a.zchunk;
     const int z1 = min(n3, z0 + a.zchunk);
     const int nthr = blockDim.x;
     const C* twg = reinterpret_cast<const C*>(a.tw);
-    for (int i = threadIdx.x; i < P1; i += nthr) tw[i] = twg[i];
+    copy_table(tw, twg, P1);
     const C* Min = reinterpret_cast<const C*>(a.min) + (long long)m * a.min_mstride;
     C* Mout = reinterpret_cast<C*>(a.mout) + (long long)m * a.mout_mstride;
     const double* lcm = a.lc + (long long)m * n3;
@@ -363,32 +421,49 @@ __global__ void __launch_bounds__(512) k_sgs_x(XArgs a) {
     const int jend = min(n3, z1 + 1);
     for (int j = max(0, z0 - 2); j <= jend; ++j) {
         const bool hasC = (j <= n3 - 1), hasI = (j <= n3 - 2);
+        C* cur = bufA;
+        C* phys = bufA;
         if (hasC) {
-            for (int i = threadIdx.x; i < NLin * P1; i += nthr) {
-                const int line = i / P1, k = i - line * P1;
-                if (k > k1max && k < P1 - k1max) {
-                    cur[i] = mk<R>(0, 0);
-                    continue;
+            const int nk = k1max + 1;
+            for (int i = threadIdx.x; i < NLin * (P1 - 2 * k1max - 1); i += nthr) {
+                const int line = i / (P1 - 2 * k1max - 1), k = k1max + 1 + i % (P1 - 2 * k1max - 1);
+                cur[line * P1 + k] = mk<R>(0, 0);
+            }
+            for (int i0 = 0; i0 < NLin * nk; i0 += 4 * nthr) {
+                C va[4], vb[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int i = i0 + q * nthr + threadIdx.x;
+                    va[q] = vb[q] = mk<R>(0, 0);
+                    if (i < NLin * nk) {
+                        const int line = i / nk, k = i - line * nk;
+                        const int yl = line / 5, qq = line - yl * 5, y = y0 + yl;
+                        switch (qq) {
+                            case 0: va[q] = mrow(Min, a, 0, j, y)[k]; vb[q] = mrow(Min, a, 1, j, y)[k]; break;
+                            case 1: va[q] = mrow(Min, a, 3, j, y)[k]; vb[q] = mrow(Min, a, 4, j, y)[k]; break;
+                            case 2: va[q] = mrow(Min, a, 5, j, y)[k]; vb[q] = mrow(Min, a, 6, j, y)[k]; break;
+                            case 3:
+                                if (hasI) { va[q] = mrow(Min, a, 2, j, y)[k]; vb[q] = mrow(Min, a, 7, j, y)[k]; }
+                                break;
+                            default:
+                                if (hasI) va[q] = mrow(Min, a, 8, j, y)[k];
+                                break;
+                        }
+                    }
                 }
-                if (k > k1max) continue;
-                const int yl = line / 5, q = line - yl * 5, y = y0 + yl;
-                const C *ra, *rb;
-                switch (q) {
-                    case 0: ra = mrow(Min, a, 0, j, y); rb = mrow(Min, a, 1, j, y); break;
-                    case 1: ra = mrow(Min, a, 3, j, y); rb = mrow(Min, a, 4, j, y); break;
-                    case 2: ra = mrow(Min, a, 5, j, y); rb = mrow(Min, a, 6, j, y); break;
-                    case 3: ra = hasI ? mrow(Min, a, 2, j, y) : nullptr; rb = hasI ? mrow(Min, a, 7, j, y) : nullptr; break;
-                    default: ra = hasI ? mrow(Min, a, 8, j, y) : nullptr; rb = nullptr; break;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int i = i0 + q * nthr + threadIdx.x;
+                    if (i < NLin * nk) {
+                        const int line = i / nk, k = i - line * nk;
+                        put_packed<R>(cur + line * P1, va[q], vb[q], k, P1);
+                    }
                 }
-                build_packed<R>(cur + line * P1, ra, rb, k, P1);
             }
             __syncthreads();
-            C* res = fft_run<R, +1>(cur, scr, NLin, P1, 1, true, a.plan, tw);
-            if (res != cur) {
-                scr = cur;
-                cur = res;
-            }
+            phys = fft_big<R, +1>(bufA, bufB, NLin, P1, 1, true, a.plan, tw);
         }
+        C* outb = (phys == bufA) ? bufB : bufA;
         const int c = j - 1;                                   // C layer completed at this step
         const bool doC = (j >= 1) && (c >= z0) && (c < z1);
         const bool do67 = (j >= 1) && (j <= n3 - 1) && (c >= z0) && (c < z1);
@@ -399,11 +474,11 @@ __global__ void __launch_bounds__(512) k_sgs_x(XArgs a) {
             const int yl = p / P1, x = p - yl * P1;
             R u = 0, v = 0, u1 = 0, u2 = 0, v1 = 0, v2 = 0, w = whi, w1 = 0, w2 = 0;
             if (hasC) {
-                const C c0 = cur[(yl * 5 + 0) * P1 + x], c1 = cur[(yl * 5 + 1) * P1 + x];
-                const C c2 = cur[(yl * 5 + 2) * P1 + x];
+                const C c0 = phys[(yl * 5 + 0) * P1 + x], c1 = phys[(yl * 5 + 1) * P1 + x];
+                const C c2 = phys[(yl * 5 + 2) * P1 + x];
                 u = c0.x; v = c0.y; u1 = c1.x; u2 = c1.y; v1 = c2.x; v2 = c2.y;
                 if (hasI) {
-                    const C c3 = cur[(yl * 5 + 3) * P1 + x], c4 = cur[(yl * 5 + 4) * P1 + x];
+                    const C c3 = phys[(yl * 5 + 3) * P1 + x], c4 = phys[(yl * 5 + 4) * P1 + x];
                     w = c3.x; w1 = c3.y; w2 = c4.x;
                 }
             }
@@ -505,7 +580,7 @@ __global__ void __launch_bounds__(512) k_sgs_x(XArgs a) {
         }
         if (doC || do5) {
             __syncthreads();
-            C* r2 = fft_run<R, -1>(outb, scr, NLout, P1, 1, true, a.plan, tw);
+            C* r2 = fft_big<R, -1>(outb, phys, NLout, P1, 1, true, a.plan, tw);
             const int nk = k1max + 1;
             for (int i = threadIdx.x; i < NLout * nk; i += nthr) {
                 const int line = i / nk, k = i - line * nk;
@@ -526,10 +601,6 @@ __global__ void __launch_bounds__(512) k_sgs_x(XArgs a) {
                 } else if (do67) {
                     mrow_w(Mout, a, tb, c, y)[k] = B;
                 }
-            }
-            if (r2 != outb) {
-                scr = outb;
-                outb = r2;
             }
         }
         __syncthreads();
@@ -577,6 +648,7 @@ struct FwdYArgs {
     int fields;                // number of target fields (3 for rates, 1 for transforms)
     int field0;                // first target field
     int m0;                    // first member
+    int NL;                    // k1 lines per block
     FftPlan plan;
     const void* tw;
 };
@@ -645,88 +717,197 @@ __device__ __forceinline__ double2 linear_terms(const Geo& g, const Linear& L, c
     return val;
 }
 
-// grid (ceil(K1/NL), n3, fields*members); smem tw[P2] + 2*P2*NL complex
-template <typename R, int NL, int MAXO>
+// Forward y pass.  Contributions with prefactor 1 or D1 (which depends on k1
+// only) are summed into NL "A" lines before the transform; the D2 contribution
+// (at most one per field) goes to NL "B" lines transformed in the same batch, so
+// the result is A + D2 * B without per-thread accumulators.
+// Layers a rate at layer z needs for the Laplacian: a window of up to three
+// consecutive layers starting at w0 (ghost extrapolation at the walls uses the
+// three layers next to the wall).
+__device__ __forceinline__ int lin_window_start(int z, int nz) { return max(0, min(z - 1, nz - 3)); }
+
+// linear_terms computed from preloaded window values W[0..2] = S[w0..w0+2]
+__device__ __forceinline__ double2 linear_terms_w(const Geo& g, const Linear& L, const double2 (&W)[3], int w0, int f,
+                                                  int z, int j, int k1, int m) {
+    double2 val = make_double2(0.0, 0.0);
+    const bool mean_mode = (j == 0 && k1 == 0);
+    if (L.diff_on[f]) {
+        const int n = (f == 2) ? g.n3 - 1 : g.n3;
+        auto at = [&](int zz) {  // selects keep the window in registers
+            const int r = zz - w0;
+            return r == 0 ? W[0] : (r == 1 ? W[1] : W[2]);
+        };
+        const double2 q0 = at(z);
+        double2 qm, qp;
+        double A, B, Cc;
+        if (f != 2) {
+            A = L.alpha_ext[z];
+            B = L.alpha_c[z];
+            Cc = L.alpha_ext[z + 1];
+            if (z == 0) {
+                const double2 l1 = at(0), l2 = at(1), l3 = at(2);
+                if (L.bc_kind[f][0] == 0) {
+                    qm.x = (-15.0 * l1.x + 5.0 * l2.x - l3.x) / 5.0;
+                    qm.y = (-15.0 * l1.y + 5.0 * l2.y - l3.y) / 5.0;
+                    if (mean_mode) qm.x += 16.0 * L.bc_val[f][0] / 5.0;
+                } else {
+                    qm.x = (21.0 * l1.x + 3.0 * l2.x - l3.x) / 23.0;
+                    qm.y = (21.0 * l1.y + 3.0 * l2.y - l3.y) / 23.0;
+                    if (mean_mode) qm.x -= 24.0 * L.bc_diff[f][0] / 23.0;
+                }
+            } else {
+                qm = at(z - 1);
+            }
+            if (z == n - 1) {
+                const double2 l1 = at(n - 1), l2 = at(n - 2), l3 = at(n - 3);
+                if (L.bc_kind[f][1] == 0) {
+                    qp.x = (-15.0 * l1.x + 5.0 * l2.x - l3.x) / 5.0;
+                    qp.y = (-15.0 * l1.y + 5.0 * l2.y - l3.y) / 5.0;
+                    if (mean_mode) qp.x += 16.0 * L.bc_val[f][1] / 5.0;
+                } else {
+                    qp.x = (21.0 * l1.x + 3.0 * l2.x - l3.x) / 23.0;
+                    qp.y = (21.0 * l1.y + 3.0 * l2.y - l3.y) / 23.0;
+                    if (mean_mode) qp.x -= 24.0 * (-L.bc_diff[f][1]) / 23.0;
+                }
+            } else {
+                qp = at(z + 1);
+            }
+        } else {
+            A = L.alpha_c[z];
+            B = L.alpha_i[z];
+            Cc = L.alpha_c[z + 1];
+            qm = (z == 0) ? make_double2(L.bc_val[2][0], 0.0) : at(z - 1);
+            qp = (z == n - 1) ? make_double2(L.bc_val[2][1], 0.0) : at(z + 1);
+        }
+        const double ab = A * B, bc = B * Cc;
+        const double coef = ((L.DD1[k1] + L.DD2[j]) - ab) - bc;
+        const double nu = L.nu[f];
+        val.x = nu * ((ab * qm.x + coef * q0.x) + bc * qp.x);
+        val.y = nu * ((ab * qm.y + coef * q0.y) + bc * qp.y);
+    }
+    if (L.src_on[f] && mean_mode) val.x += L.src[3 * m + f];
+    return val;
+}
+
+// grid (fields*members, ceil(K1/NL), n3); smem tw[P2] + 2*P2*nlines complex (nlines = NL or 2NL)
+template <typename R>
 __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     using C = cplx<R>;
+    const int NL = a.NL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* tw = reinterpret_cast<C*>(smem_raw);
-    C* b0 = tw + a.P2;
-    C* b1 = b0 + a.P2 * NL;
-    const int fi = blockIdx.z % a.fields, m = a.m0 + blockIdx.z / a.fields;
+    const int fi = blockIdx.x % a.fields, m = a.m0 + blockIdx.x / a.fields;
     const int f = a.field0 + fi;
-    const int z = blockIdx.y;
+    const int z = blockIdx.z;
     const Geo& g = a.g;
     const int nz = (f == 2) ? g.n3 - 1 : g.n3;
     if (z >= nz) return;
     const int K1 = g.K1, K2 = g.K2, k2max = g.k2max, P2 = a.P2;
-    const int k10 = blockIdx.x * NL;
-    const C* twg = reinterpret_cast<const C*>(a.tw);
-    for (int i = threadIdx.x; i < P2; i += blockDim.x) tw[i] = twg[i];
-    double2 acc[MAXO];
-#pragma unroll
-    for (int r = 0; r < MAXO; ++r) acc[r] = make_double2(0.0, 0.0);
-    const int nout = K2 * NL;
+    const int k10 = blockIdx.y * NL;
     const int nc = a.ncontrib[fi];
-    for (int ci = 0; ci < nc; ++ci) {
-        const FwdContrib cb = a.c[fi][ci];
-        const C* src = reinterpret_cast<const C*>(a.mout) + (long long)m * a.mout_mstride +
-                       (long long)(cb.term * g.n3 + z) * P2 * K1;
-        for (int i = threadIdx.x; i < P2 * NL; i += blockDim.x) {
-            const int y = i / NL, l = i - y * NL, k1 = k10 + l;
-            b0[i] = (k1 < K1) ? src[(long long)y * K1 + k1] : mk<R>(0, 0);
-        }
-        __syncthreads();
-        const C* res = fft_run<R, -1>(b0, b1, NL, 1, NL, false, a.plan, tw);
+    bool hasB = false;
+    for (int ci = 0; ci < nc; ++ci) hasB |= (a.c[fi][ci].pref == 2);
+    const int nlines = hasB ? 2 * NL : NL;
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* b0 = tw + P2;
+    C* b1 = b0 + P2 * nlines;
+    const C* twg = reinterpret_cast<const C*>(a.tw);
+    copy_table(tw, twg, P2);
+    const C* base = reinterpret_cast<const C*>(a.mout) + (long long)m * a.mout_mstride;
+    const long long layer = (long long)P2 * K1;
+    // line l < NL: A set (k1 = k10 + l); NL <= l < 2NL: B set; loads batched 4 per thread
+    constexpr int BATCH = 4;
+    const int nval = P2 * nlines;
+    for (int i0 = 0; i0 < nval; i0 += BATCH * blockDim.x) {
+        C v[BATCH];
 #pragma unroll
-        for (int r = 0; r < MAXO; ++r) {
-            const int o = threadIdx.x + r * blockDim.x;
-            if (o < nout) {
-                const int j = o / NL, l = o - j * NL;
-                const int pos = (j <= k2max) ? j : P2 - (K2 - j);
-                const C X = res[pos * NL + l];
-                double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
-                if (cb.pref == 1) {
-                    const int k1 = min(k10 + l, K1 - 1);
-                    const double d = a.d1[k1];
-                    const double tx = -d * vy;
-                    vy = d * vx;
-                    vx = tx;
-                } else if (cb.pref == 2) {
-                    const double d = a.d2[j];
-                    const double tx = -d * vy;
-                    vy = d * vx;
-                    vx = tx;
+        for (int q = 0; q < BATCH; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            v[q] = mk<R>(0, 0);
+            if (i < nval) {
+                const int y = i / nlines, l = i - y * nlines;
+                const bool isB = l >= NL;
+                const int k1 = k10 + (isB ? l - NL : l);
+                if (k1 < K1) {
+                    for (int ci = 0; ci < nc; ++ci) {
+                        const FwdContrib cb = a.c[fi][ci];
+                        if ((cb.pref == 2) != isB) continue;
+                        C x = base[(long long)(cb.term * g.n3 + z) * layer + (long long)y * K1 + k1];
+                        if (cb.pref == 1) {  // D1 = i d1[k1]
+                            const R d = (R)a.d1[k1];
+                            const R tx = -d * x.y;
+                            x.y = d * x.x;
+                            x.x = tx;
+                        }
+                        v[q].x += x.x;
+                        v[q].y += x.y;
+                    }
                 }
-                acc[r].x += vx;
-                acc[r].y += vy;
             }
         }
-        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < BATCH; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            if (i < nval) b0[i] = v[q];
+        }
     }
+    __syncthreads();
+    const C* res = fft_big<R, -1>(b0, b1, nlines, 1, nlines, false, a.plan, tw);
     double2* du = a.du + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F;
-    const double2* S = a.state ? a.state + (long long)m * g.mstride : nullptr;
+    const double2* Sf = a.state ? a.state + (long long)m * g.mstride + fld_off(g, f) : nullptr;
+    const bool need_win = (a.mode == 1) && a.lin.diff_on[f];
+    const int w0 = lin_window_start(z, nz);
+    const int wn = min(3, nz);
     bool bad = false;
+    constexpr int OB = 4;  // outputs per thread whose loads are issued together
+    const int nout = K2 * NL;
+    for (int o0 = 0; o0 < nout; o0 += OB * blockDim.x) {
+        double2 W[OB][3];
+        double2 old[OB];
 #pragma unroll
-    for (int r = 0; r < MAXO; ++r) {
-        const int o = threadIdx.x + r * blockDim.x;
-        if (o < nout) {
+        for (int q = 0; q < OB; ++q) {
+            const int o = o0 + q * blockDim.x + threadIdx.x;
             const int j = o / NL, l = o - j * NL, k1 = k10 + l;
-            if (k1 < K1) {
+            if (o < nout && k1 < K1) {
                 const long long idx = (long long)j * K1 + k1;
-                double2 v;
-                if (a.mode == 1) {
-                    const double2 lin = linear_terms(g, a.lin, S, f, z, j, k1, m);
-                    v = make_double2(lin.x + acc[r].x, lin.y + acc[r].y);
-                } else if (a.mode == 2) {
-                    v = acc[r];
-                } else {
-                    const double2 o0 = du[idx];
-                    v = make_double2(o0.x + acc[r].x, o0.y + acc[r].y);
+                if (need_win) {
+#pragma unroll
+                    for (int r = 0; r < 3; ++r)
+                        if (r < wn) W[q][r] = Sf[(long long)(w0 + r) * g.F + idx];
                 }
-                du[idx] = v;
-                if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
+                if (a.mode == 0) old[q] = du[idx];
             }
+        }
+#pragma unroll
+        for (int q = 0; q < OB; ++q) {
+            const int o = o0 + q * blockDim.x + threadIdx.x;
+            const int j = o / NL, l = o - j * NL, k1 = k10 + l;
+            if (o >= nout || k1 >= K1) continue;
+            const int pos = (j <= k2max) ? j : P2 - (K2 - j);
+            const C X = res[pos * nlines + l];
+            double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
+            if (hasB) {
+                const C Y = res[pos * nlines + NL + l];
+                const double d = a.d2[j];
+                const double bx = (double)Y.x * a.inv_n, by = (double)Y.y * a.inv_n;
+                vx += -d * by;
+                vy += d * bx;
+            }
+            const long long idx = (long long)j * K1 + k1;
+            double2 v;
+            if (a.mode == 1) {
+                double2 lin;
+                if (need_win)
+                    lin = linear_terms_w(g, a.lin, W[q], w0, f, z, j, k1, m);
+                else
+                    lin = linear_terms(g, a.lin, nullptr, f, z, j, k1, m);
+                v = make_double2(lin.x + vx, lin.y + vy);
+            } else if (a.mode == 2) {
+                v = make_double2(vx, vy);
+            } else {
+                v = make_double2(old[q].x + vx, old[q].y + vy);
+            }
+            du[idx] = v;
+            if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
         }
     }
     if (a.check && bad) atomicOr(a.flag, 1);
@@ -835,42 +1016,55 @@ __global__ void __launch_bounds__(128) k_project(ProjArgs a) {
         double2* P = a.pscr + (long long)m * n * F + c;
         double2 wprev = make_double2(0.0, 0.0);
         double2 b = make_double2(0.0, 0.0);
-        for (int z = 0; z < n; ++z) {
-            const double2 uz = stage_value(a, o1 + z * F + c);
-            const double2 vz = stage_value(a, o2 + z * F + c);
-            a.out[o1 + z * F + c] = uz;
-            a.out[o2 + z * F + c] = vz;
-            double2 wz = make_double2(0.0, 0.0);
-            if (z < n - 1) {
-                wz = stage_value(a, o3 + z * F + c);
-                a.out[o3 + z * F + c] = wz;
+        constexpr int NB = 4;  // layers whose loads are issued together
+        for (int zb = 0; zb < n; zb += NB) {
+            double2 U[NB], V[NB], W[NB];
+            double G[NB];
+#pragma unroll
+            for (int q = 0; q < NB; ++q) {
+                const int z = zb + q;
+                if (z < n) {
+                    U[q] = stage_value(a, o1 + z * F + c);
+                    V[q] = stage_value(a, o2 + z * F + c);
+                    W[q] = (z < n - 1) ? stage_value(a, o3 + z * F + c) : make_double2(0.0, 0.0);
+                    G[q] = a.gamma[(long long)z * F + c];
+                }
             }
-            const double h = 1.0 / a.alpha_c[z];
-            double2 val;
-            val.x = (-e1 * uz.y) * h + (-e2 * vz.y) * h;
-            val.y = (e1 * uz.x) * h + (e2 * vz.x) * h;
-            if (z == 0) {
-                val.x += wz.x;
-                val.y += wz.y;
-                if (mean_mode) val.x -= a.w_lo;
-            } else if (z == n - 1) {
-                val.x -= wprev.x;
-                val.y -= wprev.y;
-                if (mean_mode) val.x += a.w_hi;
-            } else {
-                val.x = val.x - wprev.x + wz.x;
-                val.y = val.y - wprev.y + wz.y;
+#pragma unroll
+            for (int q = 0; q < NB; ++q) {
+                const int z = zb + q;
+                if (z >= n) break;
+                const double2 uz = U[q], vz = V[q], wz = W[q];
+                a.out[o1 + z * F + c] = uz;
+                a.out[o2 + z * F + c] = vz;
+                if (z < n - 1) a.out[o3 + z * F + c] = wz;
+                const double h = 1.0 / a.alpha_c[z];
+                double2 val;
+                val.x = (-e1 * uz.y) * h + (-e2 * vz.y) * h;
+                val.y = (e1 * uz.x) * h + (e2 * vz.x) * h;
+                if (z == 0) {
+                    val.x += wz.x;
+                    val.y += wz.y;
+                    if (mean_mode) val.x -= a.w_lo;
+                } else if (z == n - 1) {
+                    val.x -= wprev.x;
+                    val.y -= wprev.y;
+                    if (mean_mode) val.x += a.w_hi;
+                } else {
+                    val.x = val.x - wprev.x + wz.x;
+                    val.y = val.y - wprev.y + wz.y;
+                }
+                if (mean_mode && z == n - 1) val = make_double2(0.0, 0.0);  // adjust_pressure_rhs! (:396)
+                const double gm = G[q];
+                if (z == 0) {
+                    b = make_double2(gm * val.x, gm * val.y);
+                } else {
+                    const double be = a.alpha_i[z - 1];
+                    b = make_double2(gm * (val.x - be * b.x), gm * (val.y - be * b.y));
+                }
+                P[(long long)z * F] = b;
+                wprev = wz;
             }
-            if (mean_mode && z == n - 1) val = make_double2(0.0, 0.0);  // adjust_pressure_rhs! (:396)
-            const double gm = a.gamma[(long long)z * F + c];
-            if (z == 0) {
-                b = make_double2(gm * val.x, gm * val.y);
-            } else {
-                const double be = a.alpha_i[z - 1];
-                b = make_double2(gm * (val.x - be * b.x), gm * (val.y - be * b.y));
-            }
-            P[(long long)z * F] = b;
-            wprev = wz;
         }
         // backward sweep and gradient, top to bottom
         double2 pn = b;  // p at z = n-1
@@ -882,20 +1076,37 @@ __global__ void __launch_bounds__(128) k_project(ProjArgs a) {
             a.out[o1 + z * F + c] = u;
             a.out[o2 + z * F + c] = v;
         }
-        for (int z = n - 2; z >= 0; --z) {
-            const double2 bz = P[(long long)z * F];
-            const double gb = a.gamma[(long long)z * F + c] * a.alpha_i[z];
-            const double2 pz = make_double2(bz.x - gb * pn.x, bz.y - gb * pn.y);
-            double2 u = a.out[o1 + z * F + c], v = a.out[o2 + z * F + c], w = a.out[o3 + z * F + c];
-            u.x += e1 * pz.y; u.y += -e1 * pz.x;
-            v.x += e2 * pz.y; v.y += -e2 * pz.x;
-            const double ai = a.alpha_i[z];
-            w.x += -1.0 * (-ai * pz.x + ai * pn.x);
-            w.y += -1.0 * (-ai * pz.y + ai * pn.y);
-            a.out[o1 + z * F + c] = u;
-            a.out[o2 + z * F + c] = v;
-            a.out[o3 + z * F + c] = w;
-            pn = pz;
+        for (int zt = n - 2; zt >= 0; zt -= NB) {
+            double2 Bz[NB], U[NB], V[NB], W[NB];
+            double G[NB];
+#pragma unroll
+            for (int q = 0; q < NB; ++q) {
+                const int z = zt - q;
+                if (z >= 0) {
+                    Bz[q] = P[(long long)z * F];
+                    G[q] = a.gamma[(long long)z * F + c];
+                    U[q] = a.out[o1 + z * F + c];
+                    V[q] = a.out[o2 + z * F + c];
+                    W[q] = a.out[o3 + z * F + c];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NB; ++q) {
+                const int z = zt - q;
+                if (z < 0) break;
+                const double ai = a.alpha_i[z];
+                const double gb = G[q] * ai;
+                const double2 pz = make_double2(Bz[q].x - gb * pn.x, Bz[q].y - gb * pn.y);
+                double2 u = U[q], v = V[q], w = W[q];
+                u.x += e1 * pz.y; u.y += -e1 * pz.x;
+                v.x += e2 * pz.y; v.y += -e2 * pz.x;
+                w.x += -1.0 * (-ai * pz.x + ai * pn.x);
+                w.y += -1.0 * (-ai * pz.y + ai * pn.y);
+                a.out[o1 + z * F + c] = u;
+                a.out[o2 + z * F + c] = v;
+                a.out[o3 + z * F + c] = w;
+                pn = pz;
+            }
         }
     } else if (a.kind != S_NONE || a.out != a.u) {
         for (int z = 0; z < n; ++z) {
@@ -911,6 +1122,213 @@ __global__ void __launch_bounds__(128) k_project(ProjArgs a) {
             double s = 0.0;
             for (int z = 0; z < n; ++z) s += a.out[of + z * F].x * a.mean_w[z];
             const double add = a.mean_val[3 * m + f] - s;
+            for (int z = 0; z < n; ++z) a.out[of + z * F].x += add;
+        }
+    }
+}
+
+// Segmented projection: block (32 columns, NS z segments of <= LMAX layers),
+// grid (ceil(F/32), members).  The Thomas sweeps are first-order linear
+// recurrences, so each segment solves its part as an affine function of the
+// value entering from below (forward: b_z = P_z + Q_z b_in) or from above
+// (backward: p_z = G_z + H_z p_out) and the segments are chained through shared
+// memory.  Same arithmetic as k_project up to the order of operations.
+template <int LMAX>
+__global__ void __launch_bounds__(512) k_project_seg(ProjArgs a) {
+    const Geo& g = a.g;
+    const int n = g.n3;
+    const long long F = g.F;
+    const int NS = blockDim.y, s = threadIdx.y, lane = threadIdx.x;
+    const int c = blockIdx.x * 32 + lane;
+    const int m = a.m0 + blockIdx.y;
+    const bool valid = c < g.F;
+    const int L = (n + NS - 1) / NS;
+    const int z0 = min(n, s * L), z1 = min(n, z0 + L);
+    const int len = z1 - z0;
+    __shared__ double2 sP[32][32];
+    __shared__ double sQ[32][32];
+    const long long mb = (long long)m * g.mstride;
+    const long long o1 = mb, o2 = mb + (long long)n * F, o3 = mb + 2LL * n * F;
+    const int cc = valid ? c : 0;
+    const int j = cc / g.K1, k1 = cc - j * g.K1;
+    const bool mean_mode = (c == 0);
+    const double e1 = a.d1[k1], e2 = a.d2[j];
+    // stage value of w just below the segment, read before any thread writes `out`
+    double2 wprev = make_double2(0.0, 0.0);
+    if (valid && z0 > 0 && len > 0) wprev = stage_value(a, o3 + (long long)(z0 - 1) * F + c);
+    __syncthreads();
+    double2 X[LMAX];
+    double Y[LMAX];
+    // ---- phase 1: stage values, divergence, segment-local forward sweep
+    // (loads of 4 layers issued together, then the dependent recurrence)
+    constexpr int NBL = 4;
+#pragma unroll
+    for (int qb = 0; qb < LMAX; qb += NBL) {
+        double2 Ub[NBL], Vb[NBL], Wb[NBL];
+        double Gb[NBL];
+#pragma unroll
+        for (int r = 0; r < NBL; ++r) {
+            const int q = qb + r, z = z0 + q;
+            if (q < len && valid) {
+                Ub[r] = stage_value(a, o1 + z * F + c);
+                Vb[r] = stage_value(a, o2 + z * F + c);
+                Wb[r] = (z < n - 1) ? stage_value(a, o3 + z * F + c) : make_double2(0.0, 0.0);
+                Gb[r] = a.gamma[z * F + c];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NBL; ++r) {
+            const int q = qb + r, z = z0 + q;
+            if (q < len && valid) {
+                const double2 uz = Ub[r], vz = Vb[r], wz = Wb[r];
+                a.out[o1 + z * F + c] = uz;
+                a.out[o2 + z * F + c] = vz;
+                if (z < n - 1) a.out[o3 + z * F + c] = wz;
+                const double h = 1.0 / a.alpha_c[z];
+                double2 val;
+                val.x = (-e1 * uz.y) * h + (-e2 * vz.y) * h;
+                val.y = (e1 * uz.x) * h + (e2 * vz.x) * h;
+                if (z == 0) {
+                    val.x += wz.x;
+                    val.y += wz.y;
+                    if (mean_mode) val.x -= a.w_lo;
+                } else if (z == n - 1) {
+                    val.x -= wprev.x;
+                    val.y -= wprev.y;
+                    if (mean_mode) val.x += a.w_hi;
+                } else {
+                    val.x = val.x - wprev.x + wz.x;
+                    val.y = val.y - wprev.y + wz.y;
+                }
+                if (mean_mode && z == n - 1) val = make_double2(0.0, 0.0);
+                const double gm = Gb[r];
+                if (z == 0) {
+                    X[q] = make_double2(gm * val.x, gm * val.y);
+                    Y[q] = 0.0;
+                } else if (q == 0) {
+                    X[q] = make_double2(gm * val.x, gm * val.y);
+                    Y[q] = -gm * a.alpha_i[z - 1];
+                } else {
+                    const double be = a.alpha_i[z - 1];
+                    X[q] = make_double2(gm * (val.x - be * X[q - 1].x), gm * (val.y - be * X[q - 1].y));
+                    Y[q] = -gm * be * Y[q - 1];
+                }
+                wprev = wz;
+            }
+        }
+    }
+    // segment summaries: an empty segment passes its input through unchanged
+    {
+        double2 pe = make_double2(0.0, 0.0);
+        double qe = 1.0;
+        if (len > 0 && valid) {
+#pragma unroll
+            for (int q = 0; q < LMAX; ++q)
+                if (q == len - 1) {
+                    pe = X[q];
+                    qe = Y[q];
+                }
+        }
+        sP[s][lane] = pe;
+        sQ[s][lane] = qe;
+    }
+    __syncthreads();
+    double2 bin = make_double2(0.0, 0.0);
+    for (int t = 0; t < s; ++t) {
+        const double2 pe = sP[t][lane];
+        const double qe = sQ[t][lane];
+        bin = make_double2(pe.x + qe * bin.x, pe.y + qe * bin.y);
+    }
+    __syncthreads();
+    // ---- phase 2: b_z, then the segment-local backward sweep
+#pragma unroll
+    for (int q = 0; q < LMAX; ++q)
+        if (q < len) X[q] = make_double2(X[q].x + Y[q] * bin.x, X[q].y + Y[q] * bin.y);
+#pragma unroll
+    for (int qq = 0; qq < LMAX; ++qq) {
+        const int q = LMAX - 1 - qq;
+        if (q >= len || !valid) continue;
+        const int z = z0 + q;
+        if (z == n - 1) {
+            Y[q] = 0.0;  // p_{n-1} = b_{n-1}
+        } else {
+            const double cz = a.gamma[z * F + c] * a.alpha_i[z];
+            if (q == len - 1) {
+                Y[q] = -cz;
+            } else {
+                X[q] = make_double2(X[q].x - cz * X[q + 1].x, X[q].y - cz * X[q + 1].y);
+                Y[q] = -cz * Y[q + 1];
+            }
+        }
+    }
+    {
+        double2 ps = make_double2(0.0, 0.0);
+        double hs = 1.0;
+        if (len > 0 && valid) {
+            ps = X[0];
+            hs = Y[0];
+        }
+        sP[s][lane] = ps;
+        sQ[s][lane] = hs;
+    }
+    __syncthreads();
+    double2 pout = make_double2(0.0, 0.0);
+    for (int t = NS - 1; t > s; --t) {
+        const double2 ps = sP[t][lane];
+        const double hs = sQ[t][lane];
+        pout = make_double2(ps.x + hs * pout.x, ps.y + hs * pout.y);
+    }
+    // ---- phase 3: pressure and gradient
+#pragma unroll
+    for (int q = 0; q < LMAX; ++q)
+        if (q < len) X[q] = make_double2(X[q].x + Y[q] * pout.x, X[q].y + Y[q] * pout.y);
+#pragma unroll
+    for (int qb = 0; qb < LMAX; qb += NBL) {
+        double2 Ub[NBL], Vb[NBL], Wb[NBL];
+#pragma unroll
+        for (int r = 0; r < NBL; ++r) {
+            const int q = qb + r, z = z0 + q;
+            if (q < len && valid) {
+                Ub[r] = a.out[o1 + z * F + c];
+                Vb[r] = a.out[o2 + z * F + c];
+                if (z < n - 1) Wb[r] = a.out[o3 + z * F + c];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NBL; ++r) {
+            const int q = qb + r, z = z0 + q;
+            if (q < len && valid) {
+                const double2 pz = X[q];
+                double2 pn = pout;
+#pragma unroll
+                for (int rr = 0; rr < LMAX; ++rr)
+                    if (rr == q + 1 && rr < len) pn = X[rr];
+                double2 u = Ub[r], v = Vb[r];
+                u.x += e1 * pz.y;
+                u.y += -e1 * pz.x;
+                v.x += e2 * pz.y;
+                v.y += -e2 * pz.x;
+                a.out[o1 + z * F + c] = u;
+                a.out[o2 + z * F + c] = v;
+                if (z < n - 1) {
+                    double2 w = Wb[r];
+                    const double ai = a.alpha_i[z];
+                    w.x += -1.0 * (-ai * pz.x + ai * pn.x);
+                    w.y += -1.0 * (-ai * pz.y + ai * pn.y);
+                    a.out[o3 + z * F + c] = w;
+                }
+            }
+        }
+    }
+    // ConstantMean on the (0,0) column (src/processes/sources.jl:69-77)
+    __syncthreads();
+    if (c == 0 && s == 0) {
+        for (int f = 0; f < 2; ++f) {
+            if (!a.mean_on[f]) continue;
+            const long long of = (f == 0) ? o1 : o2;
+            double sum = 0.0;
+            for (int z = 0; z < n; ++z) sum += a.out[of + z * F].x * a.mean_w[z];
+            const double add = a.mean_val[3 * m + f] - sum;
             for (int z = 0; z < n; ++z) a.out[of + z * F].x += add;
         }
     }
@@ -969,7 +1387,7 @@ __global__ void __launch_bounds__(256) k_x_r2c(XPlainArgs a) {
         b0[x] = make_double2(va, vb);
     }
     __syncthreads();
-    double2* res = fft_run<double, -1>(b0, b1, 1, a.P1, 1, true, a.plan, tw);
+    double2* res = fft_big<double, -1>(b0, b1, 1, a.P1, 1, true, a.plan, tw);
     for (int k = threadIdx.x; k <= a.k1max; k += blockDim.x) {
         double2 A, B;
         unpack_pair<double>(res, k, a.P1, A, B);
@@ -993,7 +1411,7 @@ __global__ void __launch_bounds__(256) k_x_c2r(XPlainArgs a) {
             build_packed<double>(b0, a.mixed_in + r0 * a.K1, (r1 < rows) ? a.mixed_in + r1 * a.K1 : nullptr, k, a.P1);
     }
     __syncthreads();
-    double2* res = fft_run<double, +1>(b0, b1, 1, a.P1, 1, true, a.plan, tw);
+    double2* res = fft_big<double, +1>(b0, b1, 1, a.P1, 1, true, a.plan, tw);
     for (int x = threadIdx.x; x < a.P1; x += blockDim.x) {
         a.pd_out[r0 * a.P1 + x] = res[x].x;
         if (r1 < rows) a.pd_out[r1 * a.P1 + x] = res[x].y;
