@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -110,6 +111,14 @@ struct DevTw {
     void* d32 = nullptr;
 };
 
+// a y-pass variant: per-term (per-field) blocks with a two-buffer FFT, or one
+// block for all terms (fields) of a layer with an in-place FFT
+struct YCfg {
+    int all = 0;
+    int NL = 4;    // k1 lines per term (per field and line set)
+    int thr = 256;
+};
+
 struct Space {
     bool on = false;
     int P1 = 0, P2 = 0, ref_P1 = 0, ref_P2 = 0;
@@ -118,8 +127,9 @@ struct Space {
     void* min = nullptr;
     void* mout = nullptr;
     long long min_ms = 0, mout_ms = 0;  // elements per member
-    int YT = 1, PPT = 1, zchunk = 1, nchunks = 1;
-    int NLy = 8, NLf = 8, fsets = 1;  // y-pass lines per block (inverse, forward), forward line sets
+    int YT = 1, PPT = 1, zchunk = 1, nchunks = 1;  // x kernels: rows per block, points per thread, z chunks
+    int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
+    YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
 };
 
 }  // namespace
@@ -217,30 +227,9 @@ int pick_y(int P2, bool fp32, int sets) {
 }
 
 // choose tiles for a physical-domain space
-void tile_space(const bld_handle* h, Space& s, bool is_adv) {
-    // (y rows per block, points per thread): blocks of <= 256 threads near 96
-    // (advection, double) / 128 (SGS, double) / 192 (single) threads, so several
-    // blocks stay resident per SM despite the codelet registers; fewer points per
-    // thread (registers) and fewer rows (shared memory) break ties
-    const int target = h->fp32 ? 192 : (is_adv ? 96 : 128);
-    int best = 1 << 30;
-    s.YT = 1;
-    s.PPT = 0;
-    for (int yt : {1, 2, 4}) {
-        if (s.P2 % yt || yt * s.P1 > 1024) continue;
-        const int pts = yt * s.P1;
-        for (int ppt = 1; ppt <= 4; ++ppt) {
-            if (pts % ppt) continue;
-            const int thr = pts / ppt;
-            if (thr > 256) continue;
-            const int score = std::abs(thr - target) + 24 * (ppt - 1) + 8 * (yt - 1);
-            if (score < best) {
-                best = score;
-                s.YT = yt;
-                s.PPT = ppt;
-            }
-        }
-    }
+// z chunks of the x kernels for the current rows per block: enough blocks to
+// fill the GPU a few times over, at least 8 layers per chunk
+void x_chunks(const bld_handle* h, Space& s) {
     const int n3 = h->g.n3;
     const long long blocks_per_chunk = (long long)(s.P2 / s.YT) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
@@ -249,11 +238,63 @@ void tile_space(const bld_handle* h, Space& s, bool is_adv) {
     s.nchunks = (n3 + s.zchunk - 1) / s.zchunk;
 }
 
+// (rows per block, points per thread) candidates of the x kernels: blocks of
+// 32..256 threads whose two line buffers fit in 150 KB of shared memory
+std::vector<std::pair<int, int>> x_candidates(const bld_handle* h, const Space& s, bool is_adv) {
+    std::vector<std::pair<int, int>> out;
+    const int lines = is_adv ? 3 : 5;
+    for (int yt : {1, 2, 4}) {
+        if (s.P2 % yt || yt * s.P1 > 1024) continue;
+        if ((size_t)(s.P1 + 2 * lines * yt * s.P1) * csize(h->fp32) > 150 * 1024) continue;
+        for (int ppt = 1; ppt <= 4; ++ppt) {
+            const int pts = yt * s.P1;
+            if (pts % ppt) continue;
+            const int thr = pts / ppt;
+            if (thr > 256 || thr < 32) continue;
+            out.emplace_back(yt, ppt);
+        }
+    }
+    return out;
+}
+
+void tile_space(const bld_handle* h, Space& s, bool is_adv) {
+    // initial choice near 96 (advection, double) / 128 (SGS, double) / 192 (single)
+    // threads; the autotuner replaces it with the measured best
+    const int target = h->fp32 ? 192 : (is_adv ? 96 : 128);
+    int best = 1 << 30;
+    s.YT = 1;
+    s.PPT = 0;
+    for (auto c : x_candidates(h, s, is_adv)) {
+        const int thr = c.first * s.P1 / c.second;
+        const int score = std::abs(thr - target) + 24 * (c.second - 1) + 8 * (c.first - 1);
+        if (score < best) {
+            best = score;
+            s.YT = c.first;
+            s.PPT = c.second;
+        }
+    }
+    x_chunks(h, s);
+}
+
 size_t smem_y(int P2, int NL, bool fp32) { return (size_t)(P2 + 2 * P2 * NL) * csize(fp32); }
 size_t smem_adv(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 3 * s.YT * s.P1) * csize(fp32); }
 size_t smem_sgs(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 5 * s.YT * s.P1) * csize(fp32); }
 
 // ------------------------------------------------------------------ kernel dispatch
+// threads for an in-place transform of `lines` lines (one task per thread for
+// radix >= 8, up to four for smaller radices); 0 if more than 384 are needed
+int inplace_threads(const FftPlan& pl, int lines) {
+    int thr = 32;
+    for (int i = 0; i < pl.nst; ++i) {
+        const int r = pl.radix[i];
+        const int tpt = r <= 4 ? 4 : (r == 6 ? 3 : 1);  // inplace_tpt
+        const int tasks = lines * pl.n / r;
+        thr = std::max(thr, (tasks + tpt - 1) / tpt);
+    }
+    thr = (thr + 31) / 32 * 32;
+    return thr <= 384 ? thr : 0;
+}
+
 // threads of a y-pass block: enough for the widest FFT stage of `lines` lines
 int y_threads(const FftPlan& pl, int lines) {
     int rmin = 64;
@@ -264,20 +305,32 @@ int y_threads(const FftPlan& pl, int lines) {
 
 template <typename R>
 int launch_inv_y(bld_handle* h, const Space& s, InvYArgs a, int nm) {
-    a.NL = s.NLy;
-    dim3 grid(a.nterms * nm, (h->g.K1 + s.NLy - 1) / s.NLy, h->g.n3);
-    const size_t sm = smem_y(s.P2, s.NLy, sizeof(R) == 4);
-    k_inv_y<R><<<grid, y_threads(a.plan, s.NLy), sm, h->stream>>>(a);
+    const YCfg& c = s.inv;
+    a.NL = c.NL;
+    const size_t cs = csize(sizeof(R) == 4);
+    if (c.all) {
+        dim3 grid((h->g.K1 + c.NL - 1) / c.NL, h->g.n3, nm);
+        k_inv_y_all<R><<<grid, c.thr, (size_t)(s.P2 + s.P2 * a.nterms * c.NL) * cs, h->stream>>>(a);
+    } else {
+        dim3 grid(a.nterms * nm, (h->g.K1 + c.NL - 1) / c.NL, h->g.n3);
+        k_inv_y<R><<<grid, c.thr, (size_t)(s.P2 + 2 * s.P2 * c.NL) * cs, h->stream>>>(a);
+    }
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
 }
 
 template <typename R>
 int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
-    a.NL = s.NLf;
-    dim3 grid(a.fields * nm, (h->g.K1 + s.NLf - 1) / s.NLf, h->g.n3);
-    const size_t sm = smem_y(s.P2, s.fsets * s.NLf, sizeof(R) == 4);
-    k_fwd_y<R><<<grid, y_threads(a.plan, s.fsets * s.NLf), sm, h->stream>>>(a);
+    const YCfg& c = s.fwd;
+    a.NL = c.NL;
+    const size_t cs = csize(sizeof(R) == 4);
+    if (c.all) {
+        dim3 grid((h->g.K1 + c.NL - 1) / c.NL, h->g.n3, nm);
+        k_fwd_y_all<R><<<grid, c.thr, (size_t)(s.P2 + s.P2 * 3 * s.fsets * c.NL) * cs, h->stream>>>(a);
+    } else {
+        dim3 grid(a.fields * nm, (h->g.K1 + c.NL - 1) / c.NL, h->g.n3);
+        k_fwd_y<R><<<grid, c.thr, (size_t)(s.P2 + 2 * s.P2 * s.fsets * c.NL) * cs, h->stream>>>(a);
+    }
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
 }
@@ -325,6 +378,8 @@ int set_smem_limits_R() {
     } while (0)
     BLD_SET((k_inv_y<R>));
     BLD_SET((k_fwd_y<R>));
+    BLD_SET((k_inv_y_all<R>));
+    BLD_SET((k_fwd_y_all<R>));
     BLD_SET((k_adv_x<R, 1>));
     BLD_SET((k_adv_x<R, 2>));
     BLD_SET((k_adv_x<R, 3>));
@@ -510,6 +565,110 @@ int enqueue_x(bld_handle* h, int sp, int m0, int nm) {
 int enqueue_fwd_y(bld_handle* h, int sp, bool first, bool last, const double2* st, double2* du, int m0, int nm) {
     return h->fp32 ? enqueue_fwd_y_R<float>(h, sp, first, last, st, du, m0, nm)
                    : enqueue_fwd_y_R<double>(h, sp, first, last, st, du, m0, nm);
+}
+
+// ------------------------------------------------------------------ autotuner
+// y-pass candidates: per-term blocks (two-buffer FFT) with several line counts
+// and block sizes, and all-terms blocks (in-place FFT); lines * element size of
+// at least 32 bytes keeps global accesses sector-sized
+std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_per_nl, int all_lines_per_nl) {
+    std::vector<YCfg> out;
+    const size_t cs = csize(h->fp32);
+    const int nls_pt[3] = {h->fp32 ? 4 : 2, h->fp32 ? 8 : 4, h->fp32 ? 16 : 8};
+    for (int nl : nls_pt) {
+        if ((size_t)(s.P2 + 2 * s.P2 * lines_per_nl * nl) * cs > 150 * 1024) continue;
+        int thrs[3] = {y_threads(s.plan2, lines_per_nl * nl), 128, 256};
+        for (int i = 0; i < 3; ++i) {
+            bool dup = false;
+            for (int k = 0; k < i; ++k) dup |= thrs[k] == thrs[i];
+            if (!dup) out.push_back(YCfg{0, nl, thrs[i]});
+        }
+    }
+    const int nls_all[2] = {h->fp32 ? 2 : 1, h->fp32 ? 4 : 2};
+    for (int nl : nls_all) {
+        const int thr = inplace_threads(s.plan2, all_lines_per_nl * nl);
+        if (thr && (size_t)(s.P2 + s.P2 * all_lines_per_nl * nl) * cs <= 150 * 1024) out.push_back(YCfg{1, nl, thr});
+    }
+    return out;
+}
+
+// average device time of `iters` launches of fn after one warm-up launch
+template <typename F>
+int time_launches(bld_handle* h, F&& fn, int iters, float* ms) {
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    int st = fn();
+    if (st == BLD_OK && cudaEventRecord(e0, h->stream) != cudaSuccess) st = BLD_ERR_CUDA;
+    for (int i = 0; i < iters && st == BLD_OK; ++i) st = fn();
+    if (st == BLD_OK && cudaEventRecord(e1, h->stream) != cudaSuccess) st = BLD_ERR_CUDA;
+    if (st == BLD_OK && cudaEventSynchronize(e1) != cudaSuccess) st = BLD_ERR_CUDA;
+    float t = 0;
+    if (st == BLD_OK) cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / iters;
+    return st == BLD_ERR_CUDA ? fail(BLD_ERR_CUDA, "autotune timing failed") : st;
+}
+
+// Picks, per physical-domain space, the fastest y-pass variants and x-kernel
+// tiling by timing every candidate on the handle's own buffers.  All candidates
+// perform the same arithmetic, so the choice changes speed, not results.
+int autotune(bld_handle* h) {
+    const char* env = getenv("BLD_NO_AUTOTUNE");
+    if (env && env[0] && env[0] != '0') return BLD_OK;
+    const int B = h->B;
+    for (int sp = 0; sp < 2; ++sp) {
+        Space& s = sp == 0 ? h->adv : h->sgs;
+        if (!s.on) continue;
+        float best = 1e30f, t = 0;
+        YCfg bi = s.inv;
+        for (const YCfg& c : y_candidates(h, s, 1, s.ntin)) {
+            s.inv = c;
+            BLD_TRY(time_launches(h, [&] { return enqueue_inv_y(h, sp, h->u, 0, B); }, 3, &t));
+            if (t < best) {
+                best = t;
+                bi = c;
+            }
+        }
+        s.inv = bi;
+        BLD_TRY(enqueue_inv_y(h, sp, h->u, 0, B));
+        best = 1e30f;
+        int byt = s.YT, bppt = s.PPT;
+        for (auto c : x_candidates(h, s, sp == 0)) {
+            s.YT = c.first;
+            s.PPT = c.second;
+            x_chunks(h, s);
+            BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
+            if (t < best) {
+                best = t;
+                byt = c.first;
+                bppt = c.second;
+            }
+        }
+        s.YT = byt;
+        s.PPT = bppt;
+        x_chunks(h, s);
+        best = 1e30f;
+        YCfg bf = s.fwd;
+        for (const YCfg& c : y_candidates(h, s, s.fsets, 3 * s.fsets)) {
+            s.fwd = c;
+            BLD_TRY(time_launches(h, [&] { return enqueue_fwd_y(h, sp, true, false, h->u, h->io2, 0, B); }, 3, &t));
+            if (t < best) {
+                best = t;
+                bf = c;
+            }
+        }
+        s.fwd = bf;
+        const char* v = getenv("BLD_VERBOSE");
+        if (v && v[0] && v[0] != '0')
+            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d | x YT=%d PPT=%d chunks=%d | fwd all=%d NL=%d thr=%d\n",
+                    sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.YT, s.PPT, s.nchunks,
+                    s.fwd.all, s.fwd.NL, s.fwd.thr);
+    }
+    CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
 }
 
 // compute_rates! (src/Processes.jl:39-62): nonlinear processes in the reference's
@@ -698,6 +857,11 @@ int setup_space(bld_handle* h, Space& s, int dealias, int e1, int e2, bool is_ad
     s.fsets = is_adv ? 1 : 2;
     tile_space(h, s, is_adv);
     if (!s.PPT) return fail(BLD_ERR_INVALID_CONFIG, "no thread tiling for physical size %d", s.P1);
+    // defaults until the autotuner runs: per-term y passes
+    s.inv = YCfg{0, h->fp32 ? 8 : 4, 256};
+    s.fwd = YCfg{0, h->fp32 ? 8 : 4, 256};
+    while (s.inv.NL > 1 && (size_t)(s.P2 + 2 * s.P2 * s.inv.NL) * csize(h->fp32) > 110 * 1024) s.inv.NL /= 2;
+    while (s.fwd.NL > 1 && (size_t)(s.P2 + 2 * s.P2 * s.fsets * s.fwd.NL) * csize(h->fp32) > 110 * 1024) s.fwd.NL /= 2;
     const size_t cs = csize(h->fp32);
     const long long layer = (long long)s.P2 * h->g.K1;
     s.min_ms = (long long)s.ntin * h->g.n3 * layer;
@@ -706,7 +870,7 @@ int setup_space(bld_handle* h, Space& s, int dealias, int e1, int e2, bool is_ad
     BLD_TRY(dalloc(h, &s.mout, (size_t)s.mout_ms * h->B * cs));
     CUDA_TRY(cudaMemset(s.mout, 0, (size_t)s.mout_ms * h->B * cs));
     const size_t sm = is_adv ? smem_adv(s, h->fp32) : smem_sgs(s, h->fp32);
-    if (sm > 200 * 1024 || smem_y(s.P2, s.NLy, h->fp32) > 200 * 1024)
+    if (sm > 200 * 1024 || (size_t)(s.P2 + 2 * s.P2 * s.fsets * s.fwd.NL) * csize(h->fp32) > 200 * 1024)
         return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size (%d, %d) needs too much shared memory", s.P1, s.P2);
     s.on = true;
     return BLD_OK;
@@ -957,6 +1121,7 @@ int32_t bld_create(const bld_config* cfg, bld_handle** out) {
         H_TRY(dalloc(h, &h->pd_mixed, (size_t)n3 * h->Pd2 * K1 * sizeof(double2)));
     }
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(BLD_ERR_CUDA, "set-up failed"));
+    H_TRY(autotune(h));
 #undef H_TRY
     *out = h;
     return BLD_OK;
@@ -1236,8 +1401,7 @@ int32_t bld_set_field_physical(bld_handle* h, int32_t m, int32_t field, const do
     Space s{};
     s.P1 = P1;
     s.P2 = P2;
-    s.NLy = pick_y(P2, false, 1);
-    s.NLf = s.NLy;
+    s.inv = s.fwd = YCfg{0, pick_y(P2, false, 1), 256};
     FwdYArgs fa{};
     fa.g = g;
     fa.P1 = P1;
@@ -1273,8 +1437,7 @@ int32_t bld_get_field_physical(bld_handle* h, int32_t m, int32_t field, double* 
     Space s{};
     s.P1 = P1;
     s.P2 = P2;
-    s.NLy = pick_y(P2, false, 1);
-    s.NLf = s.NLy;
+    s.inv = s.fwd = YCfg{0, pick_y(P2, false, 1), 256};
     InvYArgs ia{};
     ia.g = g;
     ia.P2 = P2;

@@ -189,7 +189,7 @@ __device__ __forceinline__ void stockham_stage(const cplx<R>* src, cplx<R>* dst,
 
 // Mixed-radix Stockham FFT with register codelets; same contract as fft_run.
 template <typename R, int DIR>
-__device__ cplx<R>* fft_big(cplx<R>* a, cplx<R>* b, int nlines, int ls, int ps, bool pos_fastest, const FftPlan& pl,
+__device__ __forceinline__ cplx<R>* fft_big(cplx<R>* a, cplx<R>* b, int nlines, int ls, int ps, bool pos_fastest, const FftPlan& pl,
                             const cplx<R>* __restrict__ tw) {
     using C = cplx<R>;
     const int n = pl.n;
@@ -231,4 +231,116 @@ __device__ cplx<R>* fft_big(cplx<R>* a, cplx<R>* b, int nlines, int ls, int ps, 
         Ns *= r;
     }
     return src;
+}
+
+// In-place Stockham stages: every task reads its RAD inputs into registers, the
+// block synchronises, then every task writes its RAD outputs into the same
+// buffer.  A thread holds up to inplace_tpt(RAD) tasks (4 for radix <= 4, 3 for
+// radix 6, else 1), so nlines * n / RAD <= inplace_tpt(RAD) * blockDim.x.  The
+// barriers sit outside the radix switch (one register array spans both halves).
+__host__ __device__ constexpr int inplace_tpt(int rad) { return rad <= 4 ? 4 : (rad == 6 ? 3 : 1); }
+
+template <typename R> struct InplaceMax;
+template <> struct InplaceMax<double> { static constexpr int X = 18; };
+template <> struct InplaceMax<float> { static constexpr int X = 32; };
+
+__device__ __forceinline__ void inplace_task(int w, int nb, int nlines, bool pos_fastest, int& j, int& l) {
+    if (pos_fastest) {
+        l = w / nb;
+        j = w - l * nb;
+    } else {
+        j = w / nlines;
+        l = w - j * nlines;
+    }
+}
+
+template <typename R, int RAD>
+__device__ __forceinline__ void inplace_load(cplx<R> (&x)[InplaceMax<R>::X], const cplx<R>* buf, int n, int nlines,
+                                             int ls, int ps, bool pos_fastest) {
+    constexpr int TPT = inplace_tpt(RAD);
+    static_assert(TPT * RAD <= InplaceMax<R>::X, "register array too small");
+    const int nb = n / RAD, total = nb * nlines;
+#pragma unroll
+    for (int u = 0; u < TPT; ++u) {
+        const int w = threadIdx.x + u * blockDim.x;
+        if (w < total) {
+            int j, l;
+            inplace_task(w, nb, nlines, pos_fastest, j, l);
+            const cplx<R>* in = buf + l * ls;
+#pragma unroll
+            for (int t = 0; t < RAD; ++t) x[u * RAD + t] = in[(j + t * nb) * ps];
+        }
+    }
+}
+
+template <typename R, int DIR, int RAD>
+__device__ __forceinline__ void inplace_store(cplx<R> (&x)[InplaceMax<R>::X], cplx<R>* buf, int n, int Ns, int nlines,
+                                              int ls, int ps, bool pos_fastest, const cplx<R>* __restrict__ tw) {
+    using C = cplx<R>;
+    constexpr int TPT = inplace_tpt(RAD);
+    const int nb = n / RAD, total = nb * nlines;
+    const int tws = n / (Ns * RAD);
+#pragma unroll
+    for (int u = 0; u < TPT; ++u) {
+        const int w = threadIdx.x + u * blockDim.x;
+        if (w < total) {
+            int j, l;
+            inplace_task(w, nb, nlines, pos_fastest, j, l);
+            const int k = j % Ns;
+            C(&y)[RAD] = *reinterpret_cast<C(*)[RAD]>(&x[u * RAD]);  // task u's slice, no copy
+            if (k) {
+#pragma unroll
+                for (int t = 1; t < RAD; ++t) y[t] = c_tw<DIR>(y[t], tw[k * t * tws]);
+            }
+            dft<R, RAD, DIR>(y);
+            const int od = (j - k) * RAD + k;
+            C* out = buf + l * ls;
+#pragma unroll
+            for (int q = 0; q < RAD; ++q) out[(od + q * Ns) * ps] = y[q];
+        }
+    }
+}
+
+// In-place mixed-radix FFT of `nlines` lines in `buf` (result in buf); all
+// threads must call it after a __syncthreads() that publishes buf.
+template <typename R, int DIR>
+__device__ __forceinline__ void fft_inplace(cplx<R>* buf, int nlines, int ls, int ps, bool pos_fastest,
+                                            const FftPlan& pl, const cplx<R>* __restrict__ tw) {
+    using C = cplx<R>;
+    const int n = pl.n;
+    int Ns = 1;
+    constexpr int MAXR = sizeof(R) == 4 ? 32 : BLD_FP64_MAXR;
+    C x[InplaceMax<R>::X];
+    for (int s = 0; s < pl.nst; ++s) {
+        const int r = pl.radix[s];
+        switch (r) {
+            case 2: inplace_load<R, 2>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 3: inplace_load<R, 3>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 4: inplace_load<R, 4>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 6: inplace_load<R, 6>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 8: inplace_load<R, 8>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 9: if constexpr (MAXR >= 9) inplace_load<R, 9>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 12: if constexpr (MAXR >= 12) inplace_load<R, 12>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 16: if constexpr (MAXR >= 16) inplace_load<R, 16>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 18: if constexpr (MAXR >= 18) inplace_load<R, 18>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 24: if constexpr (MAXR >= 24) inplace_load<R, 24>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            default: if constexpr (MAXR >= 32) inplace_load<R, 32>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+        }
+        __syncthreads();
+        switch (r) {
+            case 2: inplace_store<R, DIR, 2>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 3: inplace_store<R, DIR, 3>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 4: inplace_store<R, DIR, 4>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 6: inplace_store<R, DIR, 6>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 8: inplace_store<R, DIR, 8>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 9: if constexpr (MAXR >= 9) inplace_store<R, DIR, 9>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 12: if constexpr (MAXR >= 12) inplace_store<R, DIR, 12>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 16: if constexpr (MAXR >= 16) inplace_store<R, DIR, 16>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 18: if constexpr (MAXR >= 18) inplace_store<R, DIR, 18>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 24: if constexpr (MAXR >= 24) inplace_store<R, DIR, 24>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            default: if constexpr (MAXR >= 32) inplace_store<R, DIR, 32>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+        }
+        __syncthreads();
+        Ns *= r;
+    }
 }

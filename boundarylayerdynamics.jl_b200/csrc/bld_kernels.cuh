@@ -173,6 +173,116 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
     }
 }
 
+// value of spectral term `op` from the preloaded mode values of layer z (u, v, w)
+// and z+1 (u1, v1); same arithmetic as inv_term_value
+__device__ __forceinline__ double2 term_from(int op, int f, double2 u, double2 v, double2 w, double2 u1, double2 v1,
+                                             double e1, double e2, double al) {
+    switch (op) {
+        case T_DIRECT:
+            return f == 0 ? u : (f == 1 ? v : w);
+        case T_D1: {
+            const double2 q = f == 0 ? u : (f == 1 ? v : w);
+            return make_double2(-e1 * q.y, e1 * q.x);
+        }
+        case T_D2: {
+            const double2 q = f == 0 ? u : (f == 1 ? v : w);
+            return make_double2(-e2 * q.y, e2 * q.x);
+        }
+        case T_VORT1: {
+            const double dzx = -al * v.x + al * v1.x, dzy = -al * v.y + al * v1.y;
+            return make_double2(-e2 * w.y - dzx, e2 * w.x - dzy);
+        }
+        case T_VORT2: {
+            const double dzx = -al * u.x + al * u1.x, dzy = -al * u.y + al * u1.y;
+            return make_double2(dzx - (-e1 * w.y), dzy - e1 * w.x);
+        }
+        default:
+            return make_double2(-e1 * v.y - (-e2 * u.y), e1 * v.x - e2 * u.x);
+    }
+}
+
+// Inverse y pass of every term of a process at one layer: one block per
+// (k1 tile of NL lines, layer z, member); u, v, w at z and u, v at z+1 are read
+// once per mode and all nterms*NL lines are transformed together, in place.
+// grid (ceil(K1/NL), n3, members); smem tw[P2] + P2*nterms*NL complex.
+template <typename R>
+__global__ void __launch_bounds__(384) k_inv_y_all(InvYArgs a) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int NL = a.NL, nt = a.nterms, NLT = nt * NL;
+    const Geo& g = a.g;
+    const int K1 = g.K1, K2 = g.K2, k2max = g.k2max, P2 = a.P2, n3 = g.n3;
+    const int k10 = blockIdx.x * NL;
+    const int z = blockIdx.y;
+    const int m = a.m0 + blockIdx.z;
+    const bool hasI = z < n3 - 1;
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* buf = tw + P2;
+    copy_table(tw, reinterpret_cast<const C*>(a.tw), P2);
+    bool needW = false, needUp = false;
+    for (int t = 0; t < nt; ++t) {
+        needW |= (a.op[t] >= T_VORT1 && a.op[t] <= T_VORT2) || a.fld[t] == 2;
+        needUp |= (a.op[t] == T_VORT1 || a.op[t] == T_VORT2);
+    }
+    needW &= hasI;
+    needUp &= hasI;
+    const int band = P2 - K2;
+    for (int i = threadIdx.x; i < band * NLT; i += blockDim.x) {
+        const int p = k2max + 1 + i / NLT, L = i - (i / NLT) * NLT;
+        buf[p * NLT + L] = mk<R>(0, 0);
+    }
+    const double2* S = a.state + (long long)m * g.mstride;
+    const long long Fz = (long long)g.F;
+    const double2* Su = S + (long long)z * Fz;
+    const double2* Sv = S + (long long)n3 * Fz + (long long)z * Fz;
+    const double2* Sw = S + 2LL * n3 * Fz + (long long)z * Fz;
+    const int nmodes = K2 * NL;
+    constexpr int B = 4;
+    for (int i0 = 0; i0 < nmodes; i0 += B * blockDim.x) {
+        double2 u[B], v[B], w[B], u1[B], v1[B];
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            const int j = i / NL, l = i - j * NL, k1 = k10 + l;
+            u[q] = v[q] = w[q] = u1[q] = v1[q] = make_double2(0.0, 0.0);
+            if (i < nmodes && k1 < K1) {
+                const long long mo = (long long)j * K1 + k1;
+                u[q] = Su[mo];
+                v[q] = Sv[mo];
+                if (needW) w[q] = Sw[mo];
+                if (needUp) {
+                    u1[q] = Su[Fz + mo];
+                    v1[q] = Sv[Fz + mo];
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            if (i >= nmodes) continue;
+            const int j = i / NL, l = i - j * NL, k1 = k10 + l;
+            const int p = (j <= k2max) ? j : P2 - (K2 - j);
+            const bool ok = k1 < K1;
+            const double e1 = ok ? a.d1[k1] : 0.0, e2 = a.d2[j];
+            const double al = hasI ? a.alpha_i[z] : 0.0;
+            for (int t = 0; t < nt; ++t) {
+                double2 val = make_double2(0.0, 0.0);
+                if (ok && (!a.isI[t] || hasI)) val = term_from(a.op[t], a.fld[t], u[q], v[q], w[q], u1[q], v1[q], e1, e2, al);
+                buf[p * NLT + t * NL + l] = mk<R>((R)val.x, (R)val.y);
+            }
+        }
+    }
+    __syncthreads();
+    fft_inplace<R, +1>(buf, NLT, 1, NLT, false, a.plan, tw);
+    C* outbase = reinterpret_cast<C*>(a.mixed) + (long long)m * a.mixed_mstride;
+    for (int i = threadIdx.x; i < P2 * NLT; i += blockDim.x) {
+        const int y = i / NLT, L = i - y * NLT;
+        const int t = L / NL, l = L - t * NL, k1 = k10 + l;
+        if (k1 < K1 && (!a.isI[t] || hasI))
+            outbase[((long long)(t * n3 + z) * P2 + y) * K1 + k1] = buf[i];
+    }
+}
+
 // ----------------------------------------------------------- physical x kernels
 struct XArgs {
     Geo g;
@@ -907,6 +1017,136 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
                 v = make_double2(old[q].x + vx, old[q].y + vy);
             }
             du[idx] = v;
+            if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
+        }
+    }
+    if (a.check && bad) atomicOr(a.flag, 1);
+}
+
+// Forward y pass of all three rate fields at one layer: one block per (k1 tile,
+// layer, member).  Per field, contributions with prefactor 1 or D1 are summed
+// into an A line set and the D2 contribution into a B line set before one
+// in-place transform of all 3*sets*NL lines; the epilogue adds the linear terms.
+// grid (ceil(K1/NL), n3, members); smem tw[P2] + P2*NLT complex.
+template <typename R>
+__global__ void __launch_bounds__(384) k_fwd_y_all(FwdYArgs a) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int NL = a.NL;
+    const Geo& g = a.g;
+    const int K1 = g.K1, K2 = g.K2, k2max = g.k2max, P2 = a.P2, n3 = g.n3;
+    const int k10 = blockIdx.x * NL;
+    const int z = blockIdx.y;
+    const int m = a.m0 + blockIdx.z;
+    bool hasB = false;
+    for (int f = 0; f < 3; ++f)
+        for (int ci = 0; ci < a.ncontrib[f]; ++ci) hasB |= (a.c[f][ci].pref == 2);
+    const int sets = hasB ? 2 : 1;
+    const int NLF = sets * NL;       // lines per field
+    const int NLT = 3 * NLF;         // line index L = f*NLF + set*NL + l
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* buf = tw + P2;
+    copy_table(tw, reinterpret_cast<const C*>(a.tw), P2);
+    const C* base = reinterpret_cast<const C*>(a.mout) + (long long)m * a.mout_mstride;
+    const long long layer = (long long)P2 * K1;
+    const int nval = P2 * NLT;
+    constexpr int B = 4;
+    for (int i0 = 0; i0 < nval; i0 += B * blockDim.x) {
+        C v[B];
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            v[q] = mk<R>(0, 0);
+            if (i < nval) {
+                const int y = i / NLT, L = i - y * NLT;
+                const int f = L / NLF, r = L - f * NLF;
+                const bool isB = r >= NL;
+                const int k1 = k10 + (isB ? r - NL : r);
+                const int nz = (f == 2) ? n3 - 1 : n3;
+                if (k1 < K1 && z < nz) {
+                    for (int ci = 0; ci < a.ncontrib[f]; ++ci) {
+                        const FwdContrib cb = a.c[f][ci];
+                        if ((cb.pref == 2) != isB) continue;
+                        C x = base[(long long)(cb.term * n3 + z) * layer + (long long)y * K1 + k1];
+                        if (cb.pref == 1) {
+                            const R d = (R)a.d1[k1];
+                            const R tx = -d * x.y;
+                            x.y = d * x.x;
+                            x.x = tx;
+                        }
+                        v[q].x += x.x;
+                        v[q].y += x.y;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            if (i < nval) buf[i] = v[q];
+        }
+    }
+    __syncthreads();
+    fft_inplace<R, -1>(buf, NLT, 1, NLT, false, a.plan, tw);
+    // epilogue: outputs (f, j, l), state windows and old rates loaded OB at a time
+    const double2* S = a.state ? a.state + (long long)m * g.mstride : nullptr;
+    double2* dum = a.du + (long long)m * a.du_mstride;
+    bool bad = false;
+    const int nout = 3 * K2 * NL;
+    constexpr int OB = 2;
+    for (int o0 = 0; o0 < nout; o0 += OB * blockDim.x) {
+        double2 W[OB][3];
+        double2 old[OB];
+#pragma unroll
+        for (int q = 0; q < OB; ++q) {
+            const int o = o0 + q * blockDim.x + threadIdx.x;
+            const int f = o / (K2 * NL), r = o - f * (K2 * NL);
+            const int j = r / NL, l = r - j * NL, k1 = k10 + l;
+            const int nz = (f == 2) ? n3 - 1 : n3;
+            if (o < nout && k1 < K1 && z < nz) {
+                const long long idx = (long long)j * K1 + k1;
+                if (a.mode == 1 && a.lin.diff_on[f]) {
+                    const int w0 = lin_window_start(z, nz), wn = min(3, nz);
+                    const double2* Sf = S + fld_off(g, f);
+#pragma unroll
+                    for (int rr = 0; rr < 3; ++rr)
+                        if (rr < wn) W[q][rr] = Sf[(long long)(w0 + rr) * g.F + idx];
+                }
+                if (a.mode == 0) old[q] = dum[fld_off(g, f) + (long long)z * g.F + idx];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < OB; ++q) {
+            const int o = o0 + q * blockDim.x + threadIdx.x;
+            const int f = o / (K2 * NL), r = o - f * (K2 * NL);
+            const int j = r / NL, l = r - j * NL, k1 = k10 + l;
+            const int nz = (f == 2) ? n3 - 1 : n3;
+            if (o >= nout || k1 >= K1 || z >= nz) continue;
+            const int pos = (j <= k2max) ? j : P2 - (K2 - j);
+            const C X = buf[pos * NLT + f * NLF + l];
+            double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
+            if (hasB) {
+                const C Y = buf[pos * NLT + f * NLF + NL + l];
+                const double d = a.d2[j];
+                const double bx = (double)Y.x * a.inv_n, by = (double)Y.y * a.inv_n;
+                vx += -d * by;
+                vy += d * bx;
+            }
+            const long long idx = (long long)j * K1 + k1;
+            double2 v;
+            if (a.mode == 1) {
+                double2 lin;
+                if (a.lin.diff_on[f])
+                    lin = linear_terms_w(g, a.lin, W[q], lin_window_start(z, nz), f, z, j, k1, m);
+                else
+                    lin = linear_terms(g, a.lin, nullptr, f, z, j, k1, m);
+                v = make_double2(lin.x + vx, lin.y + vy);
+            } else if (a.mode == 2) {
+                v = make_double2(vx, vy);
+            } else {
+                v = make_double2(old[q].x + vx, old[q].y + vy);
+            }
+            dum[fld_off(g, f) + (long long)z * g.F + idx] = v;
             if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
         }
     }
