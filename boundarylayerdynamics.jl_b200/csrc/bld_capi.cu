@@ -63,10 +63,10 @@ int next_even_smooth(int n) {
 }
 
 // Fewest Stockham stages whose radices are register codelet sizes, then the
-// smallest largest radix (register pressure), capped at BLD_FP64_MAXR for double.
+// smallest largest radix (register pressure), capped at BLD_FP32_MAXR / BLD_FP64_MAXR.
 FftPlan make_plan(int n, bool fp32 = false) {
     static const int rads[] = {32, 24, 18, 16, 12, 9, 8, 6, 4, 3, 2};
-    const int cap = fp32 ? 32 : BLD_FP64_MAXR;
+    const int cap = fp32 ? BLD_FP32_MAXR : BLD_FP64_MAXR;
     FftPlan best{};
     best.n = n;
     int best_st = 99, best_max = 99;

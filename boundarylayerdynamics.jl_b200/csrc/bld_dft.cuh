@@ -15,10 +15,12 @@
 
 #define BLD_WTAB_SIZE 125
 
-// largest codelet compiled for double precision (register budget); single
-// precision always has all sizes up to 32
+// largest codelets compiled for double and single precision (register budget)
 #ifndef BLD_FP64_MAXR
 #define BLD_FP64_MAXR 18
+#endif
+#ifndef BLD_FP32_MAXR
+#define BLD_FP32_MAXR 18
 #endif
 
 // offsets of W_N (m = 0..N-1) in the twiddle table
@@ -198,7 +200,7 @@ __device__ __forceinline__ cplx<R>* fft_big(cplx<R>* a, cplx<R>* b, int nlines, 
     C* dst = b;
     for (int s = 0; s < pl.nst; ++s) {
         const int r = pl.radix[s];
-        constexpr int MAXR = sizeof(R) == 4 ? 32 : BLD_FP64_MAXR;
+        constexpr int MAXR = sizeof(R) == 4 ? BLD_FP32_MAXR : BLD_FP64_MAXR;
         switch (r) {
             case 2: stockham_stage<R, DIR, 2>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
             case 3: stockham_stage<R, DIR, 3>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
@@ -242,7 +244,7 @@ __host__ __device__ constexpr int inplace_tpt(int rad) { return rad <= 4 ? 4 : (
 
 template <typename R> struct InplaceMax;
 template <> struct InplaceMax<double> { static constexpr int X = 18; };
-template <> struct InplaceMax<float> { static constexpr int X = 32; };
+template <> struct InplaceMax<float> { static constexpr int X = BLD_FP32_MAXR > 18 ? BLD_FP32_MAXR : 18; };
 
 __device__ __forceinline__ void inplace_task(int w, int nb, int nlines, bool pos_fastest, int& j, int& l) {
     if (pos_fastest) {
@@ -309,7 +311,7 @@ __device__ __forceinline__ void fft_inplace(cplx<R>* buf, int nlines, int ls, in
     using C = cplx<R>;
     const int n = pl.n;
     int Ns = 1;
-    constexpr int MAXR = sizeof(R) == 4 ? 32 : BLD_FP64_MAXR;
+    constexpr int MAXR = sizeof(R) == 4 ? BLD_FP32_MAXR : BLD_FP64_MAXR;
     C x[InplaceMax<R>::X];
     for (int s = 0; s < pl.nst; ++s) {
         const int r = pl.radix[s];
