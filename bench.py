@@ -42,6 +42,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--error-steps", type=int, default=1000, help="steps of the mixed-vs-FP64 error run")
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds for the reference arm")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the ensemble, serving, tridiagonal and LES lines (run at N=1 only)")
+    ap.add_argument("--only", default="", help="comma list of extras to run (ensemble,serving,tridiag,les64,les512)")
+    ap.add_argument("--serve-budget-gb", type=float, default=48.0, help="HBM budget of the served stream")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="target length of the served stream")
     return ap.parse_args()
 
 
@@ -240,6 +245,7 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank != 0:
         return None
+    extras = {} if (args.no_extras or ws > 1) else run_extras(args, local)
 
     fp, mx = res["fp64"], res["mixed"]
     value = ws * npts / (fp["ms_per_step"] / 1e3)
@@ -276,6 +282,7 @@ def run_b200(args):
         "gpu_launches": lps * K,
         "clocks": fp["clocks"],
     }
+    out.update(extras)
     return out
 
 
@@ -294,6 +301,179 @@ def divergence_max(state, model, spec):
     dz = L3 / n3
     div = D1 * state["vel1"] + D2 * state["vel2"] + (wext[1:] - wext[:-1]) / dz
     return float(np.abs(div).max())
+
+
+# ------------------------------------------------------------------ extra workloads
+def _event_time(stream, fn):
+    """Device time (ms) of fn() bracketed by CUDA events on `stream`."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_les(name, precisions, steps, warmup, local):
+    """Single-member LES at one of the LES sizes: updates/s per precision."""
+    import torch
+    import BoundaryLayerDynamics as BLD
+    from BoundaryLayerDynamics import workloads
+    spec = workloads.CONFIGS[name]
+    u0, v0, w0 = workloads.initial_fields(spec)
+    n = spec["resolution"]
+    npts = n[0] * n[1] * n[2]
+    out = {"workload": f"half-channel LES {n[0]}x{n[1]}x{n[2]}, rough wall z0=1e-4 / free slip, "
+                       f"Smagorinsky Cs=0.1, nu=1e-5, SSPRK33 dt=1e-4"}
+    for prec in precisions:
+        m = workloads.build(spec, BLD, precision=prec, device=local)
+        BLD.initialize(m, vel1=u0, vel2=v0, vel3=w0)
+        m.prepare()
+        stream = torch.cuda.ExternalStream(m.stream)
+        m.step(warmup, spec["dt"])
+        m.sync()
+        ms = _event_time(stream, lambda: m.step_async(steps, spec["dt"]))
+        m.sync()
+        sb = state_bytes(m)
+        peak, _ = peaks()
+        ach = 8 * sb / (ms / steps * 1e-3) / 1e9
+        out[prec] = {"value": npts * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+                     "device_bytes": m.info.device_bytes,
+                     "roofline_step": {"algorithmic_bytes_per_step": 8 * sb, "achieved": ach, "unit": "GB/s",
+                                       "frac": ach / peak}}
+        del m
+    return out
+
+
+def run_ensemble(steps, warmup, local):
+    """64 uneven LES members (24 x 64^2x32, 24 x 96^2x48, 16 x 128^2x64), mixed form,
+    per-member z0 and Cs; one parent-graph launch per step for all three classes."""
+    import torch
+    from BoundaryLayerDynamics import workloads
+    from BoundaryLayerDynamics.ensemble import Ensemble
+    groups = workloads.ensemble_members()
+    ens = Ensemble.from_groups(groups, precision="mixed", device=local)
+    ens.initialize(groups, seed=100)
+    ens.prepare()
+    dt = 1e-4
+    ens.step(warmup, dt)
+    stream = torch.cuda.ExternalStream(ens.models[0].stream)
+    ms = _event_time(stream, lambda: ens.step(steps, dt))
+    # the same steps with the classes one after the other (one graph per class)
+    def serial():
+        for m in ens.models:
+            m.step_async(steps, dt)
+            m.sync()
+    ms_serial = _event_time(stream, serial)
+    sb = sum(state_bytes(m) * m.members for m in ens.models)
+    peak, _ = peaks()
+    ach = 8 * sb / (ms / steps * 1e-3) / 1e9
+    return {"workload": "ensemble of 64 LES members: 24 x 64^2x32, 24 x 96^2x48, 16 x 128^2x64; "
+                        "z0 ~ logU[1e-5,1e-3], Cs ~ U[0.08,0.16]; SSPRK33 dt=1e-4",
+            "dtype": "f32 transforms/products, f64 state+pressure",
+            "members": ens.members, "points_per_step": ens.points,
+            "value": ens.points * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "ms_per_step_classes_serial": ms_serial / steps,
+            "launches_per_step": 1,
+            "device_bytes": sum(m.info.device_bytes for m in ens.models),
+            "roofline_step": {"algorithmic_bytes_per_step": 8 * sb, "achieved": ach, "unit": "GB/s",
+                              "frac": ach / peak}}
+
+
+def run_serving(budget_gb, seconds, local):
+    """Served stream: Poisson arrivals at 80% of the measured batched capacity,
+    sizes {64^2x32, 128^2x64, 192^2x96, 256^2x128} with p {0.4, 0.3, 0.2, 0.1},
+    500 SSPRK33 steps each, seeded z0 and forcing; admission by HBM budget."""
+    from BoundaryLayerDynamics import serving as S
+    srv = S.Server.create(int(budget_gb * 2**30), precision="mixed", device=local, tick=10)
+    rate, per_req = S.calibrate_rate(srv, steps=500, load=0.8)
+    n = int(min(64, max(16, round(rate * seconds))))      # initial fields are made before the stream starts
+    reqs = S.make_requests(n, rate, seed=2024, steps=500)
+    st = srv.run(reqs)
+    st.update({
+        "workload": "served LES stream: sizes 64^2x32/128^2x64/192^2x96/256^2x128 (p .4/.3/.2/.1), "
+                    "500 SSPRK33 steps each, z0 ~ logU[1e-5,1e-3], forcing ~ U[0.5,1.5]",
+        "dtype": "f32 transforms/products, f64 state+pressure",
+        "arrival_rate_per_s": rate, "load": 0.8,
+        "service_s_per_request_at_full_pool": {f"{s[0]}^2x{s[1]}": v for s, v in per_req.items()},
+        "unit_latency": "s", "unit": UNIT, "tick_steps": 10,
+    })
+    return st
+
+
+def run_tridiag(iters, local):
+    """Batched tridiagonal pressure systems of the 512x512x256 LES alone:
+    (i) 256 x 511 = 130 816 complex systems of 256 (the pressure solve's shape),
+    (ii) 512 x 512 = 262 144 real systems of 256; staggered second-difference
+    matrix with the horizontal wavenumber shift, random right-hand sides."""
+    import numpy as np
+    import torch
+    from BoundaryLayerDynamics import _capi
+    lib = _capi.load()
+    n, L1, L2 = 256, 8 * math.pi, 4 * math.pi
+    alpha = float(n)                     # uniform grid on [0, 1]: N3 / (dx3/dzeta)
+    out = {}
+    peak, _ = peaks()
+    for kind, nk1, nk2, ebytes in (("complex", 256, 511, 16), ("real", 512, 512, 8)):
+        nsys = nk1 * nk2
+        rng = np.random.default_rng(5)
+        k1 = np.arange(nsys) % nk1
+        k2 = np.arange(nsys) // nk1 - nk2 // 2
+        shift = 4 * math.pi ** 2 * ((k1 / L1) ** 2 + (k2 / L2) ** 2) / alpha
+        diag = np.full((nsys, n), -2.0 * alpha)
+        diag[:, 0] = diag[:, -1] = -alpha
+        diag -= shift[:, None]
+        diag[(nk2 // 2) * nk1, -1] = -3 * alpha          # the k = (0, 0) system
+        beta = np.full(n - 1, alpha)
+        gam = np.empty((n, nsys))
+        g = 1.0 / diag[:, 0]
+        gam[0] = g
+        for z in range(1, n):
+            g = 1.0 / (diag[:, z] - g * beta[z - 1] ** 2)
+            gam[z] = g
+        g_d = torch.tensor(gam, device="cuda")
+        b_d = torch.tensor(np.concatenate([beta, [0.0]]), device="cuda")
+        if kind == "complex":
+            r0 = torch.tensor(rng.uniform(-1, 1, (n, nsys)) + 1j * rng.uniform(-1, 1, (n, nsys)), device="cuda")
+            fn = lib.bld_ldlt_solve_device
+        else:
+            r0 = torch.tensor(rng.uniform(-1, 1, (n, nsys)), device="cuda")
+            fn = lib.bld_ldlt_solve_real_device
+        bufs = [r0.clone() for _ in range(2)]          # alternate buffers: 2 x 0.5-1 GB, beyond L2
+        stream = torch.cuda.current_stream()
+        for b in bufs:
+            _capi.check(fn(g_d.data_ptr(), b_d.data_ptr(), b.data_ptr(), nsys, n, stream.cuda_stream))
+        def launches():
+            for i in range(iters):
+                b = bufs[i % 2]
+                _capi.check(fn(g_d.data_ptr(), b_d.data_ptr(), b.data_ptr(), nsys, n, stream.cuda_stream))
+        ms = _event_time(stream, launches) / iters
+        alg = nsys * n * (8 + 2 * ebytes)                 # gamma once, rhs read + solution written
+        ach = alg / (ms * 1e-3) / 1e9
+        out[kind] = {"systems": nsys, "n": n, "ms_per_solve": ms, "algorithmic_bytes": alg,
+                     "achieved": ach, "unit": "GB/s", "peak": peak, "frac": ach / peak,
+                     "unknowns_per_s": nsys * n / (ms * 1e-3)}
+        del g_d, b_d, r0, bufs
+    out["kernel"] = "k_ldlt_seg"
+    return out
+
+
+def run_extras(args, local):
+    want = set(filter(None, args.only.split(","))) or {"ensemble", "serving", "tridiag", "les64", "les512"}
+    out = {}
+    if "tridiag" in want:
+        out["tridiag"] = run_tridiag(20, local)
+    if "les64" in want:
+        out["les64"] = run_les("les64", ("fp64", "mixed"), 100, 5, local)
+    if "ensemble" in want:
+        out["ensemble"] = run_ensemble(max(args.steps // 2, 10), max(3, args.warmup), local)
+    if "les512" in want:
+        out["les512"] = run_les("les512", ("mixed",), 10, 3, local)
+    if "serving" in want:
+        out["serving"] = run_serving(args.serve_budget_gb, args.serve_seconds, local)
+    return out
 
 
 # ------------------------------------------------------------------ reference arm

@@ -431,6 +431,41 @@ class Model:
         _capi.check(self._lib.bld_state_device_ptr(self._h, C.byref(p)))
         return p.value
 
+    # -- member slots (ensembles and serving) ------------------------------------------
+    def set_active(self, mask):
+        """Members with a false entry are skipped by every kernel (their state is left as is)."""
+        a = np.ascontiguousarray(np.asarray(mask, dtype=np.int32))
+        if a.shape != (self.members,):
+            raise ValueError("the mask needs one entry per member")
+        _capi.check(self._lib.bld_set_active(self._h, a.ctypes.data))
+
+    def set_member_params(self, member, cs=None, z0=None, forcing=None):
+        """Replaces a member's Smagorinsky constant, lower roughness length or vel1 forcing."""
+        nan = float("nan")
+        _capi.check(self._lib.bld_set_member_params(
+            self._h, int(member), nan if cs is None else float(cs), nan if z0 is None else float(z0),
+            nan if forcing is None else float(forcing)))
+
+    def prepare_member(self, member):
+        """Initial projection and right-hand side of one member (the start of ``evolve!``)."""
+        _capi.check(self._lib.bld_prepare_member(self._h, int(member)))
+
+    def diverged_members(self):
+        """Members whose rates turned non-finite since the last query (clears the record)."""
+        out = np.zeros(self.members, dtype=np.int32)
+        _capi.check(self._lib.bld_get_diverged(self._h, out.ctypes.data))
+        return [int(m) for m in np.flatnonzero(out)]
+
+    def step_async(self, nsteps, dt, method=SSPRK33):
+        """Enqueues ``nsteps`` steps on the model's stream without waiting."""
+        _capi.check(self._lib.bld_step_async(self._h, int(nsteps), float(dt), _METHODS[method]))
+
+    @property
+    def stream(self):
+        p = C.c_void_p()
+        _capi.check(self._lib.bld_get_stream(self._h, C.byref(p)))
+        return p.value
+
 
 # --------------------------------------------------------------- API functions (the `!` forms)
 def initialize(model, member=0, **initial_conditions):

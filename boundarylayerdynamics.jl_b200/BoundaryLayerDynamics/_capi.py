@@ -90,9 +90,15 @@ SIGNATURES = {
     "bld_get_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bld_step_async": (C.c_int32, [C.c_void_p, C.c_int64, C.c_double, C.c_int32]),
     "bld_time_phases": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(BldPhaseTimes)]),
+    "bld_ensemble_step": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_int32]),
+    "bld_set_active": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "bld_set_member_params": (C.c_int32, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_double]),
+    "bld_prepare_member": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "bld_get_diverged": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "bld_project_noalloc": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32] + [C.c_void_p] * 5
                             + [C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
     "bld_ldlt_solve_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
+    "bld_ldlt_solve_real_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
 }
 
 _lib = None

@@ -1,0 +1,375 @@
+"""Served stream of LES requests with continuous batching on one device.
+
+Each request is an independent half-channel LES (rough wall below, free slip
+above, static Smagorinsky, forcing on vel1) of one of a few grid sizes, run for
+a fixed number of SSP-RK33 steps from its own seeded initial field, roughness
+length and forcing.  The server keeps one pool per size class: a batched handle
+(``Model(..., members=slots)``) whose member slots hold the requests' states
+resident in HBM.  Pool capacities are carved out of an HBM budget, and a
+request is admitted when its class has a free slot and its bytes fit in the
+budget left.  Requests that arrive while others run join at the next tick: the
+new member is loaded, projected and given its rates (``prepare_member``), and its
+slot is switched on in the device-side active mask, so the already-captured step
+graphs advance it together with the members in flight.  Every tick advances all
+busy pools by ``tick`` steps with one parent-graph launch per step.  A finished
+member's slot is switched off and reused.
+
+``Scheduler`` is the host-side admission logic alone (no device), so it can be
+tested and reasoned about on its own; ``Server`` binds it to pools of models.
+"""
+
+import math
+import sys
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import workloads
+from .ensemble import step_models
+
+# the served mix: (n, n3) size classes and their probabilities
+SIZES = ((64, 32), (128, 64), (192, 96), (256, 128))
+PROBS = (0.4, 0.3, 0.2, 0.1)
+LES_SIZE = (2 * math.pi, math.pi, 1.0)
+
+
+@dataclass
+class Request:
+    rid: int
+    size: tuple          # (n, n3): resolution (n, n, n3)
+    steps: int
+    arrival: float       # seconds after the start of the stream
+    z0: float
+    forcing: float
+    seed: int
+    status: str = "pending"      # pending, queued, running, done, rejected, diverged
+    error: str = ""
+    admitted: float = float("nan")
+    done: float = float("nan")
+    result: dict = None
+    fields: tuple = field(default=None, repr=False)   # physical (u, v, w) initial field
+
+    @property
+    def points(self):
+        n, n3 = self.size
+        return n * n * n3
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+def spec_for(size, z0=workloads.LES_Z0, forcing=1.0, seed=0, dt=1e-4, steps=500):
+    n, n3 = size
+    return workloads.les_spec(n, n3, LES_SIZE, seed=seed, z0=z0, forcing=forcing, dt=dt, steps=steps)
+
+
+def poisson_arrivals(rate, n, seed):
+    """Arrival times of a seeded Poisson process of ``rate`` per second."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+def make_requests(n, rate, seed=7, sizes=SIZES, probs=PROBS, steps=500, materialize=True):
+    """``n`` seeded requests: Poisson arrivals, sizes drawn with ``probs``,
+    z0 ~ logU[1e-5, 1e-3] and vel1 forcing ~ U[0.5, 1.5] per request."""
+    rng = np.random.default_rng(seed + 1)
+    times = poisson_arrivals(rate, n, seed)
+    idx = rng.choice(len(sizes), size=n, p=np.asarray(probs) / np.sum(probs))
+    z0 = np.exp(rng.uniform(math.log(1e-5), math.log(1e-3), size=n))
+    forcing = rng.uniform(0.5, 1.5, size=n)
+    reqs = []
+    for i in range(n):
+        r = Request(rid=i, size=tuple(sizes[idx[i]]), steps=steps, arrival=float(times[i]), z0=float(z0[i]),
+                    forcing=float(forcing[i]), seed=seed * 1000 + i)
+        if materialize:
+            r.fields = initial_fields(r)
+        reqs.append(r)
+    return reqs
+
+
+def initial_fields(req):
+    """The request's seeded log-law-plus-noise initial field on its default grid."""
+    return workloads.initial_fields(spec_for(req.size, z0=req.z0, forcing=req.forcing, seed=req.seed))
+
+
+def percentile(values, q):
+    """Nearest-rank percentile (q in [0, 100])."""
+    v = np.sort(np.asarray(values, dtype=float))
+    if v.size == 0:
+        return float("nan")
+    k = max(0, int(math.ceil(q / 100.0 * v.size)) - 1)
+    return float(v[k])
+
+
+class Scheduler:
+    """Slots per size class, an HBM budget and a FIFO queue (host logic only).
+
+    ``capacity[size]`` slots exist per class and each occupied slot holds
+    ``slot_bytes[size]`` bytes of the budget.  Requests are admitted in arrival
+    order; a request whose class is full (or whose bytes do not fit the budget
+    left) waits without blocking requests of other classes behind it.  A request
+    of an unknown size, or one that could never fit, is rejected at submission.
+    """
+
+    def __init__(self, capacity, slot_bytes, budget):
+        self.capacity = dict(capacity)
+        self.slot_bytes = dict(slot_bytes)
+        self.budget = int(budget)
+        self.free = {s: list(range(c)) for s, c in self.capacity.items()}
+        self.running = {s: {} for s in self.capacity}     # size -> slot -> [request, steps left]
+        self.queue = []
+        self.resident = 0
+        self.peak_resident = 0
+
+    def submit(self, req):
+        if req.size not in self.capacity or self.capacity[req.size] < 1:
+            req.status, req.error = "rejected", f"no pool serves size {req.size}"
+            return False
+        if self.slot_bytes[req.size] > self.budget:
+            req.status, req.error = "rejected", "request exceeds the HBM budget"
+            return False
+        if req.steps < 1:
+            req.status, req.error = "rejected", "a request needs at least one step"
+            return False
+        req.status = "queued"
+        self.queue.append(req)
+        return True
+
+    def admit(self):
+        """Pops every queued request that fits now; returns [(request, size, slot)]."""
+        out, keep = [], []
+        for r in self.queue:
+            need = self.slot_bytes[r.size]
+            if self.free[r.size] and self.resident + need <= self.budget:
+                slot = self.free[r.size].pop(0)
+                self.running[r.size][slot] = [r, r.steps]
+                self.resident += need
+                self.peak_resident = max(self.peak_resident, self.resident)
+                r.status = "running"
+                out.append((r, r.size, slot))
+            else:
+                keep.append(r)
+        self.queue = keep
+        return out
+
+    def busy(self):
+        return [s for s in self.capacity if self.running[s]]
+
+    def mask(self, size):
+        m = np.zeros(self.capacity[size], dtype=np.int32)
+        for slot in self.running[size]:
+            m[slot] = 1
+        return m
+
+    def next_tick(self, tick):
+        """Steps the next tick may take without running any member past its end."""
+        left = [v[1] for s in self.capacity for v in self.running[s].values()]
+        return min([tick] + left) if left else 0
+
+    def advance(self, nsteps):
+        """Counts ``nsteps`` steps for every running request; returns the finished ones."""
+        done = []
+        for s in self.capacity:
+            for slot, v in list(self.running[s].items()):
+                v[1] -= nsteps
+                if v[1] <= 0:
+                    done.append((v[0], s, slot))
+        return done
+
+    def release(self, size, slot):
+        r, _ = self.running[size].pop(slot)
+        self.free[size].append(slot)
+        self.free[size].sort()
+        self.resident -= self.slot_bytes[size]
+        return r
+
+
+def plan_capacity(budget, slot_bytes, probs, max_slots=64):
+    """Slots per class from the HBM budget.  Members of every class advance
+    together (one step graph per tick for all busy pools), so a request's time in
+    the system hardly depends on its size, and by Little's law the number of
+    resident requests of a class is proportional to its arrival probability:
+    slots are given in proportion to the probabilities, scaled to fill the budget,
+    at least one per class."""
+    sizes = list(slot_bytes)
+    scale = budget / sum(probs[s] * slot_bytes[s] for s in sizes)
+    cap = {s: max(1, min(max_slots, int(probs[s] * scale))) for s in sizes}
+    while sum(cap[s] * slot_bytes[s] for s in sizes) > budget:
+        s = max((s for s in sizes if cap[s] > 1), key=lambda s: cap[s] * slot_bytes[s], default=None)
+        if s is None:
+            raise ValueError("the HBM budget does not hold one slot of every size class")
+        cap[s] -= 1
+    return cap
+
+
+def estimate_slot_bytes(size, precision="mixed", device=0, members=2):
+    """Device bytes per member slot of a pool of ``size``: the difference of two
+    probe handles with ``members`` and one member (autotuning skipped)."""
+    api = sys.modules[__package__]
+    import os
+    old = os.environ.get("BLD_NO_AUTOTUNE")
+    os.environ["BLD_NO_AUTOTUNE"] = "1"
+    try:
+        one = workloads.build(spec_for(size), api, precision=precision, members=1, device=device)
+        b1 = one.info.device_bytes
+        del one
+        more = workloads.build(spec_for(size), api, precision=precision, members=members, device=device)
+        bm = more.info.device_bytes
+        del more
+    finally:
+        if old is None:
+            del os.environ["BLD_NO_AUTOTUNE"]
+        else:
+            os.environ["BLD_NO_AUTOTUNE"] = old
+    per = (bm - b1) / (members - 1)
+    return int(per), int(b1 - per)
+
+
+class Server:
+    """Continuous-batching server over one pool per size class.
+
+    ``pools``: size -> model-like object with ``members`` slots and the slot API
+    (``set_field``, ``set_member_params``, ``prepare_member``, ``set_active``,
+    ``get_state``, ``diverged_members``).  ``stepper(models, nsteps)`` advances the
+    given pools (default: one parent-graph launch per step for all of them).
+    """
+
+    def __init__(self, pools, slot_bytes, budget, dt=1e-4, tick=10, stepper=None, keep_results=False,
+                 clock=time.perf_counter, sleep=time.sleep):
+        self.pools = dict(pools)
+        self.sched = Scheduler({s: p.members for s, p in self.pools.items()}, slot_bytes, budget)
+        self.dt = float(dt)
+        self.tick = int(tick)
+        self.stepper = stepper or (lambda models, n: step_models(models, n, self.dt))
+        self.keep_results = keep_results
+        self.clock = clock
+        self.sleep = sleep
+        self.ticks = 0
+        self.launch_steps = 0
+        for p in self.pools.values():
+            p.set_active(np.zeros(p.members, dtype=np.int32))
+
+    @classmethod
+    def create(cls, budget, sizes=SIZES, probs=PROBS, precision="mixed", device=0, capacity=None, **kw):
+        """Pools for ``sizes`` sized from the HBM ``budget`` (bytes)."""
+        api = sys.modules[__package__]
+        est = {tuple(s): estimate_slot_bytes(tuple(s), precision, device) for s in sizes}
+        slot_bytes = {s: v[0] for s, v in est.items()}
+        if capacity is None:
+            fixed = sum(v[1] for v in est.values())
+            capacity = plan_capacity(budget - fixed, slot_bytes, dict(zip(map(tuple, sizes), probs)))
+        pools = {s: workloads.build(spec_for(s), api, precision=precision, members=capacity[s], device=device)
+                 for s in est}
+        return cls(pools, slot_bytes, budget, **kw)
+
+    def _load(self, req, size, slot):
+        pool = self.pools[size]
+        u, v, w = req.fields if req.fields is not None else initial_fields(req)
+        pool.set_field("vel1", u, member=slot)
+        pool.set_field("vel2", v, member=slot)
+        pool.set_field("vel3", w, member=slot)
+        pool.set_member_params(slot, z0=req.z0, forcing=req.forcing)
+        pool.prepare_member(slot)
+
+    def _fail(self, req, size, slot, status, msg):
+        req.status, req.error = status, msg
+        req.done = self.clock() - self.t0
+        self.sched.release(size, slot)
+
+    def run(self, requests):
+        """Serves ``requests`` (arrival times relative to the call); returns the statistics."""
+        from ._capi import DivergenceError
+        pending = sorted(requests, key=lambda r: r.arrival)
+        self.t0 = self.clock()
+        i = 0
+        while i < len(pending) or self.sched.queue or self.sched.busy():
+            now = self.clock() - self.t0
+            while i < len(pending) and pending[i].arrival <= now:
+                self.sched.submit(pending[i])
+                i += 1
+            changed = set()
+            for req, size, slot in self.sched.admit():
+                req.admitted = self.clock() - self.t0
+                try:
+                    self._load(req, size, slot)
+                except DivergenceError as e:
+                    self.pools[size].diverged_members()
+                    self._fail(req, size, slot, "diverged", str(e))
+                    continue
+                changed.add(size)
+            for size in changed:
+                self.pools[size].set_active(self.sched.mask(size))
+            busy = self.sched.busy()
+            if not busy:
+                if i < len(pending):
+                    self.sleep(max(0.0, pending[i].arrival - (self.clock() - self.t0)))
+                continue
+            n = self.sched.next_tick(self.tick)
+            models = [self.pools[s] for s in busy]
+            try:
+                self.stepper(models, n)
+            except DivergenceError:
+                for s in busy:
+                    for slot in self.pools[s].diverged_members():
+                        if slot in self.sched.running[s]:
+                            r = self.sched.running[s][slot][0]
+                            self._fail(r, s, slot, "diverged", "The simulation has diverged.")
+                    self.pools[s].set_active(self.sched.mask(s))
+            self.ticks += 1
+            self.launch_steps += n
+            finished = self.sched.advance(n)
+            for req, size, slot in finished:
+                if self.keep_results:
+                    req.result = self.pools[size].get_state(slot)
+                req.done = self.clock() - self.t0
+                req.status = "done"
+                self.sched.release(size, slot)
+            for size in {s for _, s, _ in finished}:
+                self.pools[size].set_active(self.sched.mask(size))
+        return self.stats(requests)
+
+    def stats(self, requests):
+        done = [r for r in requests if r.status == "done"]
+        lat = [r.latency for r in done]
+        t_end = max([r.done for r in done], default=0.0)
+        t_start = min([r.arrival for r in requests], default=0.0)
+        span = max(t_end - t_start, 1e-12)
+        upd = sum(r.points * r.steps for r in done)
+        return {
+            "requests": len(requests),
+            "completed": len(done),
+            "rejected": sum(r.status == "rejected" for r in requests),
+            "diverged": sum(r.status == "diverged" for r in requests),
+            "p50_latency_s": percentile(lat, 50),
+            "p99_latency_s": percentile(lat, 99),
+            "mean_latency_s": float(np.mean(lat)) if lat else float("nan"),
+            "makespan_s": span,
+            "updates_per_s": upd / span,
+            "ticks": self.ticks,
+            "capacity": {f"{s[0]}^2x{s[1]}": self.sched.capacity[s] for s in self.sched.capacity},
+            "peak_resident_bytes": self.sched.peak_resident,
+            "budget_bytes": self.sched.budget,
+        }
+
+
+def calibrate_rate(server, probs=PROBS, steps=500, load=0.8, sample_steps=20):
+    """Arrival rate that offers ``load`` of the pools' measured batched capacity:
+    per class, the time of ``sample_steps`` steps with every slot busy, divided by
+    the slots, gives the device time of one request; the rate is
+    ``load / sum(p_c * steps * t_c)``."""
+    per_request = {}
+    for size, pool in server.pools.items():
+        pool.set_active(np.ones(pool.members, dtype=np.int32))
+        for m in range(pool.members):
+            pool.set_state({}, member=m)
+            pool.prepare_member(m)
+        server.stepper([pool], 2)
+        t = time.perf_counter()
+        server.stepper([pool], sample_steps)
+        dt = time.perf_counter() - t
+        pool.set_active(np.zeros(pool.members, dtype=np.int32))
+        per_request[size] = dt / sample_steps * steps / pool.members
+    mean = sum(p * per_request[s] for s, p in zip(server.pools, probs))
+    return load / mean, per_request

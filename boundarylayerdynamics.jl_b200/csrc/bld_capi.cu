@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -156,6 +157,13 @@ struct bld_handle {
     double *lc2 = nullptr, *li2 = nullptr, *wall = nullptr, *src = nullptr, *mean_val = nullptr;
     int* flag = nullptr;
     int* flag_host = nullptr;
+    std::vector<int> diverged;   // members whose rates turned non-finite since the last bld_get_diverged
+    int* active = nullptr;        // [members] device mask of active ensemble slots
+    std::vector<int> active_host;
+    bool mask_on = false;        // the active mask applies to whole-ensemble steps only
+    int proj_variant = 1;        // 0: column kernel, 1/2: z-segmented kernel (autotuned)
+    std::vector<double> tab_dx3c, tab_dx3i, tab_x3c, tab_x3i;  // copies of the mapping tables
+    std::vector<double> member_cs, member_z0;                  // current per-member SGS parameters
     std::map<int, DevTw> tw;
     Space adv, sgs;
     // physical-domain transforms at the default size
@@ -170,6 +178,8 @@ struct bld_handle {
     bool ab2_started = false;
     double ab2_dt = 0;
     std::map<std::pair<int, double>, cudaGraphExec_t> graphs;
+    std::map<std::pair<int, double>, cudaGraph_t> graph_src;   // kept for ensemble parent graphs
+    std::map<std::vector<const void*>, cudaGraphExec_t> ens_graphs;  // parent graphs led by this handle
     size_t bytes = 0;
 };
 
@@ -439,6 +449,7 @@ int enqueue_inv_y_R(bld_handle* h, int sp, const double2* state, int m0, int nm)
     ia.d1 = h->d1;
     ia.d2 = h->d2;
     ia.alpha_i = h->alpha_i;
+    ia.active = h->mask_on ? h->active : nullptr;
     ia.plan = s.plan2;
     ia.tw = twp(h, s.P2, sizeof(R) == 4);
     if (sp == 0) {  // u, v, w, vort1, vort2, vort3 (src/processes/momentum_advection.jl:40-41)
@@ -490,6 +501,7 @@ int enqueue_x_R(bld_handle* h, int sp, int m0, int nm) {
     xa.dyn_hi = h->dyn_hi;
     xa.w_lo = h->w_lo;
     xa.w_hi = h->w_hi;
+    xa.active = h->mask_on ? h->active : nullptr;
     return sp == 0 ? launch_adv_x<R>(h, s, xa, nm) : launch_sgs_x<R>(h, s, xa, nm);
 }
 
@@ -534,6 +546,7 @@ int enqueue_fwd_y_R(bld_handle* h, int sp, bool first, bool last, const double2*
     fa.fields = 3;
     fa.field0 = 0;
     fa.m0 = m0;
+    fa.active = h->mask_on ? h->active : nullptr;
     fa.plan = s.plan2;
     fa.tw = twp(h, s.P2, sizeof(R) == 4);
     return launch_fwd_y<R>(h, s, fa, nm);
@@ -550,6 +563,7 @@ int enqueue_linear(bld_handle* h, const double2* state, double2* du, int m0, int
     fa.lin = h->lin;
     fa.flag = h->flag;
     fa.m0 = m0;
+    fa.active = h->mask_on ? h->active : nullptr;
     dim3 grid((h->g.F + 255) / 256, h->g.n3, 3 * nm);
     k_linear<<<grid, 256, 0, h->stream>>>(fa);
     CUDA_TRY(cudaGetLastError());
@@ -566,6 +580,9 @@ int enqueue_fwd_y(bld_handle* h, int sp, bool first, bool last, const double2* s
     return h->fp32 ? enqueue_fwd_y_R<float>(h, sp, first, last, st, du, m0, nm)
                    : enqueue_fwd_y_R<double>(h, sp, first, last, st, du, m0, nm);
 }
+
+int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const double2* t, const double2* du,
+                    const double2* dp, double2* out, int m0, int nm);
 
 // ------------------------------------------------------------------ autotuner
 // y-pass candidates: per-term blocks (two-buffer FFT) with several line counts
@@ -666,7 +683,23 @@ int autotune(bld_handle* h) {
                     sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.YT, s.PPT, s.nchunks,
                     s.fwd.all, s.fwd.NL, s.fwd.thr);
     }
-    CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    if (h->cfg.pressure && h->g.n3 <= 256) {
+        float best = 1e30f, t = 0;
+        int bv = h->proj_variant;
+        for (int v = 0; v < 3; ++v) {
+            h->proj_variant = v;
+            BLD_TRY(time_launches(h, [&] { return enqueue_project(h, S_NONE, 0.0, h->u, nullptr, nullptr, nullptr, h->io, 0, B); },
+                                  3, &t));
+            if (t < best) {
+                best = t;
+                bv = v;
+            }
+        }
+        h->proj_variant = bv;
+        const char* v = getenv("BLD_VERBOSE");
+        if (v && v[0] && v[0] != '0') fprintf(stderr, "bld autotune projection: variant %d\n", bv);
+    }
+    CUDA_TRY(cudaMemsetAsync(h->flag, 0, h->B * sizeof(int), h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return BLD_OK;
 }
@@ -699,6 +732,7 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
     ProjArgs a{};
     a.g = h->g;
     a.m0 = m0;
+    a.active = h->mask_on ? h->active : nullptr;
     a.u = u;
     a.t = t;
     a.du = du;
@@ -721,16 +755,22 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
     const bool any_mean = h->cfg.mean[0] || h->cfg.mean[1];
     if (!a.pressure && !any_mean && kind == S_NONE && out == u) return BLD_OK;
     const int n3 = h->g.n3;
-    if (a.pressure && n3 <= 256) {
-        // z-segmented solve: <= 16 segments of <= 8 (n3 <= 128) or <= 16 layers
+    if (a.pressure && n3 <= 256 && h->proj_variant > 0) {
+        // z-segmented solve: <= 16 segments of <= 8 (n3 <= 128) or <= 16 layers;
+        // 16 modes side by side (256-byte rows), <= 256 threads; variant 1 lets the
+        // compiler use all registers it wants, variant 2 caps them for 2 blocks per SM
         const int lmax = n3 <= 128 ? 8 : 16;
         const int ns = std::max(1, std::min(16, (n3 + lmax - 1) / lmax));
-        dim3 grid((h->g.F + 31) / 32, nm);
-        dim3 block(32, ns);
-        if (lmax == 8)
-            k_project_seg<8><<<grid, block, 0, h->stream>>>(a);
+        dim3 grid((h->g.F + 15) / 16, nm);
+        dim3 block(16, ns);
+        if (lmax == 8 && h->proj_variant == 1)
+            k_project_seg<8, 1><<<grid, block, 0, h->stream>>>(a);
+        else if (lmax == 8)
+            k_project_seg<8, 2><<<grid, block, 0, h->stream>>>(a);
+        else if (h->proj_variant == 1)
+            k_project_seg<16, 1><<<grid, block, 0, h->stream>>>(a);
         else
-            k_project_seg<16><<<grid, block, 0, h->stream>>>(a);
+            k_project_seg<16, 2><<<grid, block, 0, h->stream>>>(a);
     } else {
         dim3 grid((h->g.F + 127) / 128, nm);
         k_project<<<grid, 128, 0, h->stream>>>(a);
@@ -742,6 +782,11 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
 // one time step of `method` (perform_step! + the trailing rate!, src/ODEMethods.jl:217-234)
 int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first) {
     const int B = h->B;
+    struct MaskScope {
+        bld_handle* h;
+        ~MaskScope() { h->mask_on = false; }
+    } scope{h};
+    h->mask_on = true;
     switch (method) {
         case BLD_EULER:
             BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->u, 0, B));
@@ -781,12 +826,41 @@ int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first) {
     return BLD_OK;
 }
 
+// segmented batched LDL^T solve: LMAX layers per thread, NS = ceil(n / LMAX)
+// segments (<= 64 for n <= 1024), LANES systems per block with LANES * NS <= 512
+template <typename T>
+int ldlt_launch(const double* gamma, const double* beta, T* rhs, long long nsys, int n, cudaStream_t st) {
+    if (n > 1024) return fail(BLD_ERR_ARGUMENT, "tridiagonal systems longer than 1024 are not supported");
+    const int lmax = n <= 256 ? 8 : 16;
+    const int NS = (n + lmax - 1) / lmax;   // <= 64
+    int lanes = 32;
+    while (lanes * NS > 512) lanes /= 2;    // >= 8 lanes: rows of >= 64 bytes
+    const dim3 block(lanes, NS);
+    const long long nb = (nsys + lanes - 1) / lanes;
+    if (nb > 2147483647LL) return fail(BLD_ERR_ARGUMENT, "too many systems");
+    const size_t smem = (size_t)(n & ~1) * sizeof(double) + (size_t)NS * lanes * (sizeof(T) + sizeof(double));
+    if (lmax == 8)
+        k_ldlt_seg<T, 8><<<(unsigned)nb, block, smem, st>>>(gamma, beta, rhs, nsys, n);
+    else
+        k_ldlt_seg<T, 16><<<(unsigned)nb, block, smem, st>>>(gamma, beta, rhs, nsys, n);
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+// reads the per-member non-finite flags; members that diverged are remembered
+// (bld_get_diverged) and the flags are cleared
 int check_flag(bld_handle* h) {
-    CUDA_TRY(cudaMemcpyAsync(h->flag_host, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->flag_host, h->flag, h->B * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
-    if (*h->flag_host) {
-        *h->flag_host = 0;
-        CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    bool any = false;
+    for (int m = 0; m < h->B; ++m)
+        if (h->flag_host[m]) {
+            any = true;
+            h->diverged[m] = 1;
+            h->flag_host[m] = 0;
+        }
+    if (any) {
+        CUDA_TRY(cudaMemsetAsync(h->flag, 0, h->B * sizeof(int), h->stream));
         CUDA_TRY(cudaStreamSynchronize(h->stream));
         return fail(BLD_ERR_DIVERGED, "The simulation has diverged.");
     }
@@ -876,12 +950,56 @@ int setup_space(bld_handle* h, Space& s, int dealias, int e1, int e2, bool is_ad
     return BLD_OK;
 }
 
+// Smagorinsky length scales squared and wall-model factors of one member
+// (src/processes/static_smagorinsky.jl:44-123): l = Cs cbrt(D1 D2 D3), wall
+// damping (l^-N + (kappa z)^-N)^(-1/N), strain factor 1/(2 dz log(dz/z0)) and
+// stress factor -kappa^2/log^2(dz/z0) (upper-wall factors negated).
+void member_sgs_tables(const bld_handle* h, double cs, double z0lo, double* lc2, double* li2, double* wall4) {
+    const bld_config* cfg = &h->cfg;
+    const Geo& g = h->g;
+    const int n3 = g.n3;
+    const double D1 = cfg->l1 / (2.0 * g.k1max + 2.0), D2 = cfg->l2 / (2.0 * g.k2max + 2.0);
+    auto ml = [&](double x3) {
+        double lo = INFINITY, hi = INFINITY;
+        if (cfg->wall_kind[0] == BLD_WALL_ROUGH) lo = (x3 - cfg->x3_min) * cfg->wall_kappa[0];
+        if (cfg->wall_kind[1] == BLD_WALL_ROUGH) hi = (cfg->x3_max - x3) * cfg->wall_kappa[1];
+        return std::min(lo, hi);
+    };
+    const double N = cfg->sgs_wall_damping_exponent;
+    for (int i = 0; i < n3; ++i) {
+        double l = cs * std::cbrt(D1 * D2 * (h->tab_dx3c[i] / n3));
+        if (cfg->sgs_wall_damping) l = std::pow(std::pow(l, -N) + std::pow(ml(h->tab_x3c[i]), -N), -1.0 / N);
+        lc2[i] = l * l;
+    }
+    for (int i = 0; i < n3 - 1; ++i) {
+        double l = cs * std::cbrt(D1 * D2 * (h->tab_dx3i[i + 1] / n3));
+        if (cfg->sgs_wall_damping) l = std::pow(std::pow(l, -N) + std::pow(ml(h->tab_x3i[i]), -N), -1.0 / N);
+        li2[i] = l * l;
+    }
+    const double dxb = h->tab_x3c[0] - cfg->x3_min, dxa = cfg->x3_max - h->tab_x3c[n3 - 1];
+    double fs[2] = {0, 0}, ft[2] = {0, 0};
+    for (int sd = 0; sd < 2; ++sd) {
+        if (cfg->wall_kind[sd] != BLD_WALL_ROUGH) continue;
+        const double dx = sd == 0 ? dxb : dxa;
+        const double z0 = sd == 0 ? z0lo : cfg->wall_z0[1];
+        const double lg = std::log(dx / z0);
+        fs[sd] = 1.0 / (2.0 * dx * lg);
+        ft[sd] = -(cfg->wall_kappa[sd] * cfg->wall_kappa[sd]) / (lg * lg);
+    }
+    wall4[0] = fs[0];
+    wall4[1] = -fs[1];
+    wall4[2] = ft[0];
+    wall4[3] = -ft[1];
+}
+
 void free_handle(bld_handle* h) {
     if (!h) return;
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : h->graph_src) cudaGraphDestroy(kv.second);
+    for (auto& kv : h->ens_graphs) cudaGraphExecDestroy(kv.second);
     void* ptrs[] = {h->u, h->t, h->du, h->dp, h->io, h->io2, h->pscr, h->gamma, h->d1, h->d2, h->DD1, h->DD2,
                     h->alpha_c, h->alpha_i, h->alpha_ext, h->mean_w, h->lc2, h->li2, h->wall, h->src,
-                    h->mean_val, h->flag, h->adv.min, h->adv.mout, h->sgs.min, h->sgs.mout, h->pd_buf, h->pd_mixed};
+                    h->mean_val, h->flag, h->active, h->adv.min, h->adv.mout, h->sgs.min, h->sgs.mout, h->pd_buf, h->pd_mixed};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& kv : h->tw) {
@@ -932,6 +1050,8 @@ int32_t bld_create(const bld_config* cfg, bld_handle** out) {
     BLD_TRY(set_smem_limits());
     bld_handle* h = new bld_handle();
     h->cfg = *cfg;
+    h->cfg.dx3_c = h->cfg.dx3_i = h->cfg.x3_c = h->cfg.x3_i = nullptr;  // caller memory: copied below
+    h->cfg.member_cs = h->cfg.member_z0_lower = h->cfg.member_source1 = nullptr;
     h->device = cfg->device;
     h->B = cfg->members;
     h->fp32 = (cfg->precision == BLD_MIXED);
@@ -965,10 +1085,14 @@ int32_t bld_create(const bld_config* cfg, bld_handle** out) {
     for (void* p : {(void*)h->u, (void*)h->t, (void*)h->du, (void*)h->dp, (void*)h->io, (void*)h->io2})
         if (cudaMemset(p, 0, sbytes) != cudaSuccess) return bail(fail(BLD_ERR_CUDA, "cudaMemset failed"));
     if (cfg->pressure) H_TRY(dalloc(h, (void**)&h->pscr, (size_t)B * n3 * g.F * sizeof(double2)));
-    H_TRY(dalloc(h, (void**)&h->flag, sizeof(int)));
-    if (cudaMemset(h->flag, 0, sizeof(int)) != cudaSuccess) return bail(fail(BLD_ERR_CUDA, "cudaMemset failed"));
-    if (cudaMallocHost(&h->flag_host, sizeof(int)) != cudaSuccess) return bail(fail(BLD_ERR_CUDA, "cudaMallocHost failed"));
-    *h->flag_host = 0;
+    H_TRY(dalloc(h, (void**)&h->flag, h->B * sizeof(int)));
+    h->active_host.assign(B, 1);
+    H_TRY(upload(h, &h->active, h->active_host));
+    if (cudaMemset(h->flag, 0, h->B * sizeof(int)) != cudaSuccess) return bail(fail(BLD_ERR_CUDA, "cudaMemset failed"));
+    if (cudaMallocHost(&h->flag_host, h->B * sizeof(int)) != cudaSuccess)
+        return bail(fail(BLD_ERR_CUDA, "cudaMallocHost failed"));
+    for (int m = 0; m < h->B; ++m) h->flag_host[m] = 0;
+    h->diverged.assign(h->B, 0);
 
     // ---- wavenumber factors (src/Domains.jl:285-288, src/derivatives.jl:21-27)
     const double TWO_PI = 2.0 * M_PI;
@@ -1064,44 +1188,19 @@ int32_t bld_create(const bld_config* cfg, bld_handle** out) {
 
     // ---- SGS length scales and wall model (src/processes/static_smagorinsky.jl:44-123)
     std::vector<double> lc2((size_t)B * n3, 0.0), li2((size_t)B * (n3 - 1), 0.0), wall((size_t)4 * B, 0.0);
+    h->tab_dx3c.assign(cfg->dx3_c, cfg->dx3_c + n3);
+    h->tab_dx3i.assign(cfg->dx3_i, cfg->dx3_i + n3 + 1);
+    h->tab_x3c.assign(cfg->x3_c, cfg->x3_c + n3);
+    h->tab_x3i.assign(cfg->x3_i, cfg->x3_i + n3 - 1);
     if (cfg->sgs) {
-        const double D1 = cfg->l1 / (2.0 * g.k1max + 2.0), D2 = cfg->l2 / (2.0 * g.k2max + 2.0);
         h->dyn_lo = cfg->wall_kind[0] == BLD_WALL_ROUGH;
         h->dyn_hi = cfg->wall_kind[1] == BLD_WALL_ROUGH;
         for (int m = 0; m < B; ++m) {
             const double cs = cfg->member_cs ? cfg->member_cs[m] : cfg->sgs_cs;
             const double z0lo = (cfg->member_z0_lower) ? cfg->member_z0_lower[m] : cfg->wall_z0[0];
-            auto ml = [&](double x3) {
-                double lo = INFINITY, hi = INFINITY;
-                if (cfg->wall_kind[0] == BLD_WALL_ROUGH) lo = (x3 - cfg->x3_min) * cfg->wall_kappa[0];
-                if (cfg->wall_kind[1] == BLD_WALL_ROUGH) hi = (cfg->x3_max - x3) * cfg->wall_kappa[1];
-                return std::min(lo, hi);
-            };
-            const double N = cfg->sgs_wall_damping_exponent;
-            for (int i = 0; i < n3; ++i) {
-                double l = cs * std::cbrt(D1 * D2 * (cfg->dx3_c[i] / n3));
-                if (cfg->sgs_wall_damping) l = std::pow(std::pow(l, -N) + std::pow(ml(cfg->x3_c[i]), -N), -1.0 / N);
-                lc2[(size_t)m * n3 + i] = l * l;
-            }
-            for (int i = 0; i < n3 - 1; ++i) {
-                double l = cs * std::cbrt(D1 * D2 * (cfg->dx3_i[i + 1] / n3));
-                if (cfg->sgs_wall_damping) l = std::pow(std::pow(l, -N) + std::pow(ml(cfg->x3_i[i]), -N), -1.0 / N);
-                li2[(size_t)m * (n3 - 1) + i] = l * l;
-            }
-            const double dxb = cfg->x3_c[0] - cfg->x3_min, dxa = cfg->x3_max - cfg->x3_c[n3 - 1];
-            double fs[2] = {0, 0}, ft[2] = {0, 0};
-            for (int s = 0; s < 2; ++s) {
-                if (cfg->wall_kind[s] != BLD_WALL_ROUGH) continue;
-                const double dx = s == 0 ? dxb : dxa;
-                const double z0 = s == 0 ? z0lo : cfg->wall_z0[1];
-                const double lg = std::log(dx / z0);
-                fs[s] = 1.0 / (2.0 * dx * lg);
-                ft[s] = -(cfg->wall_kappa[s] * cfg->wall_kappa[s]) / (lg * lg);
-            }
-            wall[4 * m + 0] = fs[0];
-            wall[4 * m + 1] = -fs[1];
-            wall[4 * m + 2] = ft[0];
-            wall[4 * m + 3] = -ft[1];
+            member_sgs_tables(h, cs, z0lo, &lc2[(size_t)m * n3], &li2[(size_t)m * (n3 - 1)], &wall[4 * (size_t)m]);
+            h->member_cs.push_back(cs);
+            h->member_z0.push_back(z0lo);
         }
     }
     H_TRY(upload(h, &h->lc2, lc2));
@@ -1227,6 +1326,31 @@ int32_t bld_prepare(bld_handle* h) {
 
 static int step_impl(bld_handle* h, int64_t nsteps, double dt, int32_t method);
 
+// captures one step of `method` (regular steps; AB2 after its start-up step) into
+// a CUDA graph, kept as source graph and instantiated executable
+static int step_graph(bld_handle* h, int method, double dt) {
+    const auto key = std::make_pair(method, dt);
+    if (h->graphs.count(key)) return BLD_OK;
+    cudaGraph_t graph;
+    CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int st = enqueue_step(h, method, dt, false);
+    cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+    if (st != BLD_OK) {
+        if (ce == cudaSuccess) cudaGraphDestroy(graph);
+        return st;
+    }
+    CUDA_TRY(ce);
+    cudaGraphExec_t exec;
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        CUDA_TRY(ie);
+    }
+    h->graphs.emplace(key, exec);
+    h->graph_src.emplace(key, graph);
+    return BLD_OK;
+}
+
 int32_t bld_step(bld_handle* h, int64_t nsteps, double dt, int32_t method) {
     BLD_TRY(step_impl(h, nsteps, dt, method));
     return check_flag(h);
@@ -1256,24 +1380,63 @@ static int step_impl(bld_handle* h, int64_t nsteps, double dt, int32_t method) {
         const auto key = std::make_pair((int)method, dt);
         auto it = h->graphs.find(key);
         if (it == h->graphs.end()) {
-            cudaGraph_t graph;
-            CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            int st = enqueue_step(h, method, dt, false);
-            cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
-            if (st != BLD_OK) {
-                if (ce == cudaSuccess) cudaGraphDestroy(graph);
-                return st;
-            }
-            CUDA_TRY(ce);
-            cudaGraphExec_t exec;
-            cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
-            cudaGraphDestroy(graph);
-            CUDA_TRY(ie);
-            it = h->graphs.emplace(key, exec).first;
+            BLD_TRY(step_graph(h, method, dt));
+            it = h->graphs.find(key);
         }
         for (; done < nsteps; ++done) CUDA_TRY(cudaGraphLaunch(it->second, h->stream));
     }
     return BLD_OK;
+}
+
+int32_t bld_ensemble_step(bld_handle* const* hs, int32_t n, int64_t nsteps, double dt, int32_t method) {
+    if (!hs || n < 1) return fail(BLD_ERR_ARGUMENT, "no handles");
+    if (method == BLD_AB2) return fail(BLD_ERR_ARGUMENT, "ensemble stepping supports the one-step methods");
+    if (method < BLD_EULER || method > BLD_SSPRK33) return fail(BLD_ERR_ARGUMENT, "unknown method %d", method);
+    bld_handle* lead = hs[0];
+    for (int i = 0; i < n; ++i) {
+        if (!hs[i] || !hs[i]->slope_valid) return fail(BLD_ERR_ARGUMENT, "handle %d is not prepared", i);
+        if (hs[i]->device != lead->device) return fail(BLD_ERR_ARGUMENT, "handles on different devices");
+    }
+    if (nsteps <= 0) return BLD_OK;
+    CUDA_TRY(cudaSetDevice(lead->device));
+    std::vector<const void*> key;
+    for (int i = 0; i < n; ++i) key.push_back(hs[i]);
+    key.push_back((const void*)(intptr_t)method);
+    double dtk = dt;
+    const void* dtp;
+    memcpy(&dtp, &dtk, sizeof(dtp) < sizeof(dtk) ? sizeof(dtp) : sizeof(dtk));
+    key.push_back(dtp);
+    auto it = lead->ens_graphs.find(key);
+    if (it == lead->ens_graphs.end()) {
+        cudaGraph_t parent;
+        CUDA_TRY(cudaGraphCreate(&parent, 0));
+        for (int i = 0; i < n; ++i) {
+            int st = step_graph(hs[i], method, dt);
+            if (st != BLD_OK) {
+                cudaGraphDestroy(parent);
+                return st;
+            }
+            cudaGraphNode_t node;
+            cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, hs[i]->graph_src.at(std::make_pair((int)method, dt)));
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(parent);
+                CUDA_TRY(e);
+            }
+        }
+        cudaGraphExec_t exec;
+        cudaError_t ie = cudaGraphInstantiate(&exec, parent, 0);
+        cudaGraphDestroy(parent);
+        CUDA_TRY(ie);
+        it = lead->ens_graphs.emplace(key, exec).first;
+    }
+    for (int64_t s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(it->second, lead->stream));
+    CUDA_TRY(cudaStreamSynchronize(lead->stream));
+    int status = BLD_OK;
+    for (int i = 0; i < n; ++i) {
+        const int st = check_flag(hs[i]);
+        if (st != BLD_OK) status = st;
+    }
+    return status;
 }
 
 int32_t bld_get_stream(bld_handle* h, void** stream) {
@@ -1326,7 +1489,7 @@ int32_t bld_time_phases(bld_handle* h, int32_t iters, int32_t method, bld_phase_
     out->launches_per_step = stages * (launches_per_rhs(h) + (proj || stages > 1 ? 1 : 1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (st == BLD_OK) CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    if (st == BLD_OK) CUDA_TRY(cudaMemsetAsync(h->flag, 0, h->B * sizeof(int), h->stream));
     return st;
 }
 
@@ -1373,6 +1536,58 @@ int32_t bld_state_device_ptr(bld_handle* h, void** state) {
 int32_t bld_sync(bld_handle* h) {
     if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
     CUDA_TRY(cudaSetDevice(h->device));
+    return check_flag(h);
+}
+
+int32_t bld_set_active(bld_handle* h, const int32_t* mask) {
+    if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    for (int m = 0; m < h->B; ++m) h->active_host[m] = mask ? (mask[m] != 0) : 1;
+    CUDA_TRY(cudaMemcpyAsync(h->active, h->active_host.data(), h->B * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
+}
+
+int32_t bld_set_member_params(bld_handle* h, int32_t m, double cs, double z0_lower, double source1) {
+    if (!member_ok(h, m)) return fail(BLD_ERR_ARGUMENT, "invalid member");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int n3 = h->g.n3;
+    if (h->cfg.sgs && (!std::isnan(cs) || !std::isnan(z0_lower))) {
+        if (std::isnan(cs)) cs = h->member_cs[m];
+        if (std::isnan(z0_lower)) z0_lower = h->member_z0[m];
+        if (!(cs > 0) || (h->cfg.wall_kind[0] == BLD_WALL_ROUGH && !(z0_lower > 0)))
+            return fail(BLD_ERR_ARGUMENT, "invalid Cs or roughness length");
+        std::vector<double> lc2(n3), li2(n3 - 1), wall(4);
+        member_sgs_tables(h, cs, z0_lower, lc2.data(), li2.data(), wall.data());
+        CUDA_TRY(cudaMemcpyAsync(h->lc2 + (size_t)m * n3, lc2.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(cudaMemcpyAsync(h->li2 + (size_t)m * (n3 - 1), li2.data(), (n3 - 1) * sizeof(double),
+                                 cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(cudaMemcpyAsync(h->wall + 4 * (size_t)m, wall.data(), 4 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        h->member_cs[m] = cs;
+        h->member_z0[m] = z0_lower;
+    }
+    if (!std::isnan(source1)) {
+        CUDA_TRY(cudaMemcpyAsync(h->src + 3 * (size_t)m, &source1, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
+}
+
+int32_t bld_get_diverged(bld_handle* h, int32_t* out) {
+    if (!h || !out) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    for (int m = 0; m < h->B; ++m) {
+        out[m] = h->diverged[m];
+        h->diverged[m] = 0;
+    }
+    return BLD_OK;
+}
+
+int32_t bld_prepare_member(bld_handle* h, int32_t m) {
+    if (!member_ok(h, m)) return fail(BLD_ERR_ARGUMENT, "invalid member");
+    CUDA_TRY(cudaSetDevice(h->device));
+    BLD_TRY(enqueue_project(h, S_NONE, 0.0, h->u, nullptr, nullptr, nullptr, h->u, m, 1));
+    BLD_TRY(enqueue_rates(h, h->u, h->du, m, 1));
+    h->slope_valid = true;
     return check_flag(h);
 }
 
@@ -1475,10 +1690,13 @@ int32_t bld_get_field_physical(bld_handle* h, int32_t m, int32_t field, double* 
 
 int32_t bld_ldlt_solve_device(const double* gamma, const double* beta, void* rhs, int64_t nsys, int32_t n, void* stream) {
     if (!gamma || !beta || !rhs || nsys <= 0 || n < 1) return fail(BLD_ERR_ARGUMENT, "invalid argument");
-    const unsigned blocks = (unsigned)((nsys + 127) / 128);
-    k_ldlt_solve<<<blocks, 128, 0, (cudaStream_t)stream>>>(gamma, beta, (double2*)rhs, nsys, n);
-    CUDA_TRY(cudaGetLastError());
-    return BLD_OK;
+    return ldlt_launch<double2>(gamma, beta, (double2*)rhs, nsys, n, (cudaStream_t)stream);
+}
+
+int32_t bld_ldlt_solve_real_device(const double* gamma, const double* beta, double* rhs, int64_t nsys, int32_t n,
+                                   void* stream) {
+    if (!gamma || !beta || !rhs || nsys <= 0 || n < 1) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    return ldlt_launch<double>(gamma, beta, rhs, nsys, n, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -28,6 +28,10 @@ struct Geo {
 
 __device__ __forceinline__ long long fld_off(const Geo& g, int f) { return (long long)f * g.n3 * g.F; }
 
+// inactive ensemble slots (serving) skip their blocks; uniform per block
+#define BLD_SKIP_INACTIVE(a, m) \
+    if ((a).active && !(a).active[m]) return
+
 // Copies n table entries from global to shared memory with up to 8 loads in
 // flight per thread (a load-then-store loop would wait one DRAM latency per entry).
 template <typename C>
@@ -60,6 +64,7 @@ struct InvYArgs {
     int isI[BLD_MAXT];
     int m0;                      // first member
     int NL;                      // k1 lines per block
+    const int* active;           // [members] 0 = skip the member (NULL: all active)
     const double2* state;
     void* mixed;
     long long mixed_mstride;     // elements per member
@@ -127,6 +132,7 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
     C* b0 = tw + a.P2;
     C* b1 = b0 + a.P2 * NL;
     const int t = blockIdx.x % a.nterms, m = a.m0 + blockIdx.x / a.nterms;
+    BLD_SKIP_INACTIVE(a, m);
     const int z = blockIdx.z;
     const int nz = a.isI[t] ? a.g.n3 - 1 : a.g.n3;
     if (z >= nz) return;
@@ -215,7 +221,9 @@ __global__ void __launch_bounds__(384) k_inv_y_all(InvYArgs a) {
     const int k10 = blockIdx.x * NL;
     const int z = blockIdx.y;
     const int m = a.m0 + blockIdx.z;
+    BLD_SKIP_INACTIVE(a, m);
     const bool hasI = z < n3 - 1;
+    BLD_SKIP_INACTIVE(a, m);
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + P2;
     copy_table(tw, reinterpret_cast<const C*>(a.tw), P2);
@@ -288,6 +296,7 @@ struct XArgs {
     Geo g;
     int P1, P2, YT, zchunk;
     int m0;
+    const int* active;
     const void* min;
     void* mout;
     long long min_mstride, mout_mstride;  // elements per member
@@ -363,6 +372,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
     C* bufB = bufA + NLin * P1;
     const int y0 = blockIdx.x * YT;
     const int m = a.m0 + blockIdx.z;
+    BLD_SKIP_INACTIVE(a, m);
     const int z0 = blockIdx.y * a.zchunk;
     const int z1 = min(n3, z0 + a.zchunk);
     const int nthr = blockDim.x;
@@ -505,6 +515,7 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
     C* bufB = bufA + NLin * P1;
     const int y0 = blockIdx.x * YT;
     const int m = a.m0 + blockIdx.z;
+    BLD_SKIP_INACTIVE(a, m);
     const int z0 = blockIdx.y * a.zchunk;
     const int z1 = min(n3, z0 + a.zchunk);
     const int nthr = blockDim.x;
@@ -754,11 +765,12 @@ struct FwdYArgs {
     const double* d1;
     const double* d2;
     double inv_n;              // 1/(P1*P2)
-    int* flag;
+    int* flag;                 // per member
     int fields;                // number of target fields (3 for rates, 1 for transforms)
     int field0;                // first target field
     int m0;                    // first member
     int NL;                    // k1 lines per block
+    const int* active;
     FftPlan plan;
     const void* tw;
 };
@@ -906,6 +918,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     const int NL = a.NL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int fi = blockIdx.x % a.fields, m = a.m0 + blockIdx.x / a.fields;
+    BLD_SKIP_INACTIVE(a, m);
     const int f = a.field0 + fi;
     const int z = blockIdx.z;
     const Geo& g = a.g;
@@ -1020,7 +1033,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
             if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
         }
     }
-    if (a.check && bad) atomicOr(a.flag, 1);
+    if (a.check && bad) atomicOr(a.flag + m, 1);
 }
 
 // Forward y pass of all three rate fields at one layer: one block per (k1 tile,
@@ -1038,6 +1051,7 @@ __global__ void __launch_bounds__(384) k_fwd_y_all(FwdYArgs a) {
     const int k10 = blockIdx.x * NL;
     const int z = blockIdx.y;
     const int m = a.m0 + blockIdx.z;
+    BLD_SKIP_INACTIVE(a, m);
     bool hasB = false;
     for (int f = 0; f < 3; ++f)
         for (int ci = 0; ci < a.ncontrib[f]; ++ci) hasB |= (a.c[f][ci].pref == 2);
@@ -1150,13 +1164,14 @@ __global__ void __launch_bounds__(384) k_fwd_y_all(FwdYArgs a) {
             if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
         }
     }
-    if (a.check && bad) atomicOr(a.flag, 1);
+    if (a.check && bad) atomicOr(a.flag + m, 1);
 }
 
 // Linear terms only (no physical-domain process): grid (ceil(F/256), n3, 3*members)
 __global__ void __launch_bounds__(256) k_linear(FwdYArgs a) {
     const Geo& g = a.g;
     const int f = blockIdx.z % 3, m = a.m0 + blockIdx.z / 3;
+    BLD_SKIP_INACTIVE(a, m);
     const int z = blockIdx.y;
     const int nz = (f == 2) ? g.n3 - 1 : g.n3;
     const int mo = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1165,7 +1180,7 @@ __global__ void __launch_bounds__(256) k_linear(FwdYArgs a) {
     const double2* S = a.state + (long long)m * g.mstride;
     const double2 v = linear_terms(g, a.lin, S, f, z, j, k1, m);
     a.du[(long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F + mo] = v;
-    if (a.check && !(isfinite(v.x) && isfinite(v.y))) atomicOr(a.flag, 1);
+    if (a.check && !(isfinite(v.x) && isfinite(v.y))) atomicOr(a.flag + m, 1);
 }
 
 // --------------------------------------------------- stage update + projection
@@ -1182,6 +1197,7 @@ enum StageKind {
 struct ProjArgs {
     Geo g;
     int m0;
+    const int* active;
     const double2* u;
     const double2* t;
     const double2* du;
@@ -1244,6 +1260,7 @@ __global__ void __launch_bounds__(128) k_project(ProjArgs a) {
     const Geo& g = a.g;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = a.m0 + blockIdx.y;
+    BLD_SKIP_INACTIVE(a, m);
     if (c >= g.F) return;
     const long long mb = (long long)m * g.mstride;
     const long long F = g.F;
@@ -1373,14 +1390,15 @@ __global__ void __launch_bounds__(128) k_project(ProjArgs a) {
 // value entering from below (forward: b_z = P_z + Q_z b_in) or from above
 // (backward: p_z = G_z + H_z p_out) and the segments are chained through shared
 // memory.  Same arithmetic as k_project up to the order of operations.
-template <int LMAX>
-__global__ void __launch_bounds__(512) k_project_seg(ProjArgs a) {
+template <int LMAX, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
     const Geo& g = a.g;
     const int n = g.n3;
     const long long F = g.F;
     const int NS = blockDim.y, s = threadIdx.y, lane = threadIdx.x;
-    const int c = blockIdx.x * 32 + lane;
+    const int c = blockIdx.x * blockDim.x + lane;
     const int m = a.m0 + blockIdx.y;
+    BLD_SKIP_INACTIVE(a, m);
     const bool valid = c < g.F;
     const int L = (n + NS - 1) / NS;
     const int z0 = min(n, s * L), z1 = min(n, z0 + L);
@@ -1464,7 +1482,7 @@ __global__ void __launch_bounds__(512) k_project_seg(ProjArgs a) {
         if (len > 0 && valid) {
 #pragma unroll
             for (int q = 0; q < LMAX; ++q)
-                if (q == len - 1) {
+                if (q < len) {   // the last valid layer wins; `q == len - 1` would become a dynamic index
                     pe = X[q];
                     qe = Y[q];
                 }
@@ -1493,7 +1511,9 @@ __global__ void __launch_bounds__(512) k_project_seg(ProjArgs a) {
             Y[q] = 0.0;  // p_{n-1} = b_{n-1}
         } else {
             const double cz = a.gamma[z * F + c] * a.alpha_i[z];
-            if (q == len - 1) {
+            // len <= LMAX, so q == LMAX-1 implies q == len-1; spelling it out keeps
+            // X[q + 1] in range for the compiler and the arrays in registers
+            if (q == len - 1 || q == LMAX - 1) {
                 Y[q] = -cz;
             } else {
                 X[q] = make_double2(X[q].x - cz * X[q + 1].x, X[q].y - cz * X[q + 1].y);
@@ -1574,30 +1594,123 @@ __global__ void __launch_bounds__(512) k_project_seg(ProjArgs a) {
     }
 }
 
-// Standalone batched LDL^T solve, one thread per system (ldiv!, src/processes/pressure.jl:167-201)
-__global__ void __launch_bounds__(128) k_ldlt_solve(const double* __restrict__ gamma, const double* __restrict__ beta,
-                                                    double2* rhs, long long nsys, int n) {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nsys) return;
-    double2 b = rhs[c];
-    double gm = gamma[c];
-    b.x *= gm;
-    b.y *= gm;
-    rhs[c] = b;
-    for (int z = 1; z < n; ++z) {
-        const long long idx = (long long)z * nsys + c;
-        const double2 r = rhs[idx];
-        const double be = beta[z - 1];
-        gm = gamma[idx];
-        b = make_double2(gm * (r.x - be * b.x), gm * (r.y - be * b.y));
-        rhs[idx] = b;
+// ---------------------------------------- segmented batched tridiagonal solve
+// L D L^T x = b per system (ldiv!(::DistributedBatchLDLt, b),
+// src/processes/pressure.jl:106-201): forward b_z = g_z (b_z - beta_{z-1} b_{z-1}),
+// backward x_z = b_z - g_z beta_z x_{z+1}.  Instead of one thread walking all n
+// layers of a system twice (two reads of b and g), each thread holds LMAX
+// consecutive layers of one system in registers and solves them as an affine
+// function of the value entering its segment: forward b_z = X_z + Y_z b_in with
+// Y_z = prod(-g beta); the segment ends (X, Y) are combined through shared
+// memory, and the backward sweep is done the same way.  b and g are read once and
+// x is written once: 40 bytes per complex unknown (24 real).
+// block (LANES, NS): LANES systems side by side (coalesced rows), NS segments;
+// grid ceil(nsys / LANES); dynamic smem (n-1) doubles + NS*LANES*(sizeof(T)+8).
+__device__ __forceinline__ double v_scale(double a, double x) { return a * x; }
+__device__ __forceinline__ double2 v_scale(double a, double2 x) { return make_double2(a * x.x, a * x.y); }
+__device__ __forceinline__ double v_axpy(double a, double x, double y) { return y + a * x; }
+__device__ __forceinline__ double2 v_axpy(double a, double2 x, double2 y) {
+    return make_double2(y.x + a * x.x, y.y + a * x.y);
+}
+template <typename T>
+__device__ __forceinline__ T v_zero();
+template <>
+__device__ __forceinline__ double v_zero<double>() { return 0.0; }
+template <>
+__device__ __forceinline__ double2 v_zero<double2>() { return make_double2(0.0, 0.0); }
+
+template <typename T, int LMAX>
+__global__ void __launch_bounds__(512) k_ldlt_seg(const double* __restrict__ gamma, const double* __restrict__ beta,
+                                                  T* __restrict__ rhs, long long nsys, int n) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int LANES = blockDim.x, NS = blockDim.y, lane = threadIdx.x, s = threadIdx.y;
+    double* sb = reinterpret_cast<double*>(smem_raw);                  // beta [n-1]
+    T* sP = reinterpret_cast<T*>(sb + (n & ~1));                       // [NS][LANES] (n & ~1 >= n-1, even)
+    double* sQ = reinterpret_cast<double*>(sP + NS * LANES);            // [NS][LANES]
+    for (int i = s * LANES + lane; i < n - 1; i += NS * LANES) sb[i] = beta[i];
+    const long long c = (long long)blockIdx.x * LANES + lane;
+    const bool valid = c < nsys;
+    const int L = (n + NS - 1) / NS;
+    const int z0 = min(n, s * L), z1 = min(n, z0 + L);
+    const int len = valid ? z1 - z0 : 0;
+    T X[LMAX];
+    double G[LMAX];
+#pragma unroll
+    for (int q = 0; q < LMAX; ++q)
+        if (q < len) {
+            X[q] = rhs[(long long)(z0 + q) * nsys + c];
+            G[q] = gamma[(long long)(z0 + q) * nsys + c];
+        }
+    __syncthreads();
+    // forward sweep, local input 0
+    double y = 1.0;
+#pragma unroll
+    for (int q = 0; q < LMAX; ++q)
+        if (q < len) {
+            const int z = z0 + q;
+            if (q == 0) {
+                X[0] = v_scale(G[0], X[0]);
+                y = (z == 0) ? 0.0 : -G[0] * sb[z - 1];
+            } else {
+                X[q] = v_scale(G[q], v_axpy(-sb[z - 1], X[q - 1], X[q]));
+                y = -G[q] * sb[z - 1] * y;
+            }
+        }
+    {
+        T pe = v_zero<T>();
+        double qe = 1.0;
+#pragma unroll
+        for (int q = 0; q < LMAX; ++q)
+            if (q < len) {   // the last valid layer wins; `q == len - 1` would become a dynamic index
+                pe = X[q];
+                qe = y;
+            }
+        sP[s * LANES + lane] = pe;
+        sQ[s * LANES + lane] = qe;
     }
-    for (int z = n - 2; z >= 0; --z) {
-        const long long idx = (long long)z * nsys + c;
-        const double2 r = rhs[idx];
-        const double gb = gamma[idx] * beta[z];
-        b = make_double2(r.x - gb * b.x, r.y - gb * b.y);
-        rhs[idx] = b;
+    __syncthreads();
+    T bin = v_zero<T>();
+    for (int t = 0; t < s; ++t) bin = v_axpy(sQ[t * LANES + lane], bin, sP[t * LANES + lane]);
+    __syncthreads();
+    // b_z = X_z + Y_z b_in, with Y_z rebuilt from g and beta
+#pragma unroll
+    for (int q = 0; q < LMAX; ++q)
+        if (q < len) {
+            const int z = z0 + q;
+            y = (q == 0) ? ((z == 0) ? 0.0 : -G[0] * sb[z - 1]) : -G[q] * sb[z - 1] * y;
+            X[q] = v_axpy(y, bin, X[q]);
+        }
+    // backward sweep, local input x_{z1} = 0
+    double h = 1.0;
+#pragma unroll
+    for (int qq = 0; qq < LMAX; ++qq) {
+        const int q = LMAX - 1 - qq;
+        if (q < len) {
+            const int z = z0 + q;
+            const double cz = (z == n - 1) ? 0.0 : G[q] * sb[z];
+            if (q == len - 1 || q == LMAX - 1) {   // len <= LMAX: keeps X[q + 1] in range
+                h = -cz;
+            } else {
+                X[q] = v_axpy(-cz, X[q + 1], X[q]);
+                h = -cz * h;
+            }
+        }
+    }
+    sP[s * LANES + lane] = len > 0 ? X[0] : v_zero<T>();
+    sQ[s * LANES + lane] = len > 0 ? h : 1.0;
+    __syncthreads();
+    T xin = v_zero<T>();
+    for (int t = NS - 1; t > s; --t) xin = v_axpy(sQ[t * LANES + lane], xin, sP[t * LANES + lane]);
+    // x_z = X_z + H_z x_in, H rebuilt from the end of the segment
+#pragma unroll
+    for (int qq = 0; qq < LMAX; ++qq) {
+        const int q = LMAX - 1 - qq;
+        if (q < len) {
+            const int z = z0 + q;
+            const double cz = (z == n - 1) ? 0.0 : G[q] * sb[z];
+            h = (q == len - 1) ? -cz : -cz * h;
+            rhs[(long long)z * nsys + c] = v_axpy(h, xin, X[q]);
+        }
     }
 }
 

@@ -188,6 +188,32 @@ typedef struct {
 } bld_phase_times;
 int32_t bld_time_phases(bld_handle* h, int32_t iters, int32_t method, bld_phase_times* out);
 
+/* Ensemble slots (continuous batching); no reference counterpart (the reference
+   runs one model per process).  All members of a handle share one step graph;
+   bld_set_active marks which members bld_step / bld_step_async /
+   bld_ensemble_step advance (host array of `members` ints, nonzero = active;
+   NULL = all).  Inactive members' blocks exit at once, so a slot costs nothing
+   while free, and the mask is read on the device, so changing it needs no new
+   graph.  Single-member calls (bld_compute_rates, bld_apply_projections,
+   bld_prepare_member, bld_set_field_physical) ignore the mask.
+   bld_set_member_params replaces the per-member Cs, lower-wall roughness length
+   and vel1 forcing of `member` (NAN keeps a value).  bld_prepare_member runs the
+   initial projection and rates (what evolve! does first) for one member after
+   its state was set.  Divergence is flagged per member: after a call returned
+   BLD_ERR_DIVERGED, bld_get_diverged writes 1 for each member whose rates turned
+   non-finite since the previous bld_get_diverged (`members` ints) and clears them. */
+int32_t bld_set_active(bld_handle* h, const int32_t* mask);
+int32_t bld_set_member_params(bld_handle* h, int32_t member, double cs, double z0_lower, double source1);
+int32_t bld_prepare_member(bld_handle* h, int32_t member);
+int32_t bld_get_diverged(bld_handle* h, int32_t* out);
+
+/* Advances several handles on one device (e.g. the size classes of an uneven
+   ensemble) by `nsteps` steps of `method`: each step is ONE launch of a CUDA
+   graph whose child graphs are the handles' step graphs, run as independent
+   branches so the classes overlap on the device.  Every handle must have been
+   prepared (bld_prepare / bld_evolve).  Synchronises and checks divergence. */
+int32_t bld_ensemble_step(bld_handle* const* handles, int32_t n, int64_t nsteps, double dt, int32_t method);
+
 /* Physical-domain fields at the default size (2*k1max+2, 2*k2max+2) of one member:
    initialize!(model; vel = values) (src/State.jl:11-31, set_field! src/physical_space.jl:253-275)
    and model[:vel] (src/State.jl:81-85, get_field src/physical_space.jl:315-319).
@@ -197,11 +223,15 @@ int32_t bld_get_field_physical(bld_handle* h, int32_t member, int32_t field, dou
 
 /* Standalone batched symmetric tridiagonal solve (the kernel of
    ldiv!(::DistributedBatchLDLt, b), src/processes/pressure.jl:106-201):
-   `nsys` systems of size `n`, factor `gamma` [n][nsys] and off-diagonal `beta`
-   [n-1] shared by all systems, complex right-hand sides `rhs` [n][nsys] solved in
-   place.  Device pointers, stream-ordered. */
+   `nsys` systems of size `n` (1 <= n <= 1024), factor `gamma` [n][nsys] (the
+   reference's gamma = 1/(d_z - gamma_{z-1} beta_{z-1}^2), pressure.jl:86-95) and
+   off-diagonal `beta` [n-1] shared by all systems, right-hand sides `rhs`
+   [n][nsys] solved in place: complex (interleaved double2) or real.  Device
+   pointers, stream-ordered. */
 int32_t bld_ldlt_solve_device(const double* gamma, const double* beta, void* rhs,
                               int64_t nsys, int32_t n, void* stream);
+int32_t bld_ldlt_solve_real_device(const double* gamma, const double* beta, double* rhs,
+                                   int64_t nsys, int32_t n, void* stream);
 
 /* Pressure projection that allocates nothing.  No counterpart in the reference:
    it exists for callers that cannot call cudaMalloc -- code whose device memory

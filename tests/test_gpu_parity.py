@@ -247,22 +247,38 @@ def test_ensemble_members_match_single(oracle, BLD):
             assert rel_l2(a[f], b[f]) < 1e-14, (m, f, rel_l2(a[f], b[f]))
 
 
-def test_ldlt_solve_device(oracle, BLD):
-    """The standalone batched LDL^T kernel against the oracle's ldlt_solve."""
-    import ctypes
+LDLT_TOL = 1e-13   # the segmented solve reassociates the recurrences; diagonally dominant systems
+
+
+@pytest.mark.parametrize("n,nsys", [(1, 5), (2, 33), (3, 1), (7, 100), (24, 1000), (96, 517), (255, 64),
+                                    (256, 300), (257, 300), (511, 40), (512, 77), (700, 20), (1024, 33)])
+@pytest.mark.parametrize("kind", ["complex", "real"])
+def test_ldlt_solve_device(oracle, BLD, n, nsys, kind):
+    """The standalone batched LDL^T kernel (segmented) against the oracle's ldlt_solve,
+    including ragged sizes (n not a multiple of the segment length, nsys not a
+    multiple of the systems per block)."""
     import torch
     from BoundaryLayerDynamics import _capi
     lib = _capi.load()
-    rng = np.random.default_rng(2)
-    n, nsys = 24, 1000
+    rng = np.random.default_rng(n * 1000 + nsys)
     diag = -2.0 - rng.random((nsys, n))
-    off = 0.5 + 0.3 * rng.random(n - 1)
+    off = 0.5 + 0.3 * rng.random(max(n - 1, 1))[: n - 1]
     gam = oracle.ldlt_factor(diag, off)                    # (nsys, n)
-    rhs = rng.standard_normal((n, nsys)) + 1j * rng.standard_normal((n, nsys))
+    rhs = rng.standard_normal((n, nsys))
+    if kind == "complex":
+        rhs = rhs + 1j * rng.standard_normal((n, nsys))
     ref = oracle.ldlt_solve(gam, off, rhs.copy())
     g_d = torch.tensor(np.ascontiguousarray(gam.T), device="cuda")
-    b_d = torch.tensor(off, device="cuda")
+    b_d = torch.tensor(np.concatenate([off, [0.0]]), device="cuda")
     r_d = torch.tensor(rhs, device="cuda")
-    _capi.check(lib.bld_ldlt_solve_device(g_d.data_ptr(), b_d.data_ptr(), r_d.data_ptr(), nsys, n, None))
+    fn = lib.bld_ldlt_solve_device if kind == "complex" else lib.bld_ldlt_solve_real_device
+    _capi.check(fn(g_d.data_ptr(), b_d.data_ptr(), r_d.data_ptr(), nsys, n, None))
     torch.cuda.synchronize()
-    assert rel_l2(r_d.cpu().numpy(), ref) < 1e-14
+    assert rel_l2(r_d.cpu().numpy(), ref) < LDLT_TOL
+
+
+def test_ldlt_solve_rejects_bad_sizes(BLD):
+    from BoundaryLayerDynamics import _capi
+    lib = _capi.load()
+    assert lib.bld_ldlt_solve_device(1, 1, 1, 10, 1025, None) == _capi.BLD_ERR_ARGUMENT
+    assert lib.bld_ldlt_solve_real_device(1, 1, 1, 0, 10, None) == _capi.BLD_ERR_ARGUMENT

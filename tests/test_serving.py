@@ -1,0 +1,205 @@
+"""Host logic of the continuous-batching server (no device): admission by slots
+and HBM budget, FIFO without head-of-line blocking across size classes, exact
+step counts per request, slot reuse, rejection, percentiles and the seeded
+arrival process.  The pools here are fakes that count the steps each slot took,
+so the test checks that every request is advanced exactly its own number of
+steps no matter which other requests share its pool."""
+
+import math
+
+import numpy as np
+import pytest
+
+from BoundaryLayerDynamics import serving as S
+
+
+class FakeClock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += max(dt, 1e-6)
+
+
+class FakePool:
+    """A pool with `members` slots whose "state" is the number of steps taken."""
+
+    def __init__(self, members, clock, cost):
+        self.members = members
+        self.clock = clock
+        self.cost = cost
+        self.active = np.zeros(members, dtype=np.int32)
+        self.steps = np.zeros(members, dtype=np.int64)
+        self.params = {}
+        self.loaded = {}
+        self.diverge_at = {}
+
+    def set_field(self, f, values, member):
+        self.loaded.setdefault(member, []).append(f)
+        self.steps[member] = 0
+
+    def set_member_params(self, m, cs=None, z0=None, forcing=None):
+        self.params[m] = (z0, forcing)
+
+    def prepare_member(self, m):
+        pass
+
+    def set_active(self, mask):
+        self.active = np.array(mask, dtype=np.int32)
+
+    def get_state(self, m):
+        return {"steps": int(self.steps[m]), "params": self.params[m]}
+
+    def diverged_members(self):
+        out = [m for m, s in self.diverge_at.items() if self.active[m] and self.steps[m] >= s]
+        for m in out:
+            del self.diverge_at[m]
+        return out
+
+
+def fake_stepper(clock):
+    def step(models, n):
+        from BoundaryLayerDynamics._capi import DivergenceError
+        clock.t += n * sum(p.cost for p in models)
+        bad = False
+        for p in models:
+            p.steps += n * (p.active != 0)
+            bad |= any(p.active[m] and p.steps[m] >= s for m, s in p.diverge_at.items())
+        if bad:
+            raise DivergenceError(-3, "The simulation has diverged.")
+    return step
+
+
+def _server(capacity, budget=10**12, slot_bytes=None, tick=10, keep=True):
+    clock = FakeClock()
+    pools = {s: FakePool(c, clock, cost=1e-4 * s[0] / 64) for s, c in capacity.items()}
+    sb = slot_bytes or {s: 10**6 * s[0] for s in capacity}
+    srv = S.Server(pools, sb, budget, tick=tick, stepper=fake_stepper(clock), keep_results=keep,
+                   clock=clock, sleep=clock.sleep)
+    return srv, pools, clock
+
+
+def _reqs(n, rate, sizes, steps=500, seed=5):
+    return S.make_requests(n, rate, seed=seed, sizes=sizes, probs=[1.0 / len(sizes)] * len(sizes), steps=steps,
+                           materialize=False)
+
+
+def test_poisson_arrivals_seeded_and_rate():
+    a = S.poisson_arrivals(50.0, 20000, seed=3)
+    b = S.poisson_arrivals(50.0, 20000, seed=3)
+    assert np.array_equal(a, b)
+    assert np.all(np.diff(a) > 0)
+    assert abs(20000 / a[-1] - 50.0) / 50.0 < 0.03
+
+
+def test_make_requests_draws():
+    reqs = S.make_requests(4000, 10.0, seed=1, materialize=False)
+    sizes = [r.size for r in reqs]
+    for s, p in zip(S.SIZES, S.PROBS):
+        assert abs(sizes.count(s) / len(reqs) - p) < 0.03
+    z0 = np.array([r.z0 for r in reqs])
+    assert z0.min() >= 1e-5 and z0.max() <= 1e-3
+    lz = np.log10(z0)
+    assert abs(lz.mean() + 4.0) < 0.05        # log-uniform on [1e-5, 1e-3]
+    f = np.array([r.forcing for r in reqs])
+    assert f.min() >= 0.5 and f.max() <= 1.5
+
+
+def test_percentile_nearest_rank():
+    v = list(range(1, 101))
+    assert S.percentile(v, 50) == 50
+    assert S.percentile(v, 99) == 99
+    assert S.percentile(v, 100) == 100
+    assert S.percentile([3.0], 99) == 3.0
+    assert math.isnan(S.percentile([], 50))
+
+
+def test_plan_capacity_within_budget():
+    sb = {(64, 32): 40e6, (128, 64): 300e6, (192, 96): 1.0e9, (256, 128): 2.4e9}
+    probs = dict(zip(S.SIZES, S.PROBS))
+    for budget in (5e9, 20e9, 60e9):
+        cap = S.plan_capacity(budget, sb, probs)
+        assert all(c >= 1 for c in cap.values())
+        assert sum(cap[s] * sb[s] for s in sb) <= budget
+    cap = S.plan_capacity(60e9, sb, probs)
+    assert cap[(64, 32)] > cap[(128, 64)] > cap[(192, 96)] > cap[(256, 128)]   # follows the mix
+    with pytest.raises(ValueError):
+        S.plan_capacity(1e9, sb, probs)
+
+
+def test_scheduler_admission_budget_and_fifo():
+    a, b = (32, 16), (48, 24)
+    sch = S.Scheduler({a: 2, b: 1}, {a: 10, b: 25}, budget=40)
+    reqs = [S.Request(i, s, 5, 0.0, 1e-4, 1.0, i) for i, s in enumerate([b, b, a, a, a])]
+    for r in reqs:
+        assert sch.submit(r)
+    got = sch.admit()
+    # b takes its only slot (25 bytes); the second b waits without blocking the a
+    # requests behind it; one a fits (35 bytes resident), a second would make 45 > 40
+    assert [(r.rid, s, slot) for r, s, slot in got] == [(0, b, 0), (2, a, 0)]
+    assert [r.rid for r in sch.queue] == [1, 3, 4]
+    assert sch.resident == 35
+    assert sch.next_tick(10) == 5
+    done = sch.advance(5)
+    assert sorted(r.rid for r, _, _ in done) == [0, 2]
+    for r, s, slot in done:
+        sch.release(s, slot)
+    assert sch.resident == 0
+    got = sch.admit()
+    assert [(r.rid, s, slot) for r, s, slot in got] == [(1, b, 0), (3, a, 0)]
+
+
+def test_scheduler_rejects():
+    a = (32, 16)
+    sch = S.Scheduler({a: 1}, {a: 100}, budget=50)
+    r = S.Request(0, a, 5, 0.0, 1e-4, 1.0, 0)
+    assert not sch.submit(r) and r.status == "rejected" and "budget" in r.error
+    sch = S.Scheduler({a: 1}, {a: 10}, budget=50)
+    r = S.Request(1, (99, 9), 5, 0.0, 1e-4, 1.0, 0)
+    assert not sch.submit(r) and r.status == "rejected" and "no pool" in r.error
+    r = S.Request(2, a, 0, 0.0, 1e-4, 1.0, 0)
+    assert not sch.submit(r) and r.status == "rejected"
+
+
+def test_server_exact_steps_and_slot_reuse():
+    caps = {(32, 16): 3, (48, 24): 2}
+    srv, pools, clock = _server(caps, tick=7)
+    reqs = _reqs(40, rate=400.0, sizes=list(caps), steps=50)
+    st = srv.run(reqs)
+    assert st["completed"] == 40 and st["rejected"] == 0
+    for r in reqs:
+        assert r.result["steps"] == 50, (r.rid, r.result)          # exactly its own steps
+        assert r.result["params"] == (r.z0, r.forcing)              # its own parameters
+        assert r.done >= r.admitted >= r.arrival
+    # continuous batching: some requests ran together in one pool
+    assert srv.ticks < sum(math.ceil(50 / 7) for _ in reqs)
+    assert st["p99_latency_s"] >= st["p50_latency_s"] > 0
+    assert st["updates_per_s"] > 0
+
+
+def test_server_budget_limits_residency():
+    caps = {(32, 16): 4}
+    sb = {(32, 16): 100}
+    srv, pools, clock = _server(caps, budget=250, slot_bytes=sb, tick=5)
+    reqs = _reqs(12, rate=1e6, sizes=[(32, 16)], steps=10)        # all arrive at once
+    st = srv.run(reqs)
+    assert st["completed"] == 12
+    assert st["peak_resident_bytes"] == 200                         # never a third slot
+    assert max(int(p.active.sum()) for p in pools.values()) <= 2
+
+
+def test_server_isolates_a_diverged_member():
+    caps = {(32, 16): 3}
+    srv, pools, clock = _server(caps, tick=5)
+    reqs = _reqs(3, rate=1e6, sizes=[(32, 16)], steps=20)
+    pools[(32, 16)].diverge_at[1] = 10                              # the request in slot 1 blows up
+    st = srv.run(reqs)
+    assert st["diverged"] == 1 and st["completed"] == 2
+    bad = [r for r in reqs if r.status == "diverged"][0]
+    assert "diverged" in bad.error
+    for r in reqs:
+        if r.status == "done":
+            assert r.result["steps"] == 20
