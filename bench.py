@@ -47,6 +47,11 @@ def parse():
     ap.add_argument("--only", default="", help="comma list of extras to run (ensemble,serving,tridiag,les64,les512)")
     ap.add_argument("--serve-budget-gb", type=float, default=48.0, help="HBM budget of the served stream")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="target length of the served stream")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiler mode: set up the workload, then run --profile-steps steps between "
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off) and exit")
+    ap.add_argument("--profile-steps", type=int, default=1)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="precision of --profile")
     return ap.parse_args()
 
 
@@ -527,8 +532,32 @@ def run_reference(args):
     }
 
 
+def run_profile(args):
+    """The workload's setup (model, autotuning, initial projection, warm-up) outside
+    the profiled range; then --profile-steps steps inside cudaProfilerStart/Stop."""
+    import torch
+    import BoundaryLayerDynamics as BLD
+    from BoundaryLayerDynamics import workloads
+    spec = workloads.CONFIGS[args.config]
+    m = workloads.build(spec, BLD, precision=args.precision)
+    u0, v0, w0 = workloads.initial_fields(spec)
+    BLD.initialize(m, vel1=u0, vel2=v0, vel3=w0)
+    m.prepare()
+    m.step(max(3, args.warmup), spec["dt"])
+    m.sync()
+    torch.cuda.profiler.start()
+    m.step(args.profile_steps, spec["dt"])
+    m.sync()
+    torch.cuda.profiler.stop()
+    return {"profile": args.config, "precision": args.precision, "steps": args.profile_steps,
+            "adv_p": [m.info.adv_p1, m.info.adv_p2], "sgs_p": [m.info.sgs_p1, m.info.sgs_p2]}
+
+
 def main():
     args = parse()
+    if args.profile:
+        print(json.dumps(run_profile(args)), flush=True)
+        return
     if args.impl == "reference":
         out = run_reference(args)
     else:
