@@ -168,12 +168,10 @@ def run_b200(args):
             dist.all_reduce(t)
         torch.cuda.synchronize()
 
+    from BoundaryLayerDynamics import replicas
+
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.reduce_max(x, dist, device="cuda")
 
     res = {}
     models = {}
