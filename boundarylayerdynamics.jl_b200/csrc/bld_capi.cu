@@ -17,6 +17,7 @@
 
 #include "bld.h"
 #include "bld_kernels.cuh"
+#include "bld_warpx.cuh"
 
 double2 h_wtab64[BLD_WTAB_SIZE];
 float2 h_wtab32[BLD_WTAB_SIZE];
@@ -129,6 +130,7 @@ struct Space {
     void* mout = nullptr;
     long long min_ms = 0, mout_ms = 0;  // elements per member
     int YT = 1, PPT = 1, zchunk = 1, nchunks = 1;  // x kernels: rows per block, points per thread, z chunks
+    int xw = 0;                                     // > 0: warp-per-row x kernel with xw warps per block
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
 };
@@ -241,7 +243,8 @@ int pick_y(int P2, bool fp32, int sets) {
 // fill the GPU a few times over, at least 8 layers per chunk
 void x_chunks(const bld_handle* h, Space& s) {
     const int n3 = h->g.n3;
-    const long long blocks_per_chunk = (long long)(s.P2 / s.YT) * h->B;
+    const int rows = s.xw ? s.xw : s.YT;
+    const long long blocks_per_chunk = (long long)((s.P2 + rows - 1) / rows) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
     want = std::min(want, std::max(1, n3 / 8));
     s.zchunk = (n3 + want - 1) / want;
@@ -360,6 +363,42 @@ int launch_adv_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     return BLD_OK;
 }
 
+// radix of the warp-per-row x kernel for P1 = 32 * radix, or 0 if no variant is compiled
+template <typename R>
+int warpx_radix(int P1) {
+    if (P1 % 32) return 0;
+    const int r = P1 / 32;
+    if (sizeof(R) == 8) return (r == 2 || r == 3 || r == 4 || r == 6) ? r : 0;
+    return (r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 9 || r == 12) ? r : 0;
+}
+
+template <typename R>
+int launch_adv_xw(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    const int r = warpx_radix<R>(s.P1);
+    dim3 grid((s.P2 + s.xw - 1) / s.xw, s.nchunks, nm);
+    const int thr = 32 * s.xw;
+    const size_t sm = ((size_t)r * 32 + (size_t)s.xw * 12 * h->g.K1) * csize(sizeof(R) == 4);
+    switch (r) {
+        case 2: k_adv_xw<R, 2><<<grid, thr, sm, h->stream>>>(a); break;
+        case 3: k_adv_xw<R, 3><<<grid, thr, sm, h->stream>>>(a); break;
+        case 4: k_adv_xw<R, 4><<<grid, thr, sm, h->stream>>>(a); break;
+        case 6: k_adv_xw<R, 6><<<grid, thr, sm, h->stream>>>(a); break;
+        default:
+            if constexpr (sizeof(R) == 4) {
+                switch (r) {
+                    case 8: k_adv_xw<R, 8><<<grid, thr, sm, h->stream>>>(a); break;
+                    case 9: k_adv_xw<R, 9><<<grid, thr, sm, h->stream>>>(a); break;
+                    case 12: k_adv_xw<R, 12><<<grid, thr, sm, h->stream>>>(a); break;
+                    default: return fail(BLD_ERR_INVALID_CONFIG, "no warp x kernel for P1=%d", s.P1);
+                }
+            } else {
+                return fail(BLD_ERR_INVALID_CONFIG, "no warp x kernel for P1=%d", s.P1);
+            }
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
 template <typename R>
 int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     dim3 grid(s.P2 / s.YT, s.nchunks, nm);
@@ -398,6 +437,15 @@ int set_smem_limits_R() {
     BLD_SET((k_sgs_x<R, 2>));
     BLD_SET((k_sgs_x<R, 3>));
     BLD_SET((k_sgs_x<R, 4>));
+    BLD_SET((k_adv_xw<R, 2>));
+    BLD_SET((k_adv_xw<R, 3>));
+    BLD_SET((k_adv_xw<R, 4>));
+    BLD_SET((k_adv_xw<R, 6>));
+    if constexpr (sizeof(R) == 4) {
+        BLD_SET((k_adv_xw<R, 8>));
+        BLD_SET((k_adv_xw<R, 9>));
+        BLD_SET((k_adv_xw<R, 12>));
+    }
 #undef BLD_SET
     return BLD_OK;
 }
@@ -502,7 +550,8 @@ int enqueue_x_R(bld_handle* h, int sp, int m0, int nm) {
     xa.w_lo = h->w_lo;
     xa.w_hi = h->w_hi;
     xa.active = h->mask_on ? h->active : nullptr;
-    return sp == 0 ? launch_adv_x<R>(h, s, xa, nm) : launch_sgs_x<R>(h, s, xa, nm);
+    if (sp == 0) return s.xw ? launch_adv_xw<R>(h, s, xa, nm) : launch_adv_x<R>(h, s, xa, nm);
+    return launch_sgs_x<R>(h, s, xa, nm);
 }
 
 template <typename R>
@@ -632,8 +681,19 @@ int time_launches(bld_handle* h, F&& fn, int iters, float* ms) {
 // tiling by timing every candidate on the handle's own buffers.  All candidates
 // perform the same arithmetic, so the choice changes speed, not results.
 int autotune(bld_handle* h) {
+    // BLD_X_KERNEL=warp|block restricts the advection x kernel to one family
+    const char* xk = getenv("BLD_X_KERNEL");
+    const bool only_warp = xk && !strcmp(xk, "warp"), only_block = xk && !strcmp(xk, "block");
+    const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
+    if (only_warp && !adv_warp_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no warp x kernel for P1=%d", h->adv.P1);
     const char* env = getenv("BLD_NO_AUTOTUNE");
-    if (env && env[0] && env[0] != '0') return BLD_OK;
+    if (env && env[0] && env[0] != '0') {
+        if (only_warp && adv_warp_ok) {
+            h->adv.xw = 4;
+            x_chunks(h, h->adv);
+        }
+        return BLD_OK;
+    }
     const int B = h->B;
     for (int sp = 0; sp < 2; ++sp) {
         Space& s = sp == 0 ? h->adv : h->sgs;
@@ -653,6 +713,7 @@ int autotune(bld_handle* h) {
         best = 1e30f;
         int byt = s.YT, bppt = s.PPT;
         for (auto c : x_candidates(h, s, sp == 0)) {
+            if (sp == 0 && only_warp) break;
             s.YT = c.first;
             s.PPT = c.second;
             x_chunks(h, s);
@@ -663,6 +724,18 @@ int autotune(bld_handle* h) {
                 bppt = c.second;
             }
         }
+        int bxw = 0;
+        const bool warp_ok = sp == 0 && adv_warp_ok && !only_block;
+        for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) {
+            s.xw = wpb;
+            x_chunks(h, s);
+            BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
+            if (t < best) {
+                best = t;
+                bxw = wpb;
+            }
+        }
+        s.xw = bxw;
         s.YT = byt;
         s.PPT = bppt;
         x_chunks(h, s);
@@ -679,8 +752,8 @@ int autotune(bld_handle* h) {
         s.fwd = bf;
         const char* v = getenv("BLD_VERBOSE");
         if (v && v[0] && v[0] != '0')
-            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d | x YT=%d PPT=%d chunks=%d | fwd all=%d NL=%d thr=%d\n",
-                    sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.YT, s.PPT, s.nchunks,
+            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d | x YT=%d PPT=%d warps=%d chunks=%d | fwd all=%d NL=%d thr=%d\n",
+                    sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.YT, s.PPT, s.xw, s.nchunks,
                     s.fwd.all, s.fwd.NL, s.fwd.thr);
     }
     if (h->cfg.pressure && h->g.n3 <= 256) {

@@ -1,0 +1,111 @@
+"""Kernel families the autotuner chooses between, each forced and checked.
+
+The autotuner keeps whichever variant is fastest on the device, so the parity
+tests elsewhere exercise only the winners.  Here BLD_X_KERNEL forces the
+advection x pass to the warp-per-row kernel (register transforms with lane
+shuffles) or to the block kernel (shared-memory Stockham stages), and each is
+compared with the oracle at the plain form's 1e-12 and the mixed form's 1e-5,
+over every radix the warp kernel is compiled for.
+"""
+
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def BLD():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    import BoundaryLayerDynamics as B
+    return B
+
+
+def _build(api, res, precision=None, les=False):
+    size = (2 * math.pi, math.pi, 1.0) if les else (4 * math.pi, 2 * math.pi, 2.0)
+    if les:
+        dom = api.Domain(size, api.RoughWall(1e-4), api.FreeSlipBoundary())
+        procs = api.incompressible_flow(1e-5, constant_forcing=1, sgs_model=api.StaticSmagorinskyModel())
+    else:
+        dom = api.Domain(size, api.SmoothWall(), api.SmoothWall())
+        procs = api.incompressible_flow(1 / 180, constant_forcing=1)
+    kw = {} if precision is None else dict(precision=precision)
+    return api.Model(res, dom, procs, **kw)
+
+
+def _forced(BLD, family, res, precision, les=False):
+    old = os.environ.get("BLD_X_KERNEL")
+    os.environ["BLD_X_KERNEL"] = family
+    try:
+        return _build(BLD, res, precision, les)
+    finally:
+        if old is None:
+            del os.environ["BLD_X_KERNEL"]
+        else:
+            os.environ["BLD_X_KERNEL"] = old
+
+
+def _state(om, seed):
+    rng = np.random.default_rng(seed)
+    st = {}
+    for f in om.fields:
+        shape = om.state[f].shape
+        k1 = np.arange(shape[2])[None, None, :]
+        k2 = np.abs(om.grid.wavenumbers(2))[None, :, None]
+        st[f] = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) / (1.0 + k1 ** 2 + k2 ** 2)
+    om.apply_projections(st)
+    return st
+
+
+# (resolution, precision, tolerance): P1 = 96 (radix 3), 192 (6), 288 (9), 384 (12), 64 (2), 128 (4), 256 (8)
+CASES = [
+    ((64, 12, 6), "fp64", 1e-12),
+    ((128, 10, 5), "fp64", 1e-12),
+    ((43, 12, 6), "fp64", 1e-12),       # k1max = 21: P1 = 64, radix 2 (explicit 3k+1 rule)
+    ((85, 10, 5), "fp64", 1e-12),       # k1max = 42: P1 = 128, radix 4
+    ((64, 12, 6), "mixed", 1e-5),
+    ((192, 8, 5), "mixed", 1e-5),
+    ((256, 6, 4), "mixed", 1e-5),
+    ((171, 6, 4), "mixed", 1e-5),       # k1max = 85: P1 = 256, radix 8
+]
+
+
+@pytest.mark.parametrize("res,precision,tol", CASES)
+@pytest.mark.parametrize("family", ["warp", "block"])
+def test_advection_x_kernel_family(oracle, BLD, res, precision, tol, family):
+    om = _build(oracle, res)
+    gm = _forced(BLD, family, res, precision)
+    if family == "warp":
+        assert gm.info.adv_p1 % 32 == 0
+    st = _state(om, seed=sum(res))
+    ref = om.compute_rates(st)
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < tol, (res, precision, family, gm.info.adv_p1, f, e)
+
+
+def test_warp_kernel_les_mixed_trajectory(oracle, BLD):
+    """The warp advection kernel inside a full LES step sequence (mixed form)."""
+    res = (64, 64, 16)
+    om = _build(oracle, res, les=True)
+    gm = _forced(BLD, "warp", res, "mixed", les=True)
+    st = _state(om, seed=5)
+    for f in st:
+        st[f] *= 5.0
+    gm.set_state(st)
+    for f in om.fields:
+        om.state[f][...] = st[f]
+    gm.evolve(10 * 1e-4, 1e-4)
+    om.evolve(10 * 1e-4, 1e-4)
+    got = gm.state
+    for f in om.fields:
+        e = rel_l2(got[f], om.state[f])
+        assert e < 1e-5, (f, e)
