@@ -119,7 +119,11 @@ struct YCfg {
     int all = 0;
     int NL = 4;    // k1 lines per term (per field and line set)
     int thr = 256;
+    int wfft = 0;  // per-term kernels: radix of the warp transform (P2 = 32 wfft), 0 = block stages
 };
+
+// radices of the warp y transforms compiled for the per-term y kernels
+bool wfft_radix_ok(int r) { return r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 9 || r == 12 || r == 16; }
 
 struct Space {
     bool on = false;
@@ -131,6 +135,7 @@ struct Space {
     long long min_ms = 0, mout_ms = 0;  // elements per member
     int YT = 1, PPT = 1, zchunk = 1, nchunks = 1;  // x kernels: rows per block, points per thread, z chunks
     int xw = 0;                                     // > 0: warp-per-row x kernel with xw warps per block
+    bool xb = false;                                // block of three warps per row (advection)
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
 };
@@ -243,7 +248,7 @@ int pick_y(int P2, bool fp32, int sets) {
 // fill the GPU a few times over, at least 8 layers per chunk
 void x_chunks(const bld_handle* h, Space& s) {
     const int n3 = h->g.n3;
-    const int rows = s.xw ? s.xw : s.YT;
+    const int rows = s.xb ? 1 : (s.xw ? s.xw : s.YT);
     const long long blocks_per_chunk = (long long)((s.P2 + rows - 1) / rows) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
     want = std::min(want, std::max(1, n3 / 8));
@@ -326,7 +331,19 @@ int launch_inv_y(bld_handle* h, const Space& s, InvYArgs a, int nm) {
         k_inv_y_all<R><<<grid, c.thr, (size_t)(s.P2 + s.P2 * a.nterms * c.NL) * cs, h->stream>>>(a);
     } else {
         dim3 grid(a.nterms * nm, (h->g.K1 + c.NL - 1) / c.NL, h->g.n3);
-        k_inv_y<R><<<grid, c.thr, (size_t)(s.P2 + 2 * s.P2 * c.NL) * cs, h->stream>>>(a);
+        const size_t sm = (size_t)(s.P2 + 2 * s.P2 * c.NL) * cs;
+        switch (c.wfft) {
+            case 0: k_inv_y<R, 0><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 2: k_inv_y<R, 2><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 3: k_inv_y<R, 3><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 4: k_inv_y<R, 4><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 6: k_inv_y<R, 6><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 8: k_inv_y<R, 8><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 9: k_inv_y<R, 9><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 12: k_inv_y<R, 12><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 16: k_inv_y<R, 16><<<grid, c.thr, sm, h->stream>>>(a); break;
+            default: return fail(BLD_ERR_INVALID_CONFIG, "no warp y transform of radix %d", c.wfft);
+        }
     }
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
@@ -342,7 +359,19 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
         k_fwd_y_all<R><<<grid, c.thr, (size_t)(s.P2 + s.P2 * 3 * s.fsets * c.NL) * cs, h->stream>>>(a);
     } else {
         dim3 grid(a.fields * nm, (h->g.K1 + c.NL - 1) / c.NL, h->g.n3);
-        k_fwd_y<R><<<grid, c.thr, (size_t)(s.P2 + 2 * s.P2 * s.fsets * c.NL) * cs, h->stream>>>(a);
+        const size_t sm = (size_t)(s.P2 + 2 * s.P2 * s.fsets * c.NL) * cs;
+        switch (c.wfft) {
+            case 0: k_fwd_y<R, 0><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 2: k_fwd_y<R, 2><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 3: k_fwd_y<R, 3><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 4: k_fwd_y<R, 4><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 6: k_fwd_y<R, 6><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 8: k_fwd_y<R, 8><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 9: k_fwd_y<R, 9><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 12: k_fwd_y<R, 12><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 16: k_fwd_y<R, 16><<<grid, c.thr, sm, h->stream>>>(a); break;
+            default: return fail(BLD_ERR_INVALID_CONFIG, "no warp y transform of radix %d", c.wfft);
+        }
     }
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
@@ -399,6 +428,31 @@ int launch_adv_xw(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     return BLD_OK;
 }
 
+int xb_radix(int P1) {
+    if (P1 % 32) return 0;
+    const int r = P1 / 32;
+    return (r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 9 || r == 12) ? r : 0;
+}
+
+template <typename R>
+int launch_adv_xb(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    const int r = xb_radix(s.P1);
+    dim3 grid(s.P2, s.nchunks, nm);
+    const size_t sm = ((size_t)r * 32 + 3 * (size_t)s.P1 + 12 * (size_t)h->g.K1) * csize(sizeof(R) == 4);
+    switch (r) {
+        case 2: k_adv_xb<R, 2><<<grid, 96, sm, h->stream>>>(a); break;
+        case 3: k_adv_xb<R, 3><<<grid, 96, sm, h->stream>>>(a); break;
+        case 4: k_adv_xb<R, 4><<<grid, 96, sm, h->stream>>>(a); break;
+        case 6: k_adv_xb<R, 6><<<grid, 96, sm, h->stream>>>(a); break;
+        case 8: k_adv_xb<R, 8><<<grid, 96, sm, h->stream>>>(a); break;
+        case 9: k_adv_xb<R, 9><<<grid, 96, sm, h->stream>>>(a); break;
+        case 12: k_adv_xb<R, 12><<<grid, 96, sm, h->stream>>>(a); break;
+        default: return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", s.P1);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
 template <typename R>
 int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     dim3 grid(s.P2 / s.YT, s.nchunks, nm);
@@ -425,8 +479,24 @@ int set_smem_limits_R() {
         CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributePreferredSharedMemoryCarveout,     \
                                       cudaSharedmemCarveoutMaxShared));                      \
     } while (0)
-    BLD_SET((k_inv_y<R>));
-    BLD_SET((k_fwd_y<R>));
+    BLD_SET((k_inv_y<R, 0>));
+    BLD_SET((k_fwd_y<R, 0>));
+    BLD_SET((k_inv_y<R, 2>));
+    BLD_SET((k_fwd_y<R, 2>));
+    BLD_SET((k_inv_y<R, 3>));
+    BLD_SET((k_fwd_y<R, 3>));
+    BLD_SET((k_inv_y<R, 4>));
+    BLD_SET((k_fwd_y<R, 4>));
+    BLD_SET((k_inv_y<R, 6>));
+    BLD_SET((k_fwd_y<R, 6>));
+    BLD_SET((k_inv_y<R, 8>));
+    BLD_SET((k_fwd_y<R, 8>));
+    BLD_SET((k_inv_y<R, 9>));
+    BLD_SET((k_fwd_y<R, 9>));
+    BLD_SET((k_inv_y<R, 12>));
+    BLD_SET((k_fwd_y<R, 12>));
+    BLD_SET((k_inv_y<R, 16>));
+    BLD_SET((k_fwd_y<R, 16>));
     BLD_SET((k_inv_y_all<R>));
     BLD_SET((k_fwd_y_all<R>));
     BLD_SET((k_adv_x<R, 1>));
@@ -437,6 +507,13 @@ int set_smem_limits_R() {
     BLD_SET((k_sgs_x<R, 2>));
     BLD_SET((k_sgs_x<R, 3>));
     BLD_SET((k_sgs_x<R, 4>));
+    BLD_SET((k_adv_xb<R, 2>));
+    BLD_SET((k_adv_xb<R, 3>));
+    BLD_SET((k_adv_xb<R, 4>));
+    BLD_SET((k_adv_xb<R, 6>));
+    BLD_SET((k_adv_xb<R, 8>));
+    BLD_SET((k_adv_xb<R, 9>));
+    BLD_SET((k_adv_xb<R, 12>));
     BLD_SET((k_adv_xw<R, 2>));
     BLD_SET((k_adv_xw<R, 3>));
     BLD_SET((k_adv_xw<R, 4>));
@@ -550,7 +627,10 @@ int enqueue_x_R(bld_handle* h, int sp, int m0, int nm) {
     xa.w_lo = h->w_lo;
     xa.w_hi = h->w_hi;
     xa.active = h->mask_on ? h->active : nullptr;
-    if (sp == 0) return s.xw ? launch_adv_xw<R>(h, s, xa, nm) : launch_adv_x<R>(h, s, xa, nm);
+    if (sp == 0) {
+        if (s.xb) return launch_adv_xb<R>(h, s, xa, nm);
+        return s.xw ? launch_adv_xw<R>(h, s, xa, nm) : launch_adv_x<R>(h, s, xa, nm);
+    }
     return launch_sgs_x<R>(h, s, xa, nm);
 }
 
@@ -634,6 +714,16 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
                     const double2* dp, double2* out, int m0, int nm);
 
 // ------------------------------------------------------------------ autotuner
+// BLD_Y_KERNEL=block keeps the y passes on block-wide Stockham stages
+bool ydisable_warp() {
+    const char* e = getenv("BLD_Y_KERNEL");
+    return e && !strcmp(e, "block");
+}
+bool yforce_warp() {
+    const char* e = getenv("BLD_Y_KERNEL");
+    return e && !strcmp(e, "warp");
+}
+
 // y-pass candidates: per-term blocks (two-buffer FFT) with several line counts
 // and block sizes, and all-terms blocks (in-place FFT); lines * element size of
 // at least 32 bytes keeps global accesses sector-sized
@@ -647,13 +737,19 @@ std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_pe
         for (int i = 0; i < 3; ++i) {
             bool dup = false;
             for (int k = 0; k < i; ++k) dup |= thrs[k] == thrs[i];
-            if (!dup) out.push_back(YCfg{0, nl, thrs[i]});
+            const bool warp_possible = wfft_radix_ok(s.P2 % 32 ? 0 : s.P2 / 32);
+            if (!dup && !(yforce_warp() && warp_possible)) out.push_back(YCfg{0, nl, thrs[i], 0});
+        }
+        const int wr = s.P2 % 32 ? 0 : s.P2 / 32;
+        if (wfft_radix_ok(wr) && !ydisable_warp()) {
+            out.push_back(YCfg{0, nl, 128, wr});
+            out.push_back(YCfg{0, nl, 256, wr});
         }
     }
     const int nls_all[2] = {h->fp32 ? 2 : 1, h->fp32 ? 4 : 2};
     for (int nl : nls_all) {
         const int thr = inplace_threads(s.plan2, all_lines_per_nl * nl);
-        if (thr && (size_t)(s.P2 + s.P2 * all_lines_per_nl * nl) * cs <= 150 * 1024) out.push_back(YCfg{1, nl, thr});
+        if (thr && !yforce_warp() && (size_t)(s.P2 + s.P2 * all_lines_per_nl * nl) * cs <= 150 * 1024) out.push_back(YCfg{1, nl, thr, 0});
     }
     return out;
 }
@@ -684,12 +780,19 @@ int autotune(bld_handle* h) {
     // BLD_X_KERNEL=warp|block restricts the advection x kernel to one family
     const char* xk = getenv("BLD_X_KERNEL");
     const bool only_warp = xk && !strcmp(xk, "warp"), only_block = xk && !strcmp(xk, "block");
+    const bool only_bw = xk && !strcmp(xk, "blockwarp");
+    const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1) > 0;
+    if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
     const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
     if (only_warp && !adv_warp_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no warp x kernel for P1=%d", h->adv.P1);
     const char* env = getenv("BLD_NO_AUTOTUNE");
     if (env && env[0] && env[0] != '0') {
         if (only_warp && adv_warp_ok) {
             h->adv.xw = 4;
+            x_chunks(h, h->adv);
+        }
+        if (only_bw && adv_bw_ok) {
+            h->adv.xb = true;
             x_chunks(h, h->adv);
         }
         return BLD_OK;
@@ -713,7 +816,7 @@ int autotune(bld_handle* h) {
         best = 1e30f;
         int byt = s.YT, bppt = s.PPT;
         for (auto c : x_candidates(h, s, sp == 0)) {
-            if (sp == 0 && only_warp) break;
+            if (sp == 0 && (only_warp || only_bw)) break;
             s.YT = c.first;
             s.PPT = c.second;
             x_chunks(h, s);
@@ -725,7 +828,7 @@ int autotune(bld_handle* h) {
             }
         }
         int bxw = 0;
-        const bool warp_ok = sp == 0 && adv_warp_ok && !only_block;
+        const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw;
         for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) {
             s.xw = wpb;
             x_chunks(h, s);
@@ -735,6 +838,19 @@ int autotune(bld_handle* h) {
                 bxw = wpb;
             }
         }
+        s.xw = 0;
+        bool bxb = false;
+        if (sp == 0 && adv_bw_ok && !only_block && !only_warp) {
+            s.xb = true;
+            x_chunks(h, s);
+            BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
+            if (t < best) {
+                best = t;
+                bxb = true;
+                bxw = 0;
+            }
+        }
+        s.xb = bxb;
         s.xw = bxw;
         s.YT = byt;
         s.PPT = bppt;
@@ -752,9 +868,9 @@ int autotune(bld_handle* h) {
         s.fwd = bf;
         const char* v = getenv("BLD_VERBOSE");
         if (v && v[0] && v[0] != '0')
-            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d | x YT=%d PPT=%d warps=%d chunks=%d | fwd all=%d NL=%d thr=%d\n",
-                    sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.YT, s.PPT, s.xw, s.nchunks,
-                    s.fwd.all, s.fwd.NL, s.fwd.thr);
+            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d wfft=%d | x YT=%d PPT=%d warps=%d bw=%d chunks=%d | fwd all=%d NL=%d thr=%d wfft=%d\n",
+                    sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.inv.wfft, s.YT, s.PPT, s.xw, (int)s.xb,
+                    s.nchunks, s.fwd.all, s.fwd.NL, s.fwd.thr, s.fwd.wfft);
     }
     if (h->cfg.pressure && h->g.n3 <= 256) {
         float best = 1e30f, t = 0;

@@ -17,6 +17,7 @@
 
 #include "bld_fft.cuh"
 #include "bld_dft.cuh"
+#include "bld_warpfft.cuh"
 
 #define BLD_MAXT 10
 #define BLD_MAXC 4
@@ -123,10 +124,14 @@ __device__ __forceinline__ double2 inv_term_value(const InvYArgs& a, const doubl
 // grid (nterms*members, ceil(K1/NL), n3): the terms of one (layer, k1 tile) are
 // neighbouring blocks, so their shared state reads (vorticity needs z and z+1)
 // hit L2.  smem: tw[P2] + 2*P2*NL complex.
-template <typename R>
+// RAD > 0: the transform runs one line per warp in registers (P2 = 32 RAD)
+// on a line stride padded to NL + 1, instead of block-wide Stockham stages.
+template <typename R, int RAD>
 __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
     using C = cplx<R>;
     const int NL = a.NL;
+    const int LS = RAD ? NL + 1 : NL;   // stride of a position in the line buffer
+    const int nls = __ffs(NL) - 1;     // NL is a power of two
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* b0 = tw + a.P2;
@@ -144,8 +149,8 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
     const double2* S = a.state + (long long)m * a.g.mstride;
     // zero the padding band, then gather the K2*NL modes in batches of 8 per thread
     for (int i = threadIdx.x; i < (P2 - K2) * NL; i += blockDim.x) {
-        const int p = k2max + 1 + i / NL, l = i % NL;
-        b0[p * NL + l] = mk<R>(0, 0);
+        const int p = k2max + 1 + (i >> nls), l = i & (NL - 1);
+        b0[p * LS + l] = mk<R>(0, 0);
     }
     constexpr int BATCH = 8;
     const int nmodes = K2 * NL;
@@ -156,7 +161,7 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
             const int i = i0 + q * blockDim.x + threadIdx.x;
             v[q] = make_double2(0.0, 0.0);
             if (i < nmodes) {
-                const int j = i / NL, l = i - j * NL, k1 = k10 + l;
+                const int j = i >> nls, l = i & (NL - 1), k1 = k10 + l;
                 if (k1 < K1) v[q] = inv_term_value(a, S, op, f, z, j, k1);
             }
         }
@@ -164,18 +169,35 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
         for (int q = 0; q < BATCH; ++q) {
             const int i = i0 + q * blockDim.x + threadIdx.x;
             if (i < nmodes) {
-                const int j = i / NL, l = i - j * NL;
+                const int j = i >> nls, l = i & (NL - 1);
                 const int p = (j <= k2max) ? j : P2 - (K2 - j);
-                b0[p * NL + l] = mk<R>((R)v[q].x, (R)v[q].y);
+                b0[p * LS + l] = mk<R>((R)v[q].x, (R)v[q].y);
             }
         }
     }
     __syncthreads();
-    C* res = fft_big<R, +1>(b0, b1, NL, 1, NL, false, a.plan, tw);
+    C* res = b0;
+    if constexpr (RAD > 0) {
+        const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        const int brl = (int)(__brev((unsigned)lane) >> 27);
+        LaneTw<R> lt;
+        lane_twiddles_tab<R>(lt, lane, tw, P2);
+        for (int l = threadIdx.x >> 5; l < NL; l += nw) {
+            C zl[RAD];
+#pragma unroll
+            for (int q = 0; q < RAD; ++q) zl[q] = b0[(lane + 32 * q) * LS + l];
+            inverse_line<R, RAD>(zl, lane, tw, lane, lt);
+#pragma unroll
+            for (int k = 0; k < RAD; ++k) b0[(k + RAD * brl) * LS + l] = zl[k];
+        }
+        __syncthreads();
+    } else {
+        res = fft_big<R, +1>(b0, b1, NL, 1, NL, false, a.plan, tw);
+    }
     C* out = reinterpret_cast<C*>(a.mixed) + (long long)m * a.mixed_mstride + (long long)(t * a.g.n3 + z) * P2 * K1;
     for (int i = threadIdx.x; i < P2 * NL; i += blockDim.x) {
-        const int y = i / NL, l = i - y * NL, k1 = k10 + l;
-        if (k1 < K1) out[(long long)y * K1 + k1] = res[i];
+        const int y = i >> nls, l = i & (NL - 1), k1 = k10 + l;
+        if (k1 < K1) out[(long long)y * K1 + k1] = res[y * LS + l];
     }
 }
 
@@ -219,6 +241,7 @@ __global__ void __launch_bounds__(384) k_inv_y_all(InvYArgs a) {
     const Geo& g = a.g;
     const int K1 = g.K1, K2 = g.K2, k2max = g.k2max, P2 = a.P2, n3 = g.n3;
     const int k10 = blockIdx.x * NL;
+    const int nls = __ffs(NL) - 1;   // NL is a power of two
     const int z = blockIdx.y;
     const int m = a.m0 + blockIdx.z;
     BLD_SKIP_INACTIVE(a, m);
@@ -251,7 +274,7 @@ __global__ void __launch_bounds__(384) k_inv_y_all(InvYArgs a) {
 #pragma unroll
         for (int q = 0; q < B; ++q) {
             const int i = i0 + q * blockDim.x + threadIdx.x;
-            const int j = i / NL, l = i - j * NL, k1 = k10 + l;
+            const int j = i >> nls, l = i & (NL - 1), k1 = k10 + l;
             u[q] = v[q] = w[q] = u1[q] = v1[q] = make_double2(0.0, 0.0);
             if (i < nmodes && k1 < K1) {
                 const long long mo = (long long)j * K1 + k1;
@@ -268,7 +291,7 @@ __global__ void __launch_bounds__(384) k_inv_y_all(InvYArgs a) {
         for (int q = 0; q < B; ++q) {
             const int i = i0 + q * blockDim.x + threadIdx.x;
             if (i >= nmodes) continue;
-            const int j = i / NL, l = i - j * NL, k1 = k10 + l;
+            const int j = i >> nls, l = i & (NL - 1), k1 = k10 + l;
             const int p = (j <= k2max) ? j : P2 - (K2 - j);
             const bool ok = k1 < K1;
             const double e1 = ok ? a.d1[k1] : 0.0, e2 = a.d2[j];
@@ -912,7 +935,8 @@ __device__ __forceinline__ double2 linear_terms_w(const Geo& g, const Linear& L,
 }
 
 // grid (fields*members, ceil(K1/NL), n3); smem tw[P2] + 2*P2*nlines complex (nlines = NL or 2NL)
-template <typename R>
+// RAD > 0: one line per warp in registers on a padded line stride (see k_inv_y)
+template <typename R, int RAD>
 __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     using C = cplx<R>;
     const int NL = a.NL;
@@ -930,6 +954,8 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     bool hasB = false;
     for (int ci = 0; ci < nc; ++ci) hasB |= (a.c[fi][ci].pref == 2);
     const int nlines = hasB ? 2 * NL : NL;
+    const int LS = RAD ? nlines + 1 : nlines;                 // stride of a position in the line buffer
+    const int nls = __ffs(NL) - 1, nlsl = __ffs(nlines) - 1;   // NL and nlines are powers of two
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* b0 = tw + P2;
     C* b1 = b0 + P2 * nlines;
@@ -947,7 +973,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
             const int i = i0 + q * blockDim.x + threadIdx.x;
             v[q] = mk<R>(0, 0);
             if (i < nval) {
-                const int y = i / nlines, l = i - y * nlines;
+                const int y = i >> nlsl, l = i & (nlines - 1);
                 const bool isB = l >= NL;
                 const int k1 = k10 + (isB ? l - NL : l);
                 if (k1 < K1) {
@@ -970,11 +996,31 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
 #pragma unroll
         for (int q = 0; q < BATCH; ++q) {
             const int i = i0 + q * blockDim.x + threadIdx.x;
-            if (i < nval) b0[i] = v[q];
+            if (i < nval) {
+                const int y = i >> nlsl, l = i & (nlines - 1);
+                b0[y * LS + l] = v[q];
+            }
         }
     }
     __syncthreads();
-    const C* res = fft_big<R, -1>(b0, b1, nlines, 1, nlines, false, a.plan, tw);
+    const C* res = b0;
+    if constexpr (RAD > 0) {
+        const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        const int brl = (int)(__brev((unsigned)lane) >> 27);
+        LaneTw<R> lt;
+        lane_twiddles_tab<R>(lt, lane, tw, P2);
+        for (int l = threadIdx.x >> 5; l < nlines; l += nw) {
+            C zl[RAD];
+#pragma unroll
+            for (int k = 0; k < RAD; ++k) zl[k] = b0[(k + RAD * brl) * LS + l];
+            forward_line<R, RAD>(zl, lane, tw, lane, lt);
+#pragma unroll
+            for (int b = 0; b < RAD; ++b) b0[(lane + 32 * b) * LS + l] = zl[b];
+        }
+        __syncthreads();
+    } else {
+        res = fft_big<R, -1>(b0, b1, nlines, 1, nlines, false, a.plan, tw);
+    }
     double2* du = a.du + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F;
     const double2* Sf = a.state ? a.state + (long long)m * g.mstride + fld_off(g, f) : nullptr;
     const bool need_win = (a.mode == 1) && a.lin.diff_on[f];
@@ -989,7 +1035,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
 #pragma unroll
         for (int q = 0; q < OB; ++q) {
             const int o = o0 + q * blockDim.x + threadIdx.x;
-            const int j = o / NL, l = o - j * NL, k1 = k10 + l;
+            const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
             if (o < nout && k1 < K1) {
                 const long long idx = (long long)j * K1 + k1;
                 if (need_win) {
@@ -1003,13 +1049,13 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
 #pragma unroll
         for (int q = 0; q < OB; ++q) {
             const int o = o0 + q * blockDim.x + threadIdx.x;
-            const int j = o / NL, l = o - j * NL, k1 = k10 + l;
+            const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
             if (o >= nout || k1 >= K1) continue;
             const int pos = (j <= k2max) ? j : P2 - (K2 - j);
-            const C X = res[pos * nlines + l];
+            const C X = res[pos * LS + l];
             double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
             if (hasB) {
-                const C Y = res[pos * nlines + NL + l];
+                const C Y = res[pos * LS + NL + l];
                 const double d = a.d2[j];
                 const double bx = (double)Y.x * a.inv_n, by = (double)Y.y * a.inv_n;
                 vx += -d * by;
