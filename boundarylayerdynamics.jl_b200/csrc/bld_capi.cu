@@ -136,6 +136,7 @@ struct Space {
     int YT = 1, PPT = 1, zchunk = 1, nchunks = 1;  // x kernels: rows per block, points per thread, z chunks
     int xw = 0;                                     // > 0: warp-per-row x kernel with xw warps per block
     bool xb = false;                                // block of three warps per row (advection)
+    int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
 };
@@ -377,16 +378,39 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
     return BLD_OK;
 }
 
+// radices of the warp line transforms compiled into the block x kernels, and the
+// points per thread that go with each (so that YT * 32 RAD / PPT threads are whole warps)
+bool xr_radix_ok(int r) { return r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 9 || r == 12 || r == 16 || r == 24; }
+constexpr int xr_ppt(int r) { return r <= 4 ? 1 : r <= 8 ? 2 : r <= 12 ? 3 : 4; }
+
+#define BLD_XR_CASES(KERNEL)                                                                          \
+    case 2: KERNEL<R, xr_ppt(2), 2><<<grid, thr, sm, h->stream>>>(a); break;                         \
+    case 3: KERNEL<R, xr_ppt(3), 3><<<grid, thr, sm, h->stream>>>(a); break;                         \
+    case 4: KERNEL<R, xr_ppt(4), 4><<<grid, thr, sm, h->stream>>>(a); break;                         \
+    case 6: KERNEL<R, xr_ppt(6), 6><<<grid, thr, sm, h->stream>>>(a); break;                         \
+    case 8: KERNEL<R, xr_ppt(8), 8><<<grid, thr, sm, h->stream>>>(a); break;                         \
+    case 9: KERNEL<R, xr_ppt(9), 9><<<grid, thr, sm, h->stream>>>(a); break;                         \
+    case 12: KERNEL<R, xr_ppt(12), 12><<<grid, thr, sm, h->stream>>>(a); break;                      \
+    case 16: KERNEL<R, xr_ppt(16), 16><<<grid, thr, sm, h->stream>>>(a); break;                      \
+    case 24: KERNEL<R, xr_ppt(24), 24><<<grid, thr, sm, h->stream>>>(a); break;
+
 template <typename R>
 int launch_adv_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     dim3 grid(s.P2 / s.YT, s.nchunks, nm);
     const int thr = s.YT * s.P1 / s.PPT;
     const size_t sm = smem_adv(s, sizeof(R) == 4);
-    switch (s.PPT) {
-        case 1: k_adv_x<R, 1><<<grid, thr, sm, h->stream>>>(a); break;
-        case 2: k_adv_x<R, 2><<<grid, thr, sm, h->stream>>>(a); break;
-        case 3: k_adv_x<R, 3><<<grid, thr, sm, h->stream>>>(a); break;
-        default: k_adv_x<R, 4><<<grid, thr, sm, h->stream>>>(a); break;
+    if (s.xr) {
+        switch (s.xr) {
+            BLD_XR_CASES(k_adv_x)
+            default: return fail(BLD_ERR_INVALID_CONFIG, "no warp x transform of radix %d", s.xr);
+        }
+    } else {
+        switch (s.PPT) {
+            case 1: k_adv_x<R, 1, 0><<<grid, thr, sm, h->stream>>>(a); break;
+            case 2: k_adv_x<R, 2, 0><<<grid, thr, sm, h->stream>>>(a); break;
+            case 3: k_adv_x<R, 3, 0><<<grid, thr, sm, h->stream>>>(a); break;
+            default: k_adv_x<R, 4, 0><<<grid, thr, sm, h->stream>>>(a); break;
+        }
     }
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
@@ -458,11 +482,18 @@ int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     dim3 grid(s.P2 / s.YT, s.nchunks, nm);
     const int thr = s.YT * s.P1 / s.PPT;
     const size_t sm = smem_sgs(s, sizeof(R) == 4);
-    switch (s.PPT) {
-        case 1: k_sgs_x<R, 1><<<grid, thr, sm, h->stream>>>(a); break;
-        case 2: k_sgs_x<R, 2><<<grid, thr, sm, h->stream>>>(a); break;
-        case 3: k_sgs_x<R, 3><<<grid, thr, sm, h->stream>>>(a); break;
-        default: k_sgs_x<R, 4><<<grid, thr, sm, h->stream>>>(a); break;
+    if (s.xr) {
+        switch (s.xr) {
+            BLD_XR_CASES(k_sgs_x)
+            default: return fail(BLD_ERR_INVALID_CONFIG, "no warp x transform of radix %d", s.xr);
+        }
+    } else {
+        switch (s.PPT) {
+            case 1: k_sgs_x<R, 1, 0><<<grid, thr, sm, h->stream>>>(a); break;
+            case 2: k_sgs_x<R, 2, 0><<<grid, thr, sm, h->stream>>>(a); break;
+            case 3: k_sgs_x<R, 3, 0><<<grid, thr, sm, h->stream>>>(a); break;
+            default: k_sgs_x<R, 4, 0><<<grid, thr, sm, h->stream>>>(a); break;
+        }
     }
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
@@ -499,14 +530,27 @@ int set_smem_limits_R() {
     BLD_SET((k_fwd_y<R, 16>));
     BLD_SET((k_inv_y_all<R>));
     BLD_SET((k_fwd_y_all<R>));
-    BLD_SET((k_adv_x<R, 1>));
-    BLD_SET((k_adv_x<R, 2>));
-    BLD_SET((k_adv_x<R, 3>));
-    BLD_SET((k_adv_x<R, 4>));
-    BLD_SET((k_sgs_x<R, 1>));
-    BLD_SET((k_sgs_x<R, 2>));
-    BLD_SET((k_sgs_x<R, 3>));
-    BLD_SET((k_sgs_x<R, 4>));
+    BLD_SET((k_adv_x<R, 1, 0>));
+    BLD_SET((k_adv_x<R, 2, 0>));
+    BLD_SET((k_adv_x<R, 3, 0>));
+    BLD_SET((k_adv_x<R, 4, 0>));
+    BLD_SET((k_sgs_x<R, 1, 0>));
+    BLD_SET((k_sgs_x<R, 2, 0>));
+    BLD_SET((k_sgs_x<R, 3, 0>));
+    BLD_SET((k_sgs_x<R, 4, 0>));
+#define BLD_SET_XR(r)                              \
+    BLD_SET((k_adv_x<R, xr_ppt(r), r>));           \
+    BLD_SET((k_sgs_x<R, xr_ppt(r), r>));
+    BLD_SET_XR(2)
+    BLD_SET_XR(3)
+    BLD_SET_XR(4)
+    BLD_SET_XR(6)
+    BLD_SET_XR(8)
+    BLD_SET_XR(9)
+    BLD_SET_XR(12)
+    BLD_SET_XR(16)
+    BLD_SET_XR(24)
+#undef BLD_SET_XR
     BLD_SET((k_adv_xb<R, 2>));
     BLD_SET((k_adv_xb<R, 3>));
     BLD_SET((k_adv_xb<R, 4>));
@@ -714,6 +758,12 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
                     const double2* dp, double2* out, int m0, int nm);
 
 // ------------------------------------------------------------------ autotuner
+// BLD_X_LINES=block keeps the block x kernels on block-wide Stockham stages
+bool xdisable_wlines() {
+    const char* e = getenv("BLD_X_LINES");
+    return e && !strcmp(e, "block");
+}
+
 // BLD_Y_KERNEL=block keeps the y passes on block-wide Stockham stages
 bool ydisable_warp() {
     const char* e = getenv("BLD_Y_KERNEL");
@@ -781,6 +831,7 @@ int autotune(bld_handle* h) {
     const char* xk = getenv("BLD_X_KERNEL");
     const bool only_warp = xk && !strcmp(xk, "warp"), only_block = xk && !strcmp(xk, "block");
     const bool only_bw = xk && !strcmp(xk, "blockwarp");
+    const bool only_lines = xk && !strcmp(xk, "lines");   // block kernels with warp line transforms
     const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1) > 0;
     if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
     const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
@@ -816,7 +867,7 @@ int autotune(bld_handle* h) {
         best = 1e30f;
         int byt = s.YT, bppt = s.PPT;
         for (auto c : x_candidates(h, s, sp == 0)) {
-            if (sp == 0 && (only_warp || only_bw)) break;
+            if ((sp == 0 && (only_warp || only_bw)) || only_lines) break;
             s.YT = c.first;
             s.PPT = c.second;
             x_chunks(h, s);
@@ -827,8 +878,29 @@ int autotune(bld_handle* h) {
                 bppt = c.second;
             }
         }
+        // block x kernels with warp line transforms (YT = 1, 2)
+        int bxr = 0;
+        const int xrr = s.P1 % 32 ? 0 : s.P1 / 32;
+        if (xr_radix_ok(xrr) && !(sp == 0 && (only_warp || only_bw)) && !only_block && !xdisable_wlines()) {
+            for (int yt = 1; yt <= 2; ++yt) {
+                const size_t smx = (size_t)(s.P1 + 2 * (sp == 0 ? 3 : 5) * yt * s.P1) * csize(h->fp32);
+                if (s.P2 % yt || smx > 150 * 1024 || yt * s.P1 / xr_ppt(xrr) > 256) continue;
+                s.xr = xrr;
+                s.YT = yt;
+                s.PPT = xr_ppt(xrr);
+                x_chunks(h, s);
+                BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
+                if (t < best) {
+                    best = t;
+                    bxr = xrr;
+                    byt = yt;
+                    bppt = xr_ppt(xrr);
+                }
+            }
+            s.xr = 0;
+        }
         int bxw = 0;
-        const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw;
+        const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw && !only_lines;
         for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) {
             s.xw = wpb;
             x_chunks(h, s);
@@ -836,11 +908,12 @@ int autotune(bld_handle* h) {
             if (t < best) {
                 best = t;
                 bxw = wpb;
+                bxr = 0;
             }
         }
         s.xw = 0;
         bool bxb = false;
-        if (sp == 0 && adv_bw_ok && !only_block && !only_warp) {
+        if (sp == 0 && adv_bw_ok && !only_block && !only_warp && !only_lines) {
             s.xb = true;
             x_chunks(h, s);
             BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
@@ -848,10 +921,12 @@ int autotune(bld_handle* h) {
                 best = t;
                 bxb = true;
                 bxw = 0;
+                bxr = 0;
             }
         }
         s.xb = bxb;
         s.xw = bxw;
+        s.xr = bxr;
         s.YT = byt;
         s.PPT = bppt;
         x_chunks(h, s);
@@ -868,8 +943,8 @@ int autotune(bld_handle* h) {
         s.fwd = bf;
         const char* v = getenv("BLD_VERBOSE");
         if (v && v[0] && v[0] != '0')
-            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d wfft=%d | x YT=%d PPT=%d warps=%d bw=%d chunks=%d | fwd all=%d NL=%d thr=%d wfft=%d\n",
-                    sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.inv.wfft, s.YT, s.PPT, s.xw, (int)s.xb,
+            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d wfft=%d | x YT=%d PPT=%d xr=%d warps=%d bw=%d chunks=%d | fwd all=%d NL=%d thr=%d wfft=%d\n",
+                    sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.inv.wfft, s.YT, s.PPT, s.xr, s.xw, (int)s.xb,
                     s.nchunks, s.fwd.all, s.fwd.NL, s.fwd.thr, s.fwd.wfft);
     }
     if (h->cfg.pressure && h->g.n3 <= 256) {

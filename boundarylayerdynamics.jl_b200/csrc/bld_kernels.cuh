@@ -383,7 +383,8 @@ __device__ __forceinline__ void unpack_pair(const cplx<R>* line, int k, int P1, 
 // Inputs: terms 0 u, 1 v, 5 vort3 (C); 2 w, 3 vort1, 4 vort2 (I).
 // Outputs: 0 adv1, 1 adv2 (C); 2 adv3 (I).
 // grid (P2/YT, nchunks, members), block YT*P1/PPT <= 256 threads.
-template <typename R, int PPT>
+// RAD > 0: the x transforms run one line per warp in registers (P1 = 32 RAD).
+template <typename R, int PPT, int RAD>
 __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -449,7 +450,18 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
             }
         }
         __syncthreads();
-        C* phys = fft_big<R, +1>(bufA, bufB, NLin, P1, 1, true, a.plan, tw);
+        C* phys = bufA;
+        if constexpr (RAD > 0) {
+            warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw);
+            __syncthreads();
+        } else {
+            if constexpr (RAD > 0) {
+                warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw);
+                __syncthreads();
+            } else {
+                phys = fft_big<R, +1>(bufA, bufB, NLin, P1, 1, true, a.plan, tw);
+            }
+        }
         C* outb = (phys == bufA) ? bufB : bufA;
         const bool emitC = (j >= z0);
         const bool emitI = (j >= z0) && (j >= 1);
@@ -496,7 +508,13 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
         }
         if (emitC) {
             __syncthreads();
-            C* r2 = fft_big<R, -1>(outb, phys, NLout, P1, 1, true, a.plan, tw);
+            C* r2 = outb;
+            if constexpr (RAD > 0) {
+                warp_lines_inplace<R, RAD, -1>(outb, NLout, P1, tw);
+                __syncthreads();
+            } else {
+                r2 = fft_big<R, -1>(outb, phys, NLout, P1, 1, true, a.plan, tw);
+            }
             const int nk = k1max + 1;
             for (int i = threadIdx.x; i < NLout * nk; i += nthr) {
                 const int line = i / nk, k = i - line * nk;
@@ -527,7 +545,8 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
 //   5 -d3 tau33 (I -> vel3)    6 -tau13 (I, D1 -> vel3)   7 -tau23 (I, D2 -> vel3)
 // Streaming in z with a two-layer lag: step j loads C layer j and I layer j and
 // completes C layer j-1, I layer j-1 and the d3 tau33 of I layer j-2.
-template <typename R, int PPT>
+// RAD > 0: the x transforms run one line per warp in registers (P1 = 32 RAD).
+template <typename R, int PPT, int RAD>
 __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -605,7 +624,12 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
                 }
             }
             __syncthreads();
-            phys = fft_big<R, +1>(bufA, bufB, NLin, P1, 1, true, a.plan, tw);
+            if constexpr (RAD > 0) {
+                warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw);
+                __syncthreads();
+            } else {
+                phys = fft_big<R, +1>(bufA, bufB, NLin, P1, 1, true, a.plan, tw);
+            }
         }
         C* outb = (phys == bufA) ? bufB : bufA;
         const int c = j - 1;                                   // C layer completed at this step
@@ -724,7 +748,13 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
         }
         if (doC || do5) {
             __syncthreads();
-            C* r2 = fft_big<R, -1>(outb, phys, NLout, P1, 1, true, a.plan, tw);
+            C* r2 = outb;
+            if constexpr (RAD > 0) {
+                warp_lines_inplace<R, RAD, -1>(outb, NLout, P1, tw);
+                __syncthreads();
+            } else {
+                r2 = fft_big<R, -1>(outb, phys, NLout, P1, 1, true, a.plan, tw);
+            }
             const int nk = k1max + 1;
             for (int i = threadIdx.x; i < NLout * nk; i += nthr) {
                 const int line = i / nk, k = i - line * nk;

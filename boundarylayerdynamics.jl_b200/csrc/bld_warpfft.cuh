@@ -182,3 +182,34 @@ __device__ __forceinline__ cplx<R> mirror_mode(const cplx<R> (&z)[RAD], int lane
     return lane == 0 ? z[(RAD - b) % RAD] : other;
 }
 
+
+__device__ __forceinline__ int brev5(int lane) { return (int)(__brev((unsigned)lane) >> 27); }
+
+// In-place transforms of `nlines` contiguous lines of P = 32 RAD points in shared
+// memory, natural order in and out, one line per warp at a time (the block-wide
+// Stockham stages replaced by register work).  `tw` is the [P] table W_P^(-m).
+// The caller synchronises the block before and after.
+template <typename R, int RAD, int DIR>
+__device__ __forceinline__ void warp_lines_inplace(cplx<R>* lines, int nlines, int P, const cplx<R>* __restrict__ tw) {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int brl = brev5(lane);
+    LaneTw<R> lt;
+    lane_twiddles_tab<R>(lt, lane, tw, P);
+    for (int l = threadIdx.x >> 5; l < nlines; l += nw) {
+        cplx<R>* L = lines + (size_t)l * P;
+        cplx<R> z[RAD];
+        if constexpr (DIR > 0) {
+#pragma unroll
+            for (int m = 0; m < RAD; ++m) z[m] = L[lane + 32 * m];
+            inverse_line<R, RAD>(z, lane, tw, lane, lt);
+#pragma unroll
+            for (int k = 0; k < RAD; ++k) L[k + RAD * brl] = z[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < RAD; ++k) z[k] = L[k + RAD * brl];
+            forward_line<R, RAD>(z, lane, tw, lane, lt);
+#pragma unroll
+            for (int b = 0; b < RAD; ++b) L[lane + 32 * b] = z[b];
+        }
+    }
+}

@@ -79,7 +79,7 @@ CASES = [
 
 
 @pytest.mark.parametrize("res,precision,tol", CASES)
-@pytest.mark.parametrize("family", ["warp", "block", "blockwarp"])
+@pytest.mark.parametrize("family", ["warp", "block", "blockwarp", "lines"])
 def test_advection_x_kernel_family(oracle, BLD, res, precision, tol, family):
     if family == "warp" and precision == "fp64" and res[0] == 192:
         pytest.skip("the warp-per-row kernel is compiled for radix <= 6 in FP64 (P1 = 288 is radix 9)")
@@ -146,6 +146,29 @@ def test_y_kernel_family(oracle, BLD, res, precision, les, tol, family):
     om = _build(oracle, res, les=les)
     gm = _forced_y(BLD, family, res, precision, les)
     st = _state(om, seed=sum(res) + 1)
+    ref = om.compute_rates(st)
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < tol, (res, precision, family, f, e)
+
+
+# LES: the SGS x kernel (block Stockham or warp line transforms) with the advection
+# kernel of the same family; P1 (SGS, advection) = (64, 96), (128, 192), (256, 384), (512, 768)
+SGS_CASES = [
+    ((64, 12, 6), "fp64", 1e-12),
+    ((128, 8, 5), "mixed", 1e-5),
+    ((256, 6, 4), "fp64", 1e-12),
+    ((512, 4, 4), "mixed", 1e-5),
+]
+
+
+@pytest.mark.parametrize("res,precision,tol", SGS_CASES)
+@pytest.mark.parametrize("family", ["block", "lines"])
+def test_sgs_x_kernel_family(oracle, BLD, res, precision, tol, family):
+    om = _build(oracle, res, les=True)
+    gm = _forced(BLD, family, res, precision, les=True)
+    st = _state(om, seed=sum(res) + 2)
     ref = om.compute_rates(st)
     got = gm.compute_rates(st)
     for f in om.fields:
