@@ -29,6 +29,12 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "boundarylayerdynamics.jl_b200"))
 
 METRIC = "grid-pt updates/s (plain FP64 vs mixed) @192^2x96"
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the x-pass
+# kernel the autotuner picks at 192^2x96, from one ncu capture of a step
+# (profiles/step_kernels_dns192_fp64.md, profiles/step_kernels_dns192_mixed.md)
+TRAFFIC = {("dns192", "k_adv_xb<double, 9>"): (259.0 + 99.02) * 1e6,
+           ("dns192", "k_adv_xw<float, 9>"): (130.8 + 35.33) * 1e6}
 UNIT = "grid-pt updates/s"
 
 
@@ -195,7 +201,7 @@ def run_b200(args):
         ms = max_over_ranks(e0.elapsed_time(e1))
         barrier()
         _capi.check(lib.bld_time_phases(m._h, 20, _capi.SSPRK33, ctypes.byref(pt)))
-        res[prec] = dict(ms_total=ms, ms_per_step=ms / K, clocks=clk.summary(),
+        res[prec] = dict(ms_total=ms, ms_per_step=ms / K, clocks=clk.summary(), kernels=m.kernels(),
                          phases=dict(inv_y=pt.inv_y_ms[0], adv_x=pt.x_ms[0], fwd_y=pt.fwd_y_ms[0],
                                      project=pt.project_ms),
                          launches_per_step=pt.launches_per_step)
@@ -261,6 +267,21 @@ def run_b200(args):
     dom = max(share, key=share.get)
     pb = phase_bytes(m, "fp64")
     ach = pb[dom] / (ph[dom] * 1e-3) / 1e9
+    names = {"inv_y": "inv_y", "adv_x": "x", "fwd_y": "fwd_y"}
+
+    def kname(kern, phase):
+        return kern["projection"] if phase == "project" else kern["advection"][names[phase]]
+
+    def roofline(prec, phases):
+        share = {k: phases[k] for k in phases}
+        d = max(share, key=share.get)
+        b = phase_bytes(models[prec][0], prec)[d]
+        a = b / (phases[d] * 1e-3) / 1e9
+        kn = kname(res[prec]["kernels"], d)
+        tr = TRAFFIC.get((args.config, kn))
+        return {"bound": "hbm", "kernel": kn, "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b, "avg_launch_ms": phases[d],
+                "traffic": tr}
     step_ach = 8 * sbytes / (fp["ms_per_step"] * 1e-3) / 1e9
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
@@ -273,9 +294,9 @@ def run_b200(args):
         "mixed": {"value": ws * npts / (mx["ms_per_step"] / 1e3), "ms_per_step": mx["ms_per_step"],
                   "speedup_vs_fp64": fp["ms_per_step"] / mx["ms_per_step"], "dtype": "f32 transforms/products, f64 state+pressure",
                   "error_vs_fp64": err, "clocks": mx["clocks"]},
-        "roofline": {"bound": "hbm", "kernel": f"k_{dom}" if dom != "project" else "k_project",
-                     "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": pb[dom], "avg_launch_ms": ph[dom], "traffic": None},
+        "roofline": roofline("fp64", ph),
+        "roofline_mixed": roofline("mixed", mx["phases"]),
+        "kernels": {"fp64": fp["kernels"], "mixed": mx["kernels"]},
         "roofline_step": {"bound": "hbm", "algorithmic_bytes_per_step": 8 * sbytes, "achieved": step_ach,
                           "peak": peak, "unit": "GB/s", "frac": step_ach / peak},
         "phases_ms_fp64": ph, "phases_ms_mixed": mx["phases"],

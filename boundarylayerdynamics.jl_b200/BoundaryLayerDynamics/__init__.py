@@ -450,6 +450,13 @@ class Model:
         """Initial projection and right-hand side of one member (the start of ``evolve!``)."""
         _capi.check(self._lib.bld_prepare_member(self._h, int(member)))
 
+    def kernels(self):
+        """The kernel variants the autotuner chose (dict)."""
+        import json
+        buf = C.create_string_buffer(4096)
+        _capi.check(self._lib.bld_describe(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
     def diverged_members(self):
         """Members whose rates turned non-finite since the last query (clears the record)."""
         out = np.zeros(self.members, dtype=np.int32)

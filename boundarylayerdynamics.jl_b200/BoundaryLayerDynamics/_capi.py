@@ -95,6 +95,7 @@ SIGNATURES = {
     "bld_set_member_params": (C.c_int32, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "bld_prepare_member": (C.c_int32, [C.c_void_p, C.c_int32]),
     "bld_get_diverged": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "bld_describe": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "bld_project_noalloc": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32] + [C.c_void_p] * 5
                             + [C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
     "bld_ldlt_solve_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),

@@ -1837,6 +1837,47 @@ int32_t bld_set_member_params(bld_handle* h, int32_t m, double cs, double z0_low
     return BLD_OK;
 }
 
+int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
+    if (!h || !buf || len == 0) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    const char* R = h->fp32 ? "float" : "double";
+    std::string out = "{";
+    for (int sp = 0; sp < 2; ++sp) {
+        const Space& s = sp == 0 ? h->adv : h->sgs;
+        if (!s.on) continue;
+        char tmp[768];
+        const char* xk = sp == 0 ? "k_adv_x" : "k_sgs_x";
+        char xname[96];
+        if (sp == 0 && s.xb)
+            snprintf(xname, sizeof xname, "k_adv_xb<%s, %d>", R, s.P1 / 32);
+        else if (sp == 0 && s.xw)
+            snprintf(xname, sizeof xname, "k_adv_xw<%s, %d>", R, s.P1 / 32);
+        else
+            snprintf(xname, sizeof xname, "%s<%s, %d, %d>", xk, R, s.PPT, s.xr);
+        char iname[64], fname[64];
+        if (s.inv.all) snprintf(iname, sizeof iname, "k_inv_y_all<%s>", R);
+        else snprintf(iname, sizeof iname, "k_inv_y<%s, %d>", R, s.inv.wfft);
+        if (s.fwd.all) snprintf(fname, sizeof fname, "k_fwd_y_all<%s>", R);
+        else snprintf(fname, sizeof fname, "k_fwd_y<%s, %d>", R, s.fwd.wfft);
+        snprintf(tmp, sizeof tmp,
+                 "%s\"%s\": {\"P\": [%d, %d], \"inv_y\": \"%s\", \"x\": \"%s\", \"fwd_y\": \"%s\", "
+                 "\"inv_NL\": %d, \"fwd_NL\": %d, \"x_rows\": %d, \"x_chunks\": %d}",
+                 out.size() > 1 ? ", " : "", sp == 0 ? "advection" : "sgs", s.P1, s.P2, iname, xname, fname, s.inv.NL,
+                 s.fwd.NL, s.xb ? 1 : (s.xw ? s.xw : s.YT), s.nchunks);
+        out += tmp;
+    }
+    char tmp[160];
+    const bool seg = h->cfg.pressure && h->g.n3 <= 256 && h->proj_variant > 0;
+    if (seg)
+        snprintf(tmp, sizeof tmp, "%s\"projection\": \"k_project_seg<%d, %d>\"}", out.size() > 1 ? ", " : "",
+                 h->g.n3 <= 128 ? 8 : 16, h->proj_variant);
+    else
+        snprintf(tmp, sizeof tmp, "%s\"projection\": \"k_project\"}", out.size() > 1 ? ", " : "");
+    out += tmp;
+    if (out.size() + 1 > len) return fail(BLD_ERR_ARGUMENT, "buffer too small (%zu bytes needed)", out.size() + 1);
+    memcpy(buf, out.c_str(), out.size() + 1);
+    return BLD_OK;
+}
+
 int32_t bld_get_diverged(bld_handle* h, int32_t* out) {
     if (!h || !out) return fail(BLD_ERR_ARGUMENT, "invalid argument");
     for (int m = 0; m < h->B; ++m) {

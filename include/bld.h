@@ -207,6 +207,11 @@ int32_t bld_set_member_params(bld_handle* h, int32_t member, double cs, double z
 int32_t bld_prepare_member(bld_handle* h, int32_t member);
 int32_t bld_get_diverged(bld_handle* h, int32_t* out);
 
+/* The kernel variants the autotuner chose for this handle, as a JSON object
+   (per physical-domain space: sizes, y-pass and x-pass kernels; the projection
+   kernel), NUL-terminated in `buf`.  Diagnostics; no reference counterpart. */
+int32_t bld_describe(bld_handle* h, char* buf, size_t len);
+
 /* Advances several handles on one device (e.g. the size classes of an uneven
    ensemble) by `nsteps` steps of `method`: each step is ONE launch of a CUDA
    graph whose child graphs are the handles' step graphs, run as independent
