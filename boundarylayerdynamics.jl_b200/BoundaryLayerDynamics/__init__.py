@@ -396,25 +396,69 @@ class Model:
               else [Fraction(i, n) for i in range(1, n)])
         return x1, x2, np.array([self.domain.vmap(z) for z in zs])
 
-    def set_field(self, field, values, member=0):
-        """Forward-transform physical values (n3, P2, P1) at the default size into the state."""
+    def set_field(self, field, values, member=0, centered=False):
+        """Forward-transform physical values (n3, P2, P1) at the default size into the state
+        (``centered``: values at the centres of the grid intervals)."""
         P1, P2 = self.default_size
         v = np.ascontiguousarray(np.broadcast_to(np.asarray(values, dtype=np.float64), (self.nz(field), P2, P1)))
-        _capi.check(self._lib.bld_set_field_physical(self._h, member, FIELDS.index(field), v.ctypes.data))
+        fn = self._lib.bld_set_field_centered if centered else self._lib.bld_set_field_physical
+        _capi.check(fn(self._h, member, FIELDS.index(field), v.ctypes.data))
 
     def __getitem__(self, field):
         return self.get_field(field)
 
-    def get_field(self, field, member=0):
+    def get_field(self, field, member=0, centered=False):
         P1, P2 = self.default_size
         out = np.empty((self.nz(field), P2, P1))
-        _capi.check(self._lib.bld_get_field_physical(self._h, member, FIELDS.index(field), out.ctypes.data))
+        fn = self._lib.bld_get_field_centered if centered else self._lib.bld_get_field_physical
+        _capi.check(fn(self._h, member, FIELDS.index(field), out.ctypes.data))
+        return out
+
+    # -- mean profiles on the device --------------------------------------------------------
+    def profiles_start(self, on=True):
+        _capi.check(self._lib.bld_profiles_start(self._h, 1 if on else 0))
+
+    def profiles_read(self, member=0):
+        out = np.zeros(3 * (self.n3 + 1))
+        _capi.check(self._lib.bld_profiles_read(self._h, int(member), out.ctypes.data))
+        return out
+
+    def profiles_sample(self, member=0):
+        out = np.zeros(3 * (self.n3 + 1))
+        _capi.check(self._lib.bld_profiles_sample(self._h, int(member), out.ctypes.data))
         return out
 
     # -- time integration ---------------------------------------------------------------
-    def evolve(self, tspan, dt, method=SSPRK33):
+    def evolve(self, tspan, dt, method=SSPRK33, output=()):
+        """``evolve!`` (src/BoundaryLayerDynamics.jl:190-219).  Without output modules
+        the whole integration is one call; with them, the steps between output times
+        run as graph launches on the device and the modules act at their times."""
         t1, t2 = (0.0, float(tspan)) if np.isscalar(tspan) else (float(tspan[0]), float(tspan[1]))
-        _capi.check(self._lib.bld_evolve(self._h, t1, t2, float(dt), _METHODS[method]))
+        if not output:
+            _capi.check(self._lib.bld_evolve(self._h, t1, t2, float(dt), _METHODS[method]))
+            return self
+        if t1 > t2:
+            raise ValueError("Integration start time is larger than end time")
+        nt = _approxdiv(t2 - t1, dt) if t2 > t1 else 0
+        self.prepare()
+        for o in output:
+            o.start(self, t1)
+        events = set()
+        for o in output:
+            for t in o.output_times(t1, t2):
+                k = _approxdiv(t - t1, dt)
+                if 0 < k <= nt:
+                    events.add(k)
+        done = 0
+        for k in sorted(events | {nt}):
+            if k > done:
+                self.step(k - done, dt, method)
+            t = t2 if k == nt else t1 + k * dt
+            for o in output:
+                o.at(self, t, k - done)
+            done = k
+        for o in output:
+            o.finish(self, t2)
         return self
 
     def prepare(self):
@@ -475,8 +519,24 @@ class Model:
 
 
 # --------------------------------------------------------------- API functions (the `!` forms)
-def initialize(model, member=0, **initial_conditions):
-    """``initialize!(model; vel1=f, ...)`` (src/State.jl:11-31): unspecified fields are zeroed."""
+def _approxdiv(a, b):
+    """approxdiv (src/util.jl): a / b when it is an integer up to rounding, else an error."""
+    r = a / b
+    ri = round(r)
+    if abs(r - ri) > math.sqrt(np.finfo(float).eps) * max(abs(r), abs(ri)):
+        raise ValueError("Division has a non-integer result")
+    return int(ri)
+
+
+def initialize(model, path=None, member=0, **initial_conditions):
+    """``initialize!(model; vel1=f, ...)`` (src/State.jl:11-31): unspecified fields are zeroed.
+    ``initialize(model, path)`` reads a snapshot folder (src/State.jl:33-66)."""
+    if path is not None:
+        if initial_conditions:
+            raise ValueError("initialize from a snapshot path or from initial conditions, not both")
+        from .output import initialize_from_snapshot
+        initialize_from_snapshot(model, path, member=member)
+        return model
     for f in initial_conditions:
         if f not in FIELDS:
             raise KeyError(f"Cannot initialize `{f}`: unknown field")
@@ -521,3 +581,6 @@ def openchannelflow(Re, dims, roughness_length=None, **kw):
     wall = SmoothWall() if roughness_length is None else RoughWall(roughness_length)
     domain = Domain((4 * math.pi, 2 * math.pi, 1), wall, FreeSlipBoundary())
     return Model(dims, domain, incompressible_flow(1 / Re, **kw))
+
+
+from .output import MeanProfiles, Snapshots  # noqa: E402  (output modules for evolve)

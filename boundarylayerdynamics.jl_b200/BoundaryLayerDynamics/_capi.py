@@ -87,6 +87,11 @@ SIGNATURES = {
     "bld_sync": (C.c_int32, [C.c_void_p]),
     "bld_set_field_physical": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
     "bld_get_field_physical": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "bld_set_field_centered": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "bld_get_field_centered": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "bld_profiles_start": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "bld_profiles_read": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "bld_profiles_sample": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p]),
     "bld_get_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bld_step_async": (C.c_int32, [C.c_void_p, C.c_int64, C.c_double, C.c_int32]),
     "bld_time_phases": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(BldPhaseTimes)]),

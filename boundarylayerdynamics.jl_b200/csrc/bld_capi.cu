@@ -170,6 +170,9 @@ struct bld_handle {
     std::vector<int> active_host;
     bool mask_on = false;        // the active mask applies to whole-ensemble steps only
     int proj_variant = 1;        // 0: column kernel, 1/2: z-segmented kernel (autotuned)
+    double* prof_acc = nullptr;  // [members][3][n3+1] time integral of the mean profiles
+    double* prof_prev = nullptr; // [members][3][n3+1] last sample
+    bool prof_on = false;        // step graphs sample the profiles after every step
     std::vector<double> tab_dx3c, tab_dx3i, tab_x3c, tab_x3i;  // copies of the mapping tables
     std::vector<double> member_cs, member_z0;                  // current per-member SGS parameters
     std::map<int, DevTw> tw;
@@ -1260,6 +1263,8 @@ void free_handle(bld_handle* h) {
     if (!h) return;
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
     for (auto& kv : h->graph_src) cudaGraphDestroy(kv.second);
+    if (h->prof_acc) cudaFree(h->prof_acc);
+    if (h->prof_prev) cudaFree(h->prof_prev);
     for (auto& kv : h->ens_graphs) cudaGraphExecDestroy(kv.second);
     void* ptrs[] = {h->u, h->t, h->du, h->dp, h->io, h->io2, h->pscr, h->gamma, h->d1, h->d2, h->DD1, h->DD2,
                     h->alpha_c, h->alpha_i, h->alpha_ext, h->mean_w, h->lc2, h->li2, h->wall, h->src,
@@ -1590,14 +1595,30 @@ int32_t bld_prepare(bld_handle* h) {
 
 static int step_impl(bld_handle* h, int64_t nsteps, double dt, int32_t method);
 
+// step graphs with and without the mean-profile sample are kept apart
+static int gkey(const bld_handle* h, int method) { return method + (h->prof_on ? 16 : 0); }
+
+// one trapezoid of the device mean profiles for every member (w = dt/2), or a bare sample (w = 0)
+static int enqueue_profile_sample(bld_handle* h, double w) {
+    k_profile_sample<<<h->B, 128, 0, h->stream>>>(h->g, h->u, h->prof_acc, h->prof_prev, w, 0,
+                                                  h->mask_on ? h->active : nullptr);
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
 // captures one step of `method` (regular steps; AB2 after its start-up step) into
 // a CUDA graph, kept as source graph and instantiated executable
 static int step_graph(bld_handle* h, int method, double dt) {
-    const auto key = std::make_pair(method, dt);
+    const auto key = std::make_pair(gkey(h, method), dt);
     if (h->graphs.count(key)) return BLD_OK;
     cudaGraph_t graph;
     CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int st = enqueue_step(h, method, dt, false);
+    if (st == BLD_OK && h->prof_on) {
+        h->mask_on = true;
+        st = enqueue_profile_sample(h, 0.5 * dt);
+        h->mask_on = false;
+    }
     cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
     if (st != BLD_OK) {
         if (ce == cudaSuccess) cudaGraphDestroy(graph);
@@ -1635,13 +1656,19 @@ static int step_impl(bld_handle* h, int64_t nsteps, double dt, int32_t method) {
         if (h->ab2_started && h->ab2_dt != dt) return fail(BLD_ERR_ARGUMENT, "Cannot change time step for multi-step methods");
         if (!h->ab2_started) {
             BLD_TRY(enqueue_step(h, method, dt, true));
+            if (h->prof_on) {
+                h->mask_on = true;
+                const int st = enqueue_profile_sample(h, 0.5 * dt);
+                h->mask_on = false;
+                BLD_TRY(st);
+            }
             h->ab2_started = true;
             h->ab2_dt = dt;
             done = 1;
         }
     }
     if (done < nsteps) {
-        const auto key = std::make_pair((int)method, dt);
+        const auto key = std::make_pair(gkey(h, method), dt);
         auto it = h->graphs.find(key);
         if (it == h->graphs.end()) {
             BLD_TRY(step_graph(h, method, dt));
@@ -1664,8 +1691,10 @@ int32_t bld_ensemble_step(bld_handle* const* hs, int32_t n, int64_t nsteps, doub
     if (nsteps <= 0) return BLD_OK;
     CUDA_TRY(cudaSetDevice(lead->device));
     std::vector<const void*> key;
-    for (int i = 0; i < n; ++i) key.push_back(hs[i]);
-    key.push_back((const void*)(intptr_t)method);
+    for (int i = 0; i < n; ++i) {
+        key.push_back(hs[i]);
+        key.push_back((const void*)(intptr_t)gkey(hs[i], method));
+    }
     double dtk = dt;
     const void* dtp;
     memcpy(&dtp, &dtk, sizeof(dtp) < sizeof(dtk) ? sizeof(dtp) : sizeof(dtk));
@@ -1681,7 +1710,8 @@ int32_t bld_ensemble_step(bld_handle* const* hs, int32_t n, int64_t nsteps, doub
                 return st;
             }
             cudaGraphNode_t node;
-            cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, hs[i]->graph_src.at(std::make_pair((int)method, dt)));
+            cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0,
+                                                       hs[i]->graph_src.at(std::make_pair(gkey(hs[i], method), dt)));
             if (e != cudaSuccess) {
                 cudaGraphDestroy(parent);
                 CUDA_TRY(e);
@@ -1761,6 +1791,9 @@ int32_t bld_evolve(bld_handle* h, double t1, double t2, double dt, int32_t metho
     if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
     if (t1 > t2) return fail(BLD_ERR_ARGUMENT, "Integration start time is larger than end time");
     BLD_TRY(bld_prepare(h));
+    if (h->prof_on) {  // the first sample is the projected initial state (src/ODEMethods.jl:179-185)
+        BLD_TRY(enqueue_profile_sample(h, 0.0));
+    }
     if (t2 > t1) {
         const double r = (t2 - t1) / dt;
         const double ri = std::round(r);
@@ -1991,6 +2024,85 @@ int32_t bld_get_field_physical(bld_handle* h, int32_t m, int32_t field, double* 
     CUDA_TRY(cudaMemcpyAsync(values, h->pd_buf, (size_t)nz * P2 * P1 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return BLD_OK;
+}
+
+static int half_shift(bld_handle* h, double2* dst, const double2* src, int field, double sign) {
+    const Geo& g = h->g;
+    const int nz = field == 2 ? g.n3 - 1 : g.n3;
+    dim3 grid((unsigned)((g.F + 255) / 256), nz);
+    k_half_shift<<<grid, 256, 0, h->stream>>>(dst, src, g, h->Pd1, h->Pd2, sign);
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+int32_t bld_get_field_centered(bld_handle* h, int32_t m, int32_t field, double* values) {
+    if (!member_ok(h, m) || field < 0 || field > 2 || !values) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    if (!h->pd_buf) return fail(BLD_ERR_INVALID_CONFIG, "default physical size is not an even 2^a*3^b");
+    CUDA_TRY(cudaSetDevice(h->device));
+    // shift a copy of the member's field (in the staging buffer) and transform it
+    const size_t off = (size_t)m * h->g.mstride + fld_off(h->g, field);
+    BLD_TRY(half_shift(h, h->io + off, h->u + off, field, 1.0));
+    double2* keep = h->u;
+    h->u = h->io;
+    const int st = bld_get_field_physical(h, m, field, values);
+    h->u = keep;
+    return st;
+}
+
+int32_t bld_set_field_centered(bld_handle* h, int32_t m, int32_t field, const double* values) {
+    BLD_TRY(bld_set_field_physical(h, m, field, values));
+    CUDA_TRY(cudaSetDevice(h->device));
+    const size_t off = (size_t)m * h->g.mstride + fld_off(h->g, field);
+    BLD_TRY(half_shift(h, h->u + off, h->u + off, field, -1.0));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
+}
+
+int32_t bld_profiles_start(bld_handle* h, int32_t on) {
+    if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (!on) {
+        h->prof_on = false;
+        return BLD_OK;
+    }
+    const size_t n = (size_t)h->B * 3 * (h->g.n3 + 1);
+    if (!h->prof_acc) {
+        BLD_TRY(dalloc(h, (void**)&h->prof_acc, n * sizeof(double)));
+        BLD_TRY(dalloc(h, (void**)&h->prof_prev, n * sizeof(double)));
+    }
+    CUDA_TRY(cudaMemsetAsync(h->prof_acc, 0, n * sizeof(double), h->stream));
+    BLD_TRY(enqueue_profile_sample(h, 0.0));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->prof_on = true;
+    return BLD_OK;
+}
+
+static int profiles_copy(bld_handle* h, int m, const double* src, double* out) {
+    if (!member_ok(h, m) || !out) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    if (!h->prof_acc) return fail(BLD_ERR_ARGUMENT, "bld_profiles_start was not called");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const size_t n = 3 * (size_t)(h->g.n3 + 1);
+    CUDA_TRY(cudaMemcpyAsync(out, src + (size_t)m * n, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
+}
+
+int32_t bld_profiles_read(bld_handle* h, int32_t m, double* out) {
+    return h ? profiles_copy(h, m, h->prof_acc, out) : fail(BLD_ERR_ARGUMENT, "null handle");
+}
+
+int32_t bld_profiles_sample(bld_handle* h, int32_t m, double* out) {
+    if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (!h->prof_acc) {
+        const size_t n = (size_t)h->B * 3 * (h->g.n3 + 1);
+        BLD_TRY(dalloc(h, (void**)&h->prof_acc, n * sizeof(double)));
+        BLD_TRY(dalloc(h, (void**)&h->prof_prev, n * sizeof(double)));
+        CUDA_TRY(cudaMemsetAsync(h->prof_acc, 0, n * sizeof(double), h->stream));
+    }
+    // a bare sample only replaces the last sample, which is the current state's anyway
+    BLD_TRY(enqueue_profile_sample(h, 0.0));
+    return profiles_copy(h, m, h->prof_prev, out);
 }
 
 int32_t bld_ldlt_solve_device(const double* gamma, const double* beta, void* rhs, int64_t nsys, int32_t n, void* stream) {

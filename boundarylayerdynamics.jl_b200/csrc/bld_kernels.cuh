@@ -27,7 +27,7 @@ struct Geo {
     long long mstride;                // complex values per member state (3*n3-1)*F
 };
 
-__device__ __forceinline__ long long fld_off(const Geo& g, int f) { return (long long)f * g.n3 * g.F; }
+__host__ __device__ __forceinline__ long long fld_off(const Geo& g, int f) { return (long long)f * g.n3 * g.F; }
 
 // inactive ensemble slots (serving) skip their blocks; uniform per block
 #define BLD_SKIP_INACTIVE(a, m) \
@@ -1844,5 +1844,50 @@ __global__ void __launch_bounds__(256) k_x_c2r(XPlainArgs a) {
     for (int x = threadIdx.x; x < a.P1; x += blockDim.x) {
         a.pd_out[r0 * a.P1 + x] = res[x].x;
         if (r1 < rows) a.pd_out[r1 * a.P1 + x] = res[x].y;
+    }
+}
+
+// ------------------------------------------- output helpers (snapshots, profiles)
+// Half-grid-point shift of one field in the frequency domain (shift!/unshift!,
+// src/physical_space.jl:321-336): q(k1, k2) *= exp(sign i pi (k1/P1 + k2/P2)) for
+// the default physical size (P1, P2).  grid (ceil(F/256), nz), dst may equal src.
+__global__ void __launch_bounds__(256) k_half_shift(double2* dst, const double2* __restrict__ src, Geo g, int P1, int P2,
+                                                     double sign) {
+    const int mo = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mo >= g.F) return;
+    const int z = blockIdx.y;
+    const int j = mo / g.K1, k1 = mo - j * g.K1;
+    const int k2 = j <= g.k2max ? j : j - g.K2;
+    double s, c;
+    sincospi(sign * ((double)k1 / (double)P1 + (double)k2 / (double)P2), &s, &c);
+    const long long idx = (long long)z * g.F + mo;
+    const double2 q = src[idx];
+    dst[idx] = make_double2(q.x * c - q.y * s, q.x * s + q.y * c);
+}
+
+// Mean profiles on the device (MeanProfiles, src/logging.jl:333-491): the
+// horizontal mean of a frequency-space field is the real part of its (0,0) mode.
+// prof[m][f][0..n3] holds one sample per field (vel3 with its two boundary entries,
+// which stay zero as in log_state!); acc += w (prev + sample) adds one trapezoid,
+// and prev takes the new sample.  w = 0 only records the sample.
+// grid (members), block 128.
+__global__ void __launch_bounds__(128) k_profile_sample(Geo g, const double2* __restrict__ u, double* acc, double* prev,
+                                                         double w, int m0, const int* active) {
+    const int m = m0 + blockIdx.x;
+    if (active && !active[m]) return;
+    const int n = g.n3 + 1;
+    const double2* S = u + (long long)m * g.mstride;
+    double* A = acc + (long long)m * 3 * n;
+    double* Pv = prev + (long long)m * 3 * n;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+        const int f = i / n, z = i - f * n;
+        double v = 0.0;
+        if (f < 2) {
+            if (z < g.n3) v = S[fld_off(g, f) + (long long)z * g.F].x;
+        } else if (z >= 1 && z <= g.n3 - 1) {
+            v = S[fld_off(g, 2) + (long long)(z - 1) * g.F].x;
+        }
+        A[i] += w * (Pv[i] + v);
+        Pv[i] = v;
     }
 }

@@ -226,6 +226,29 @@ int32_t bld_ensemble_step(bld_handle* const* handles, int32_t n, int64_t nsteps,
 int32_t bld_set_field_physical(bld_handle* h, int32_t member, int32_t field, const double* values);
 int32_t bld_get_field_physical(bld_handle* h, int32_t member, int32_t field, double* values);
 
+/* The same at the centres of the grid intervals (x1, x2 shifted by half a grid
+   spacing): get_field(...; centered = true) / set_field!(...; centered = true)
+   with shift!/unshift! (src/physical_space.jl:277-336), as Snapshots writes and
+   initialize!(model, path) reads them (src/logging.jl:582-601, src/State.jl:33-66). */
+int32_t bld_get_field_centered(bld_handle* h, int32_t member, int32_t field, double* values);
+int32_t bld_set_field_centered(bld_handle* h, int32_t member, int32_t field, const double* values);
+
+/* Mean profiles accumulated on the device (MeanProfiles, src/logging.jl:333-491).
+   The horizontal mean of a frequency-space field is the real part of its (0,0)
+   mode.  bld_profiles_start(h, 1) zeroes the time integrals and records the
+   current state as the first sample; from then on every step (bld_step,
+   bld_step_async, bld_evolve, bld_ensemble_step) adds the trapezoid
+   (dt/2)(previous sample + new sample) for every member inside the step graph,
+   so nothing leaves the device between outputs; bld_evolve records the projected
+   initial state as the first sample.  bld_profiles_start(h, 0) stops sampling.
+   bld_profiles_read copies member m's integrals and bld_profiles_sample its
+   current sample, each 3*(n3+1) doubles: vel1 at the n3 C nodes (one unused
+   zero), vel2 likewise, vel3 as lower boundary, the n3-1 I nodes, upper boundary
+   (the boundary entries stay zero, as for log_state! of the state). */
+int32_t bld_profiles_start(bld_handle* h, int32_t on);
+int32_t bld_profiles_read(bld_handle* h, int32_t member, double* out);
+int32_t bld_profiles_sample(bld_handle* h, int32_t member, double* out);
+
 /* Standalone batched symmetric tridiagonal solve (the kernel of
    ldiv!(::DistributedBatchLDLt, b), src/processes/pressure.jl:106-201):
    `nsys` systems of size `n` (1 <= n <= 1024), factor `gamma` [n][nsys] (the

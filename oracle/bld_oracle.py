@@ -301,7 +301,7 @@ class Transform2D:
         self.k1m = min(self.P1 // 2 + 1, self.K1) - 1                   # :280
         self.k2m = (min(self.P2, self.K2) - 1) // 2                     # :281
 
-    def get_field(self, fd, prefactors=None):
+    def get_field(self, fd, prefactors=None, centered=False):
         nz = fd.shape[0]
         k1m, k2m, P1, P2 = self.k1m, self.k2m, self.P1, self.P2
         src = fd if prefactors is None else fd * prefactors
@@ -309,11 +309,15 @@ class Transform2D:
         h[:, :k2m + 1, :k1m + 1] = src[:, :k2m + 1, :k1m + 1]           # :283-285
         if k2m > 0:
             h[:, P2 - k2m:, :k1m + 1] = src[:, self.K2 - k2m:, :k1m + 1]  # :286-288
+        if centered:
+            h = h * half_shift_factors(P1, P2, +1)                      # :291
         return _irfft2_unnormalised(h, (P2, P1))                        # :293
 
-    def add_field(self, fd, pd, prefactors=None):
+    def add_field(self, fd, pd, prefactors=None, centered=False):
         k1m, k2m, P1, P2 = self.k1m, self.k2m, self.P1, self.P2
         x = _rfft2_unnormalised(pd)                                     # :222
+        if centered:
+            x = x * half_shift_factors(P1, P2, -1)                      # :223
         f = 1 / (P1 * P2)                                               # :219
         if prefactors is not None:                                      # (1,K1) or (K2,1) broadcast
             pr = np.asarray(prefactors)
@@ -331,9 +335,96 @@ class Transform2D:
             fd[:, self.K2 - k2m:, :k1m + 1] += b                        # :228-230
         return fd
 
-    def set_field(self, fd, pd):                                        # :253-256
+    def set_field(self, fd, pd, centered=False):                        # :253-256
         fd[...] = 0
-        return self.add_field(fd, pd)
+        return self.add_field(fd, pd, centered=centered)
+
+
+def half_shift_factors(P1, P2, sign):
+    """shift!/unshift! (src/physical_space.jl:321-336): exp(sign i pi (k1/P1 + k2/P2))
+    on the (P2, P1/2+1) half spectrum, the Nyquist row counted as negative."""
+    k1 = np.arange(P1 // 2 + 1)
+    i2 = np.arange(1, P2 + 1)
+    k2 = np.where(2 * i2 > P2, i2 - P2 - 1, i2 - 1)
+    return np.exp(sign * 1j * np.pi * (k1[None, :] / P1 + k2[:, None] / P2))[None, :, :]
+
+
+# --------------------------------------------------------------------------------------
+# Output: CBD files (src/fileio.jl) and mean profiles (src/logging.jl:333-491)
+# --------------------------------------------------------------------------------------
+
+CBD_MAGIC = bytes.fromhex("CBDF")
+
+
+def writecbd(dtype, filename, field, x1, x2, x3, xmin, xmax):
+    """writecbd (src/fileio.jl:26-62): identifier, sizes, limits, coordinates, data
+    (x1 fastest).  ``field`` is indexed [x3][x2][x1]."""
+    import struct
+    dtype = np.dtype(dtype)
+    n3, n2, n1 = np.shape(field)
+    ident = bytes([0xCB, 0xDF, 1, 0, 0, 0, 0, dtype.itemsize])        # :29-32
+    with open(filename, "wb") as f:
+        f.write(ident)
+        f.write(struct.pack("<3Q", n1, n2, n3))                          # :44
+        f.write(struct.pack("<3d", *xmin))                               # :45
+        f.write(struct.pack("<3d", *xmax))                               # :46
+        f.write(struct.pack(f"<{n1}d", *x1))                             # :47
+        f.write(struct.pack(f"<{n2}d", *x2))                             # :48
+        f.write(struct.pack(f"<{n3}d", *x3))                             # :54
+        f.write(np.asarray(field, dtype=dtype.newbyteorder("<")).tobytes())  # :59
+
+
+def readcbd(filename):
+    """readcbd (src/fileio.jl:64-108) for the whole x3 range."""
+    import struct
+    with open(filename, "rb") as f:
+        ident = f.read(8)
+        assert ident[:2] == CBD_MAGIC and ident[2] == 1
+        dtype = {4: np.dtype("<f4"), 8: np.dtype("<f8")}[ident[7]]
+        n1, n2, n3 = struct.unpack("<3Q", f.read(24))
+        xmin = struct.unpack("<3d", f.read(24))
+        xmax = struct.unpack("<3d", f.read(24))
+        x1 = np.array(struct.unpack(f"<{n1}d", f.read(8 * n1)))
+        x2 = np.array(struct.unpack(f"<{n2}d", f.read(8 * n2)))
+        x3 = np.array(struct.unpack(f"<{n3}d", f.read(8 * n3)))
+        data = np.frombuffer(f.read(), dtype=dtype).reshape(n3, n2, n1)
+    return xmin, xmax, x1, x2, x3, data
+
+
+class MeanProfiles:
+    """Time-averaged horizontal means (MeanProfiles, src/logging.jl:333-491): one
+    sample per checkpoint (every step), trapezoidal rule in time, vel3 profiles
+    with their two boundary entries (zero for state samples)."""
+
+    def __init__(self, n3, t1, profiles=("vel1", "vel2", "vel3")):
+        size = lambda f: n3 + 1 if f == "vel3" else n3                  # :351-353
+        self.means = {f: np.zeros(size(f)) for f in profiles}
+        self.samples = {f: np.zeros(size(f)) for f in profiles}
+        self.timespan = [t1, t1]
+        self.intervals = 0
+
+    def sample_state(self, state):                                      # :380-413
+        for f in self.samples:
+            col = state[f][:, 0, 0].real                                # hmean, :411
+            if f == "vel3":
+                self.samples[f][1:-1] = col
+            else:
+                self.samples[f][:] = col
+
+    def step(self, state, t):
+        """prepare_samples! + log_state! + process_log! for a checkpoint at t."""
+        w = (t - self.timespan[1]) / 2                                  # :372
+        for f in self.means:
+            self.means[f] += w * self.samples[f]
+        self.sample_state(state)
+        for f in self.means:                                            # :434-437
+            self.means[f] += w * self.samples[f]
+        self.timespan[1] = t
+        self.intervals += 1
+
+    def averages(self):                                                 # :461-467
+        dt = self.timespan[1] - self.timespan[0]
+        return {f: v / dt for f, v in self.means.items()}
 
 
 def h1range(P, centered=False):                                         # :64-65
@@ -920,8 +1011,13 @@ class Model:
         """getterm at the default physical size (src/State.jl:81-85)."""
         return self._t.get_field(self.state[field])
 
-    def get_field(self, field, dims=None):
-        return self.transform(pdsize(self.grid) if dims is None else dims).get_field(self.state[field])
+    def get_field(self, field, dims=None, centered=False):
+        t = self._t if dims is None else self.transform(dims)
+        return t.get_field(self.state[field], centered=centered)
+
+    def set_field(self, field, values, centered=False):
+        """set_field! at the default size (src/physical_space.jl:253-256), e.g. from a snapshot."""
+        self._t.set_field(self.state[field], np.ascontiguousarray(values, dtype=np.float64), centered=centered)
 
     # -- time integration -----------------------------------------------------------
     def rate(self):
