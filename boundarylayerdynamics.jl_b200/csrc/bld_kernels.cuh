@@ -1466,8 +1466,11 @@ __global__ void __launch_bounds__(128) k_project(ProjArgs a) {
 // value entering from below (forward: b_z = P_z + Q_z b_in) or from above
 // (backward: p_z = G_z + H_z p_out) and the segments are chained through shared
 // memory.  Same arithmetic as k_project up to the order of operations.
-template <int LMAX, int MINB>
+// TILE: the stage values of the block's columns stay in shared memory between
+// the phases ([3][n3][lanes], dynamic) instead of a round trip through `out`.
+template <int LMAX, int MINB, bool TILE>
 __global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
+    extern __shared__ __align__(16) double2 tile[];
     const Geo& g = a.g;
     const int n = g.n3;
     const long long F = g.F;
@@ -1515,9 +1518,16 @@ __global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
             const int q = qb + r, z = z0 + q;
             if (q < len && valid) {
                 const double2 uz = Ub[r], vz = Vb[r], wz = Wb[r];
-                a.out[o1 + z * F + c] = uz;
-                a.out[o2 + z * F + c] = vz;
-                if (z < n - 1) a.out[o3 + z * F + c] = wz;
+                if constexpr (TILE) {
+                    const int LN = blockDim.x;
+                    tile[(0 * n + z) * LN + lane] = uz;
+                    tile[(1 * n + z) * LN + lane] = vz;
+                    if (z < n - 1) tile[(2 * n + z) * LN + lane] = wz;
+                } else {
+                    a.out[o1 + z * F + c] = uz;
+                    a.out[o2 + z * F + c] = vz;
+                    if (z < n - 1) a.out[o3 + z * F + c] = wz;
+                }
                 const double h = 1.0 / a.alpha_c[z];
                 double2 val;
                 val.x = (-e1 * uz.y) * h + (-e2 * vz.y) * h;
@@ -1625,9 +1635,16 @@ __global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
         for (int r = 0; r < NBL; ++r) {
             const int q = qb + r, z = z0 + q;
             if (q < len && valid) {
-                Ub[r] = a.out[o1 + z * F + c];
-                Vb[r] = a.out[o2 + z * F + c];
-                if (z < n - 1) Wb[r] = a.out[o3 + z * F + c];
+                if constexpr (TILE) {
+                    const int LN = blockDim.x;
+                    Ub[r] = tile[(0 * n + z) * LN + lane];
+                    Vb[r] = tile[(1 * n + z) * LN + lane];
+                    if (z < n - 1) Wb[r] = tile[(2 * n + z) * LN + lane];
+                } else {
+                    Ub[r] = a.out[o1 + z * F + c];
+                    Vb[r] = a.out[o2 + z * F + c];
+                    if (z < n - 1) Wb[r] = a.out[o3 + z * F + c];
+                }
             }
         }
 #pragma unroll

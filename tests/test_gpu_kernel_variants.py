@@ -174,3 +174,36 @@ def test_sgs_x_kernel_family(oracle, BLD, res, precision, tol, family):
     for f in om.fields:
         e = rel_l2(got[f], ref[f])
         assert e < tol, (res, precision, family, f, e)
+
+
+@pytest.mark.parametrize("variant", ["0", "1", "2", "3"])
+@pytest.mark.parametrize("res", [(16, 12, 7), (24, 20, 40), (16, 16, 200)])
+def test_projection_variants(oracle, BLD, variant, res):
+    """Column kernel (0), z-segmented kernels (1, 2) and the shared-tile one (3, n3 <= 128),
+    each forced, against the oracle's projection (1e-12)."""
+    if variant == "3" and res[2] > 128:
+        pytest.skip("the tile variant is for n3 <= 128")
+    old = os.environ.get("BLD_PROJ_VARIANT")
+    os.environ["BLD_PROJ_VARIANT"] = variant
+    try:
+        gm = _build(BLD, res, "fp64")
+    finally:
+        if old is None:
+            del os.environ["BLD_PROJ_VARIANT"]
+        else:
+            os.environ["BLD_PROJ_VARIANT"] = old
+    om = _build(oracle, res)
+    rng = np.random.default_rng(int(variant) + sum(res))
+    st = {f: rng.standard_normal(om.state[f].shape) + 1j * rng.standard_normal(om.state[f].shape)
+          for f in om.fields}
+    ref = om.apply_projections({f: v.copy() for f, v in st.items()})
+    got = gm.apply_projections({f: v.copy() for f, v in st.items()})
+    for f in om.fields:
+        assert rel_l2(got[f], ref[f]) < 1e-12, (variant, res, f)
+    # and inside time steps (stage updates of SSPRK33)
+    gm.set_state(st)
+    om.state.update({f: v.copy() for f, v in st.items()})
+    gm.evolve(3 * 1e-3, 1e-3)
+    om.evolve(3 * 1e-3, 1e-3)
+    for f in om.fields:
+        assert rel_l2(gm.state[f], om.state[f]) < 1e-10, (variant, res, f)
