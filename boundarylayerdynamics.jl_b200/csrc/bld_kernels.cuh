@@ -1329,6 +1329,37 @@ __device__ __forceinline__ double2 stage_value(const ProjArgs& a, long long idx)
     }
 }
 
+// the same with the stage kind fixed at compile time: the loads of a layer batch
+// are straight-line code that the compiler issues together
+template <int KIND>
+__device__ __forceinline__ double2 stage_value_k(const ProjArgs& a, long long idx) {
+    const double2 u = a.u[idx];
+    const double dt = a.dt;
+    if constexpr (KIND == S_NONE) {
+        return u;
+    } else if constexpr (KIND == S_EULER) {
+        const double2 d = a.du[idx];
+        return make_double2(u.x + dt * d.x, u.y + dt * d.y);
+    } else if constexpr (KIND == S_RK22_2) {
+        const double2 t = a.t[idx], d = a.du[idx];
+        return make_double2((u.x + t.x + dt * d.x) / 2.0, (u.y + t.y + dt * d.y) / 2.0);
+    } else if constexpr (KIND == S_RK33_2) {
+        const double2 t = a.t[idx], d = a.du[idx];
+        return make_double2((3.0 * u.x + t.x + dt * d.x) / 4.0, (3.0 * u.y + t.y + dt * d.y) / 4.0);
+    } else if constexpr (KIND == S_RK33_3) {
+        const double2 t = a.t[idx], d = a.du[idx];
+        const double dt2 = 2.0 * dt;
+        return make_double2((u.x + 2.0 * t.x + dt2 * d.x) / 3.0, (u.y + 2.0 * t.y + dt2 * d.y) / 3.0);
+    } else if constexpr (KIND == S_AB2_1) {
+        const double2 d = a.du[idx], p = a.dp[idx];
+        return make_double2(u.x + dt * (d.x - p.x) / 2.0, u.y + dt * (d.y - p.y) / 2.0);
+    } else {  // S_AB2
+        const double2 d = a.du[idx], p = a.dp[idx];
+        const double h = dt / 2.0;
+        return make_double2(u.x + h * (3.0 * d.x - p.x), u.y + h * (3.0 * d.y - p.y));
+    }
+}
+
 // One thread per (k1, k2) column: stage update, divergence (div!, src/processes/pressure.jl:368-378),
 // forward/backward Thomas (:106-165), gradient (add_gradient!, :405-426), then ConstantMean
 // (src/processes/sources.jl:69-77) on the (0,0) column.  grid (ceil(F/128), members)
@@ -1466,11 +1497,12 @@ __global__ void __launch_bounds__(128) k_project(ProjArgs a) {
 // value entering from below (forward: b_z = P_z + Q_z b_in) or from above
 // (backward: p_z = G_z + H_z p_out) and the segments are chained through shared
 // memory.  Same arithmetic as k_project up to the order of operations.
-// TILE: the stage values of the block's columns stay in shared memory between
-// the phases ([3][n3][lanes], dynamic) instead of a round trip through `out`.
-template <int LMAX, int MINB, bool TILE>
-__global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
-    extern __shared__ __align__(16) double2 tile[];
+// Body of k_project_seg for one stage kind.  TILE: the stage values of the
+// block's columns stay in shared memory between the phases ([3][n3][lanes],
+// dynamic) instead of a round trip through `out`.
+template <int LMAX, bool TILE, int KIND>
+__device__ __forceinline__ void project_seg_body(const ProjArgs& a, double2* tile, double2 (&sP)[32][32],
+                                                 double (&sQ)[32][32]) {
     const Geo& g = a.g;
     const int n = g.n3;
     const long long F = g.F;
@@ -1482,8 +1514,6 @@ __global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
     const int L = (n + NS - 1) / NS;
     const int z0 = min(n, s * L), z1 = min(n, z0 + L);
     const int len = z1 - z0;
-    __shared__ double2 sP[32][32];
-    __shared__ double sQ[32][32];
     const long long mb = (long long)m * g.mstride;
     const long long o1 = mb, o2 = mb + (long long)n * F, o3 = mb + 2LL * n * F;
     const int cc = valid ? c : 0;
@@ -1492,7 +1522,7 @@ __global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
     const double e1 = a.d1[k1], e2 = a.d2[j];
     // stage value of w just below the segment, read before any thread writes `out`
     double2 wprev = make_double2(0.0, 0.0);
-    if (valid && z0 > 0 && len > 0) wprev = stage_value(a, o3 + (long long)(z0 - 1) * F + c);
+    if (valid && z0 > 0 && len > 0) wprev = stage_value_k<KIND>(a, o3 + (long long)(z0 - 1) * F + c);
     __syncthreads();
     double2 X[LMAX];
     double Y[LMAX];
@@ -1507,9 +1537,9 @@ __global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
         for (int r = 0; r < NBL; ++r) {
             const int q = qb + r, z = z0 + q;
             if (q < len && valid) {
-                Ub[r] = stage_value(a, o1 + z * F + c);
-                Vb[r] = stage_value(a, o2 + z * F + c);
-                Wb[r] = (z < n - 1) ? stage_value(a, o3 + z * F + c) : make_double2(0.0, 0.0);
+                Ub[r] = stage_value_k<KIND>(a, o1 + z * F + c);
+                Vb[r] = stage_value_k<KIND>(a, o2 + z * F + c);
+                Wb[r] = (z < n - 1) ? stage_value_k<KIND>(a, o3 + z * F + c) : make_double2(0.0, 0.0);
                 Gb[r] = a.gamma[z * F + c];
             }
         }
@@ -1684,6 +1714,22 @@ __global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
             const double add = a.mean_val[3 * m + f] - sum;
             for (int z = 0; z < n; ++z) a.out[of + z * F].x += add;
         }
+    }
+}
+
+template <int LMAX, int MINB, bool TILE>
+__global__ void __launch_bounds__(256, MINB) k_project_seg(ProjArgs a) {
+    extern __shared__ __align__(16) double2 tile[];
+    __shared__ double2 sP[32][32];
+    __shared__ double sQ[32][32];
+    switch (a.kind) {
+        case S_NONE: project_seg_body<LMAX, TILE, S_NONE>(a, tile, sP, sQ); break;
+        case S_EULER: project_seg_body<LMAX, TILE, S_EULER>(a, tile, sP, sQ); break;
+        case S_RK22_2: project_seg_body<LMAX, TILE, S_RK22_2>(a, tile, sP, sQ); break;
+        case S_RK33_2: project_seg_body<LMAX, TILE, S_RK33_2>(a, tile, sP, sQ); break;
+        case S_RK33_3: project_seg_body<LMAX, TILE, S_RK33_3>(a, tile, sP, sQ); break;
+        case S_AB2_1: project_seg_body<LMAX, TILE, S_AB2_1>(a, tile, sP, sQ); break;
+        default: project_seg_body<LMAX, TILE, S_AB2>(a, tile, sP, sQ); break;
     }
 }
 
