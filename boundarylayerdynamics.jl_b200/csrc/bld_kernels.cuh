@@ -121,6 +121,37 @@ __device__ __forceinline__ double2 inv_term_value(const InvYArgs& a, const doubl
 }
 
 // grid (ceil(K1/NL), n3, nterms*members); smem: tw[P2] + 2*P2*NL complex
+// Gather of one term's K2 x NL modes into the line buffer with the term kind
+// fixed at compile time (the loads of a batch are straight-line code).
+template <typename R, int OP>
+__device__ __forceinline__ void gather_term(const InvYArgs& a, const double2* __restrict__ S, int f, int z, int k10,
+                                            int nls, int LS, cplx<R>* b0) {
+    const int NL = a.NL, K1 = a.g.K1, K2 = a.g.K2, k2max = a.g.k2max, P2 = a.P2;
+    constexpr int BATCH = 8;
+    const int nmodes = K2 * NL;
+    for (int i0 = 0; i0 < nmodes; i0 += BATCH * blockDim.x) {
+        double2 v[BATCH];
+#pragma unroll
+        for (int q = 0; q < BATCH; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            v[q] = make_double2(0.0, 0.0);
+            if (i < nmodes) {
+                const int j = i >> nls, l = i & (NL - 1), k1 = k10 + l;
+                if (k1 < K1) v[q] = inv_term_value(a, S, OP, f, z, j, k1);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < BATCH; ++q) {
+            const int i = i0 + q * blockDim.x + threadIdx.x;
+            if (i < nmodes) {
+                const int j = i >> nls, l = i & (NL - 1);
+                const int p = (j <= k2max) ? j : P2 - (K2 - j);
+                b0[p * LS + l] = mk<R>((R)v[q].x, (R)v[q].y);
+            }
+        }
+    }
+}
+
 // grid (nterms*members, ceil(K1/NL), n3): the terms of one (layer, k1 tile) are
 // neighbouring blocks, so their shared state reads (vorticity needs z and z+1)
 // hit L2.  smem: tw[P2] + 2*P2*NL complex.
@@ -152,28 +183,13 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
         const int p = k2max + 1 + (i >> nls), l = i & (NL - 1);
         b0[p * LS + l] = mk<R>(0, 0);
     }
-    constexpr int BATCH = 8;
-    const int nmodes = K2 * NL;
-    for (int i0 = 0; i0 < nmodes; i0 += BATCH * blockDim.x) {
-        double2 v[BATCH];
-#pragma unroll
-        for (int q = 0; q < BATCH; ++q) {
-            const int i = i0 + q * blockDim.x + threadIdx.x;
-            v[q] = make_double2(0.0, 0.0);
-            if (i < nmodes) {
-                const int j = i >> nls, l = i & (NL - 1), k1 = k10 + l;
-                if (k1 < K1) v[q] = inv_term_value(a, S, op, f, z, j, k1);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < BATCH; ++q) {
-            const int i = i0 + q * blockDim.x + threadIdx.x;
-            if (i < nmodes) {
-                const int j = i >> nls, l = i & (NL - 1);
-                const int p = (j <= k2max) ? j : P2 - (K2 - j);
-                b0[p * LS + l] = mk<R>((R)v[q].x, (R)v[q].y);
-            }
-        }
+    switch (op) {
+        case T_DIRECT: gather_term<R, T_DIRECT>(a, S, f, z, k10, nls, LS, b0); break;
+        case T_D1: gather_term<R, T_D1>(a, S, f, z, k10, nls, LS, b0); break;
+        case T_D2: gather_term<R, T_D2>(a, S, f, z, k10, nls, LS, b0); break;
+        case T_VORT1: gather_term<R, T_VORT1>(a, S, f, z, k10, nls, LS, b0); break;
+        case T_VORT2: gather_term<R, T_VORT2>(a, S, f, z, k10, nls, LS, b0); break;
+        default: gather_term<R, T_VORT3>(a, S, f, z, k10, nls, LS, b0); break;
     }
     __syncthreads();
     C* res = b0;
@@ -996,6 +1012,30 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     // line l < NL: A set (k1 = k10 + l); NL <= l < 2NL: B set; loads batched 4 per thread
     constexpr int BATCH = 4;
     const int nval = P2 * nlines;
+    if (nc == 1 && a.c[fi][0].pref == 0) {
+        // a single contribution without prefactor (the advection rates): a plain
+        // strided copy, whose loads issue together
+        const C* src = base + (long long)(a.c[fi][0].term * g.n3 + z) * layer + k10;
+        constexpr int B2 = 8;
+        for (int i0 = 0; i0 < nval; i0 += B2 * blockDim.x) {
+            C v[B2];
+#pragma unroll
+            for (int q = 0; q < B2; ++q) {
+                const int i = i0 + q * blockDim.x + threadIdx.x;
+                v[q] = mk<R>(0, 0);
+                const int y = i >> nlsl, l = i & (nlines - 1);
+                if (i < nval && k10 + l < K1) v[q] = src[(long long)y * K1 + l];
+            }
+#pragma unroll
+            for (int q = 0; q < B2; ++q) {
+                const int i = i0 + q * blockDim.x + threadIdx.x;
+                if (i < nval) {
+                    const int y = i >> nlsl, l = i & (nlines - 1);
+                    b0[y * LS + l] = v[q];
+                }
+            }
+        }
+    } else
     for (int i0 = 0; i0 < nval; i0 += BATCH * blockDim.x) {
         C v[BATCH];
 #pragma unroll
