@@ -15,6 +15,8 @@
 //                                                               (add_layer! part 2)
 #pragma once
 
+#include <type_traits>
+
 #include "bld_fft.cuh"
 #include "bld_dft.cuh"
 #include "bld_warpfft.cuh"
@@ -444,16 +446,12 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
                 if (i < NLin * nk) {
                     const int line = i / nk, k = i - line * nk;
                     const int yl = line / 3, qq = line - yl * 3, y = y0 + yl;
-                    if (qq == 0) {
-                        va[q] = mrow(Min, a, 0, j, y)[k];
-                        vb[q] = mrow(Min, a, 1, j, y)[k];
-                    } else if (qq == 1) {
-                        va[q] = mrow(Min, a, 5, j, y)[k];
-                        if (hasI) vb[q] = mrow(Min, a, 2, j, y)[k];
-                    } else if (hasI) {
-                        va[q] = mrow(Min, a, 3, j, y)[k];
-                        vb[q] = mrow(Min, a, 4, j, y)[k];
-                    }
+                    // packed line qq: terms (0,1) (5,2) (3,4); w and the I-node
+                    // vorticities only below the top layer (branch-free loads)
+                    const int ta = (0x350 >> (4 * qq)) & 0xF, tb = (0x421 >> (4 * qq)) & 0xF;
+                    const bool oka = qq < 2 || hasI, okb = qq == 0 || hasI;
+                    if (oka) va[q] = mrow(Min, a, ta, j, y)[k];
+                    if (okb) vb[q] = mrow(Min, a, tb, j, y)[k];
                 }
             }
 #pragma unroll
@@ -617,17 +615,12 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
                     if (i < NLin * nk) {
                         const int line = i / nk, k = i - line * nk;
                         const int yl = line / 5, qq = line - yl * 5, y = y0 + yl;
-                        switch (qq) {
-                            case 0: va[q] = mrow(Min, a, 0, j, y)[k]; vb[q] = mrow(Min, a, 1, j, y)[k]; break;
-                            case 1: va[q] = mrow(Min, a, 3, j, y)[k]; vb[q] = mrow(Min, a, 4, j, y)[k]; break;
-                            case 2: va[q] = mrow(Min, a, 5, j, y)[k]; vb[q] = mrow(Min, a, 6, j, y)[k]; break;
-                            case 3:
-                                if (hasI) { va[q] = mrow(Min, a, 2, j, y)[k]; vb[q] = mrow(Min, a, 7, j, y)[k]; }
-                                break;
-                            default:
-                                if (hasI) va[q] = mrow(Min, a, 8, j, y)[k];
-                                break;
-                        }
+                        // packed line qq: terms (0,1) (3,4) (5,6) (2,7) (8,-), the last two
+                        // only below the top layer; table lookups keep the loads branch-free
+                        const int ta = (0x82530 >> (4 * qq)) & 0xF, tb = (0xF7641 >> (4 * qq)) & 0xF;
+                        const bool oka = qq < 3 || hasI, okb = qq < 3 || (qq == 3 && hasI);
+                        if (oka) va[q] = mrow(Min, a, ta, j, y)[k];
+                        if (okb) vb[q] = mrow(Min, a, tb, j, y)[k];
                     }
                 }
 #pragma unroll
@@ -1035,6 +1028,40 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
                 }
             }
         }
+    } else if (nc == 3 && hasB && a.c[fi][0].pref == 0 && a.c[fi][1].pref == 1 && a.c[fi][2].pref == 2) {
+        // the SGS pattern: A lines = T0 + D1 T1, B lines = T2; loads predicated, not branched
+        const C* s0 = base + (long long)(a.c[fi][0].term * g.n3 + z) * layer;
+        const C* s1 = base + (long long)(a.c[fi][1].term * g.n3 + z) * layer;
+        const C* s2 = base + (long long)(a.c[fi][2].term * g.n3 + z) * layer;
+        for (int i0 = 0; i0 < nval; i0 += BATCH * blockDim.x) {
+            C v[BATCH];
+#pragma unroll
+            for (int q = 0; q < BATCH; ++q) {
+                const int i = i0 + q * blockDim.x + threadIdx.x;
+                const int y = i >> nlsl, l = i & (nlines - 1);
+                const bool isB = l >= NL;
+                const int k1 = k10 + (isB ? l - NL : l);
+                const bool ok = i < nval && k1 < K1;
+                const long long off = (long long)y * K1 + k1;
+                C x0 = mk<R>(0, 0), x1 = mk<R>(0, 0), x2 = mk<R>(0, 0);
+                if (ok && !isB) {
+                    x0 = s0[off];
+                    x1 = s1[off];
+                }
+                if (ok && isB) x2 = s2[off];
+                const R d = ok ? (R)a.d1[k1] : R(0);
+                // D1 = i d1[k1] applied to T1, added after T0 (the order of the generic path)
+                v[q] = isB ? x2 : mk<R>(x0.x + (-d * x1.y), x0.y + d * x1.x);
+            }
+#pragma unroll
+            for (int q = 0; q < BATCH; ++q) {
+                const int i = i0 + q * blockDim.x + threadIdx.x;
+                if (i < nval) {
+                    const int y = i >> nlsl, l = i & (nlines - 1);
+                    b0[y * LS + l] = v[q];
+                }
+            }
+        }
     } else
     for (int i0 = 0; i0 < nval; i0 += BATCH * blockDim.x) {
         C v[BATCH];
@@ -1099,56 +1126,75 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     bool bad = false;
     constexpr int OB = 4;  // outputs per thread whose loads are issued together
     const int nout = K2 * NL;
-    for (int o0 = 0; o0 < nout; o0 += OB * blockDim.x) {
-        double2 W[OB][3];
-        double2 old[OB];
+    // the epilogue with the mode and the window loads fixed at compile time, so
+    // that the loads of OB outputs are straight-line code
+    auto epilogue = [&](auto mode_c, auto win_c) {
+        constexpr int MODE = decltype(mode_c)::value;
+        constexpr bool WIN = decltype(win_c)::value;
+        for (int o0 = 0; o0 < nout; o0 += OB * blockDim.x) {
+            double2 W[OB][3];
+            double2 old[OB];
 #pragma unroll
-        for (int q = 0; q < OB; ++q) {
-            const int o = o0 + q * blockDim.x + threadIdx.x;
-            const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
-            if (o < nout && k1 < K1) {
-                const long long idx = (long long)j * K1 + k1;
-                if (need_win) {
+            for (int q = 0; q < OB; ++q) {
+                const int o = o0 + q * blockDim.x + threadIdx.x;
+                const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
+                if (o < nout && k1 < K1) {
+                    const long long idx = (long long)j * K1 + k1;
+                    if constexpr (WIN) {
 #pragma unroll
-                    for (int r = 0; r < 3; ++r)
-                        if (r < wn) W[q][r] = Sf[(long long)(w0 + r) * g.F + idx];
+                        for (int r = 0; r < 3; ++r)
+                            if (r < wn) W[q][r] = Sf[(long long)(w0 + r) * g.F + idx];
+                    }
+                    if constexpr (MODE == 0) old[q] = du[idx];
                 }
-                if (a.mode == 0) old[q] = du[idx];
             }
-        }
 #pragma unroll
-        for (int q = 0; q < OB; ++q) {
-            const int o = o0 + q * blockDim.x + threadIdx.x;
-            const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
-            if (o >= nout || k1 >= K1) continue;
-            const int pos = (j <= k2max) ? j : P2 - (K2 - j);
-            const C X = res[pos * LS + l];
-            double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
-            if (hasB) {
-                const C Y = res[pos * LS + NL + l];
-                const double d = a.d2[j];
-                const double bx = (double)Y.x * a.inv_n, by = (double)Y.y * a.inv_n;
-                vx += -d * by;
-                vy += d * bx;
+            for (int q = 0; q < OB; ++q) {
+                const int o = o0 + q * blockDim.x + threadIdx.x;
+                const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
+                if (o >= nout || k1 >= K1) continue;
+                const int pos = (j <= k2max) ? j : P2 - (K2 - j);
+                const C X = res[pos * LS + l];
+                double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
+                if (hasB) {
+                    const C Y = res[pos * LS + NL + l];
+                    const double d = a.d2[j];
+                    const double bx = (double)Y.x * a.inv_n, by = (double)Y.y * a.inv_n;
+                    vx += -d * by;
+                    vy += d * bx;
+                }
+                const long long idx = (long long)j * K1 + k1;
+                double2 v;
+                if constexpr (MODE == 1) {
+                    double2 lin;
+                    if constexpr (WIN)
+                        lin = linear_terms_w(g, a.lin, W[q], w0, f, z, j, k1, m);
+                    else
+                        lin = linear_terms(g, a.lin, nullptr, f, z, j, k1, m);
+                    v = make_double2(lin.x + vx, lin.y + vy);
+                } else if constexpr (MODE == 2) {
+                    v = make_double2(vx, vy);
+                } else {
+                    v = make_double2(old[q].x + vx, old[q].y + vy);
+                }
+                du[idx] = v;
+                if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
             }
-            const long long idx = (long long)j * K1 + k1;
-            double2 v;
-            if (a.mode == 1) {
-                double2 lin;
-                if (need_win)
-                    lin = linear_terms_w(g, a.lin, W[q], w0, f, z, j, k1, m);
-                else
-                    lin = linear_terms(g, a.lin, nullptr, f, z, j, k1, m);
-                v = make_double2(lin.x + vx, lin.y + vy);
-            } else if (a.mode == 2) {
-                v = make_double2(vx, vy);
-            } else {
-                v = make_double2(old[q].x + vx, old[q].y + vy);
-            }
-            du[idx] = v;
-            if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
         }
-    }
+    };
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    using I2 = std::integral_constant<int, 2>;
+    using BT = std::integral_constant<bool, true>;
+    using BF = std::integral_constant<bool, false>;
+    if (a.mode == 1 && need_win)
+        epilogue(I1{}, BT{});
+    else if (a.mode == 1)
+        epilogue(I1{}, BF{});
+    else if (a.mode == 0)
+        epilogue(I0{}, BF{});
+    else
+        epilogue(I2{}, BF{});
     if (a.check && bad) atomicOr(a.flag + m, 1);
 }
 
