@@ -511,6 +511,12 @@ class Model:
         """Enqueues ``nsteps`` steps on the model's stream without waiting."""
         _capi.check(self._lib.bld_step_async(self._h, int(nsteps), float(dt), _METHODS[method]))
 
+    def idle(self):
+        """True when the work enqueued on the model's stream has finished (non-blocking)."""
+        v = C.c_int32(0)
+        _capi.check(self._lib.bld_stream_idle(self._h, C.byref(v)))
+        return bool(v.value)
+
     @property
     def stream(self):
         p = C.c_void_p()

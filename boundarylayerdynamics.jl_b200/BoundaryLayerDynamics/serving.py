@@ -10,9 +10,10 @@ request is admitted when its class has a free slot and its bytes fit in the
 budget left.  Requests that arrive while others run join at the next tick: the
 new member is loaded, projected and given its rates (``prepare_member``), and its
 slot is switched on in the device-side active mask, so the already-captured step
-graphs advance it together with the members in flight.  Every tick advances all
-busy pools by ``tick`` steps with one parent-graph launch per step.  A finished
-member's slot is switched off and reused.
+graphs advance it together with the members in flight.  Every pool advances on
+its own stream in ticks of ``tick`` steps, so the classes run concurrently on
+the device and a small request does not wait for the ticks of a large pool.  A
+finished member's slot is switched off and reused.
 
 ``Scheduler`` is the host-side admission logic alone (no device), so it can be
 tested and reasoned about on its own; ``Server`` binds it to pools of models.
@@ -26,7 +27,6 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import workloads
-from .ensemble import step_models
 
 # the served mix: (n, n3) size classes and their probabilities
 SIZES = ((64, 32), (128, 64), (192, 96), (256, 128))
@@ -137,12 +137,13 @@ class Scheduler:
         self.queue.append(req)
         return True
 
-    def admit(self):
-        """Pops every queued request that fits now; returns [(request, size, slot)]."""
+    def admit(self, ready=None):
+        """Pops every queued request that fits now (and whose pool is ``ready``,
+        when given); returns [(request, size, slot)]."""
         out, keep = [], []
         for r in self.queue:
             need = self.slot_bytes[r.size]
-            if self.free[r.size] and self.resident + need <= self.budget:
+            if (ready is None or ready(r.size)) and self.free[r.size] and self.resident + need <= self.budget:
                 slot = self.free[r.size].pop(0)
                 self.running[r.size][slot] = [r, r.steps]
                 self.resident += need
@@ -168,15 +169,21 @@ class Scheduler:
         left = [v[1] for s in self.capacity for v in self.running[s].values()]
         return min([tick] + left) if left else 0
 
-    def advance(self, nsteps):
-        """Counts ``nsteps`` steps for every running request; returns the finished ones."""
+    def advance(self, nsteps, size=None):
+        """Counts ``nsteps`` steps for every running request (of one pool, when
+        ``size`` is given); returns the finished ones."""
         done = []
-        for s in self.capacity:
+        for s in (self.capacity if size is None else (size,)):
             for slot, v in list(self.running[s].items()):
                 v[1] -= nsteps
                 if v[1] <= 0:
                     done.append((v[0], s, slot))
         return done
+
+    def next_tick_of(self, size, tick):
+        """Steps the next tick of one pool may take without running a member past its end."""
+        left = [v[1] for v in self.running[size].values()]
+        return min([tick] + left) if left else 0
 
     def release(self, size, slot):
         r, _ = self.running[size].pop(slot)
@@ -232,20 +239,25 @@ class Server:
 
     ``pools``: size -> model-like object with ``members`` slots and the slot API
     (``set_field``, ``set_member_params``, ``prepare_member``, ``set_active``,
-    ``get_state``, ``diverged_members``).  ``stepper(models, nsteps)`` advances the
-    given pools (default: one parent-graph launch per step for all of them).
+    ``get_state``, ``diverged_members``) and asynchronous stepping
+    (``step_async``, ``idle``, ``sync``).  Every pool advances on its own stream
+    in ticks of up to ``tick`` steps (graph launches) with no host wait: the loop
+    only polls which pools finished their tick, harvests their finished requests,
+    admits queued requests into pools that are between ticks and launches their
+    next tick.  Pools therefore run concurrently on the device and a small
+    request is not held back by the ticks of a large pool.
     """
 
-    def __init__(self, pools, slot_bytes, budget, dt=1e-4, tick=10, stepper=None, keep_results=False,
-                 clock=time.perf_counter, sleep=time.sleep):
+    def __init__(self, pools, slot_bytes, budget, dt=1e-4, tick=10, keep_results=False,
+                 clock=time.perf_counter, sleep=time.sleep, poll=1e-4):
         self.pools = dict(pools)
         self.sched = Scheduler({s: p.members for s, p in self.pools.items()}, slot_bytes, budget)
         self.dt = float(dt)
         self.tick = int(tick)
-        self.stepper = stepper or (lambda models, n: step_models(models, n, self.dt))
         self.keep_results = keep_results
         self.clock = clock
         self.sleep = sleep
+        self.poll = float(poll)
         self.ticks = 0
         self.launch_steps = 0
         for p in self.pools.values():
@@ -282,15 +294,41 @@ class Server:
         """Serves ``requests`` (arrival times relative to the call); returns the statistics."""
         from ._capi import DivergenceError
         pending = sorted(requests, key=lambda r: r.arrival)
+        inflight = {s: 0 for s in self.pools}        # steps of the tick on the device, 0 = idle
         self.t0 = self.clock()
         i = 0
-        while i < len(pending) or self.sched.queue or self.sched.busy():
+        while i < len(pending) or self.sched.queue or self.sched.busy() or any(inflight.values()):
+            progressed = False
             now = self.clock() - self.t0
             while i < len(pending) and pending[i].arrival <= now:
                 self.sched.submit(pending[i])
                 i += 1
+            # ticks that finished: divergence check, finished requests, slots freed
+            for size, pool in self.pools.items():
+                n = inflight[size]
+                if not n or not pool.idle():
+                    continue
+                progressed = True
+                inflight[size] = 0
+                try:
+                    pool.sync()
+                except DivergenceError:
+                    for slot in pool.diverged_members():
+                        if slot in self.sched.running[size]:
+                            r = self.sched.running[size][slot][0]
+                            self._fail(r, size, slot, "diverged", "The simulation has diverged.")
+                finished = self.sched.advance(n, size)
+                for req, s, slot in finished:
+                    if self.keep_results:
+                        req.result = pool.get_state(slot)
+                    req.done = self.clock() - self.t0
+                    req.status = "done"
+                    self.sched.release(s, slot)
+                pool.set_active(self.sched.mask(size))
+            # admissions into pools between ticks
             changed = set()
-            for req, size, slot in self.sched.admit():
+            for req, size, slot in self.sched.admit(ready=lambda s: inflight[s] == 0):
+                progressed = True
                 req.admitted = self.clock() - self.t0
                 try:
                     self._load(req, size, slot)
@@ -301,33 +339,21 @@ class Server:
                 changed.add(size)
             for size in changed:
                 self.pools[size].set_active(self.sched.mask(size))
-            busy = self.sched.busy()
-            if not busy:
-                if i < len(pending):
-                    self.sleep(max(0.0, pending[i].arrival - (self.clock() - self.t0)))
-                continue
-            n = self.sched.next_tick(self.tick)
-            models = [self.pools[s] for s in busy]
-            try:
-                self.stepper(models, n)
-            except DivergenceError:
-                for s in busy:
-                    for slot in self.pools[s].diverged_members():
-                        if slot in self.sched.running[s]:
-                            r = self.sched.running[s][slot][0]
-                            self._fail(r, s, slot, "diverged", "The simulation has diverged.")
-                    self.pools[s].set_active(self.sched.mask(s))
-            self.ticks += 1
-            self.launch_steps += n
-            finished = self.sched.advance(n)
-            for req, size, slot in finished:
-                if self.keep_results:
-                    req.result = self.pools[size].get_state(slot)
-                req.done = self.clock() - self.t0
-                req.status = "done"
-                self.sched.release(size, slot)
-            for size in {s for _, s, _ in finished}:
-                self.pools[size].set_active(self.sched.mask(size))
+            # next ticks of the idle pools that hold requests
+            for size, pool in self.pools.items():
+                if inflight[size] or not self.sched.running[size]:
+                    continue
+                n = self.sched.next_tick_of(size, self.tick)
+                pool.step_async(n, self.dt)
+                inflight[size] = n
+                self.ticks += 1
+                self.launch_steps += n
+                progressed = True
+            if not progressed:
+                if any(inflight.values()):
+                    self.sleep(self.poll)
+                elif i < len(pending):
+                    self.sleep(max(self.poll, pending[i].arrival - (self.clock() - self.t0)))
         return self.stats(requests)
 
     def stats(self, requests):
@@ -365,9 +391,11 @@ def calibrate_rate(server, probs=PROBS, steps=500, load=0.8, sample_steps=20):
         for m in range(pool.members):
             pool.set_state({}, member=m)
             pool.prepare_member(m)
-        server.stepper([pool], 2)
+        pool.step(2, server.dt)
+        pool.sync()
         t = time.perf_counter()
-        server.stepper([pool], sample_steps)
+        pool.step(sample_steps, server.dt)
+        pool.sync()
         dt = time.perf_counter() - t
         pool.set_active(np.zeros(pool.members, dtype=np.int32))
         per_request[size] = dt / sample_steps * steps / pool.members

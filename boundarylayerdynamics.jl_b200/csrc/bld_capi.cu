@@ -1846,6 +1846,19 @@ int32_t bld_sync(bld_handle* h) {
     return check_flag(h);
 }
 
+int32_t bld_stream_idle(bld_handle* h, int32_t* idle) {
+    if (!h || !idle) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const cudaError_t e = cudaStreamQuery(h->stream);
+    if (e == cudaErrorNotReady) {
+        *idle = 0;
+        return BLD_OK;
+    }
+    CUDA_TRY(e);
+    *idle = 1;
+    return BLD_OK;
+}
+
 int32_t bld_set_active(bld_handle* h, const int32_t* mask) {
     if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
     CUDA_TRY(cudaSetDevice(h->device));

@@ -174,6 +174,9 @@ int32_t bld_get_stream(bld_handle* h, void** stream);
 /* bld_step without the trailing synchronisation and divergence check: enqueues
    `nsteps` graph launches and returns; bld_sync reports the outcome. */
 int32_t bld_step_async(bld_handle* h, int64_t nsteps, double dt, int32_t method);
+/* Non-blocking: *idle = 1 when all work enqueued on the handle's stream has
+   finished (then bld_sync returns at once with the divergence check), else 0. */
+int32_t bld_stream_idle(bld_handle* h, int32_t* idle);
 
 /* Average device time of each launch kind of one right-hand side, measured with
    CUDA events on the handle's stream over `iters` back-to-back launches of that

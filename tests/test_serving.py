@@ -25,7 +25,8 @@ class FakeClock:
 
 
 class FakePool:
-    """A pool with `members` slots whose "state" is the number of steps taken."""
+    """A pool with `members` slots whose "state" is the number of steps taken;
+    a tick of n steps keeps it busy for n * cost seconds of the fake clock."""
 
     def __init__(self, members, clock, cost):
         self.members = members
@@ -36,8 +37,11 @@ class FakePool:
         self.params = {}
         self.loaded = {}
         self.diverge_at = {}
+        self.busy_until = 0.0
+        self.ticks = 0
 
     def set_field(self, f, values, member):
+        assert self.idle(), "a pool is loaded only between ticks"
         self.loaded.setdefault(member, []).append(f)
         self.steps[member] = 0
 
@@ -53,6 +57,21 @@ class FakePool:
     def get_state(self, m):
         return {"steps": int(self.steps[m]), "params": self.params[m]}
 
+    def step_async(self, n, dt):
+        assert self.idle(), "one tick at a time per pool"
+        self.steps += n * (self.active != 0)
+        self.busy_until = self.clock.t + n * self.cost
+        self.ticks += 1
+
+    def idle(self):
+        return self.clock.t >= self.busy_until
+
+    def sync(self):
+        from BoundaryLayerDynamics._capi import DivergenceError
+        self.clock.t = max(self.clock.t, self.busy_until)
+        if any(self.active[m] and self.steps[m] >= s for m, s in self.diverge_at.items()):
+            raise DivergenceError(-3, "The simulation has diverged.")
+
     def diverged_members(self):
         out = [m for m, s in self.diverge_at.items() if self.active[m] and self.steps[m] >= s]
         for m in out:
@@ -60,25 +79,11 @@ class FakePool:
         return out
 
 
-def fake_stepper(clock):
-    def step(models, n):
-        from BoundaryLayerDynamics._capi import DivergenceError
-        clock.t += n * sum(p.cost for p in models)
-        bad = False
-        for p in models:
-            p.steps += n * (p.active != 0)
-            bad |= any(p.active[m] and p.steps[m] >= s for m, s in p.diverge_at.items())
-        if bad:
-            raise DivergenceError(-3, "The simulation has diverged.")
-    return step
-
-
 def _server(capacity, budget=10**12, slot_bytes=None, tick=10, keep=True):
     clock = FakeClock()
     pools = {s: FakePool(c, clock, cost=1e-4 * s[0] / 64) for s, c in capacity.items()}
     sb = slot_bytes or {s: 10**6 * s[0] for s in capacity}
-    srv = S.Server(pools, sb, budget, tick=tick, stepper=fake_stepper(clock), keep_results=keep,
-                   clock=clock, sleep=clock.sleep)
+    srv = S.Server(pools, sb, budget, tick=tick, keep_results=keep, clock=clock, sleep=clock.sleep, poll=1e-5)
     return srv, pools, clock
 
 
@@ -176,6 +181,7 @@ def test_server_exact_steps_and_slot_reuse():
         assert r.done >= r.admitted >= r.arrival
     # continuous batching: some requests ran together in one pool
     assert srv.ticks < sum(math.ceil(50 / 7) for _ in reqs)
+    assert srv.ticks == sum(p.ticks for p in pools.values())
     assert st["p99_latency_s"] >= st["p50_latency_s"] > 0
     assert st["updates_per_s"] > 0
 
@@ -203,3 +209,18 @@ def test_server_isolates_a_diverged_member():
     for r in reqs:
         if r.status == "done":
             assert r.result["steps"] == 20
+
+
+def test_server_pools_advance_independently():
+    """A small request finishes while a large pool is still busy with long ticks."""
+    small, large = (32, 16), (256, 128)
+    clock = FakeClock()
+    pools = {small: FakePool(2, clock, cost=1e-5), large: FakePool(2, clock, cost=1e-2)}
+    srv = S.Server(pools, {small: 1, large: 1}, 10**9, tick=10, keep_results=True, clock=clock,
+                   sleep=clock.sleep, poll=1e-5)
+    big = S.Request(0, large, 50, 0.0, 1e-4, 1.0, 0)
+    tiny = S.Request(1, small, 50, 0.001, 1e-4, 1.0, 1)
+    srv.run([big, tiny])
+    assert big.status == tiny.status == "done"
+    assert tiny.result["steps"] == 50 and big.result["steps"] == 50
+    assert tiny.latency < 0.01 < big.latency          # 50 x 1e-5 s vs 50 x 1e-2 s of device time
