@@ -135,6 +135,7 @@ struct Space {
     long long min_ms = 0, mout_ms = 0;  // elements per member
     int YT = 1, PPT = 1, zchunk = 1, nchunks = 1;  // x kernels: rows per block, points per thread, z chunks
     int xw = 0;                                     // > 0: warp-per-row x kernel with xw warps per block
+    int zmult = 1;                                  // x kernels: z-chunk count multiplier (autotuned)
     bool xb = false;                                // block of three warps per row (advection)
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
@@ -256,6 +257,9 @@ void x_chunks(const bld_handle* h, Space& s) {
     const long long blocks_per_chunk = (long long)((s.P2 + rows - 1) / rows) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
     want = std::min(want, std::max(1, n3 / 8));
+    // the autotuner may ask for more chunks (shorter streams, more blocks: a
+    // smaller partial last wave), down to 4 layers per chunk
+    want = std::min(want * s.zmult, std::max(1, n3 / 4));
     s.zchunk = (n3 + want - 1) / want;
     s.nchunks = (n3 + s.zchunk - 1) / s.zchunk;
 }
@@ -933,6 +937,23 @@ int autotune(bld_handle* h) {
         s.xr = bxr;
         s.YT = byt;
         s.PPT = bppt;
+        // z-chunk count of the chosen x kernel
+        {
+            float bz = 1e30f;
+            int bm = 1, last_chunks = -1;
+            for (int mult = 1; mult <= 8; mult *= 2) {
+                s.zmult = mult;
+                x_chunks(h, s);
+                if (s.nchunks == last_chunks) continue;
+                last_chunks = s.nchunks;
+                BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
+                if (t < bz) {
+                    bz = t;
+                    bm = mult;
+                }
+            }
+            s.zmult = bm;
+        }
         x_chunks(h, s);
         best = 1e30f;
         YCfg bf = s.fwd;
