@@ -565,11 +565,11 @@ def reset(model):
         model.set_state({}, member=m)
 
 
-def evolve(model, tspan, dt=None, method=SSPRK33):
-    """``evolve!(model, tspan; dt, method)`` (src/BoundaryLayerDynamics.jl:190-219)."""
+def evolve(model, tspan, dt=None, method=SSPRK33, output=()):
+    """``evolve!(model, tspan; dt, method, output)`` (src/BoundaryLayerDynamics.jl:190-219)."""
     if dt is None:
         raise ValueError("The keyword argument `dt` is mandatory")
-    return model.evolve(tspan, dt, method)
+    return model.evolve(tspan, dt, method, output=output)
 
 
 def coordinates(model, field="vel1"):
