@@ -1125,19 +1125,32 @@ int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first) {
 }
 
 // segmented batched LDL^T solve: LMAX layers per thread, NS = ceil(n / LMAX)
-// segments (<= 64 for n <= 1024), LANES systems per block with LANES * NS <= 512
+// segments, LANES systems per block with LANES * NS <= 512
 template <typename T>
 int ldlt_launch(const double* gamma, const double* beta, T* rhs, long long nsys, int n, cudaStream_t st) {
     if (n > 1024) return fail(BLD_ERR_ARGUMENT, "tridiagonal systems longer than 1024 are not supported");
-    const int lmax = n <= 256 ? 8 : 16;
-    const int NS = (n + lmax - 1) / lmax;   // <= 64
-    int lanes = 32;
-    while (lanes * NS > 512) lanes /= 2;    // >= 8 lanes: rows of >= 64 bytes
+    // layers per thread and systems per block (BLD_LDLT_LMAX = 4|8|16, BLD_LDLT_LANES override them).
+    // 16 layers and 16 systems per thread row measured best at n = 256 (5.5 TB/s complex,
+    // against 3.5 TB/s with 8 layers x 16 systems): more loads in flight per thread
+    int lmax = 16;
+    const char* el = getenv("BLD_LDLT_LMAX");
+    if (el && (atoi(el) == 4 || atoi(el) == 8 || atoi(el) == 16) && (n + atoi(el) - 1) / atoi(el) <= 512)
+        lmax = atoi(el);
+    const int NS = (n + lmax - 1) / lmax;
+    int lanes = 16;
+    while (lanes > 1 && lanes * NS > 512) lanes /= 2;    // rows of >= 64 bytes for n <= 1024 at lmax 16
+    const char* eln = getenv("BLD_LDLT_LANES");
+    if (eln) {
+        const int v = atoi(eln);
+        if ((v == 4 || v == 8 || v == 16 || v == 32) && v * NS <= 512) lanes = v;
+    }
     const dim3 block(lanes, NS);
     const long long nb = (nsys + lanes - 1) / lanes;
     if (nb > 2147483647LL) return fail(BLD_ERR_ARGUMENT, "too many systems");
     const size_t smem = (size_t)(n & ~1) * sizeof(double) + (size_t)NS * lanes * (sizeof(T) + sizeof(double));
-    if (lmax == 8)
+    if (lmax == 4)
+        k_ldlt_seg<T, 4><<<(unsigned)nb, block, smem, st>>>(gamma, beta, rhs, nsys, n);
+    else if (lmax == 8)
         k_ldlt_seg<T, 8><<<(unsigned)nb, block, smem, st>>>(gamma, beta, rhs, nsys, n);
     else
         k_ldlt_seg<T, 16><<<(unsigned)nb, block, smem, st>>>(gamma, beta, rhs, nsys, n);
