@@ -213,6 +213,21 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
         res = fft_big<R, +1>(b0, b1, NL, 1, NL, false, a.plan, tw);
     }
     C* out = reinterpret_cast<C*>(a.mixed) + (long long)m * a.mixed_mstride + (long long)(t * a.g.n3 + z) * P2 * K1;
+    if constexpr (sizeof(C) == 8) {
+        // single precision: two neighbouring modes per 16-byte store (rows and
+        // tiles start at even k1 when K1 is even)
+        if ((K1 & 1) == 0 && NL >= 2) {
+            const int half = NL >> 1;
+            for (int i = threadIdx.x; i < P2 * half; i += blockDim.x) {
+                const int y = i >> (nls - 1), l = 2 * (i & (half - 1)), k1 = k10 + l;
+                if (k1 < K1) {
+                    const C v0 = res[y * LS + l], v1 = res[y * LS + l + 1];
+                    *reinterpret_cast<float4*>(out + (long long)y * K1 + k1) = make_float4(v0.x, v0.y, v1.x, v1.y);
+                }
+            }
+            return;
+        }
+    }
     for (int i = threadIdx.x; i < P2 * NL; i += blockDim.x) {
         const int y = i >> nls, l = i & (NL - 1), k1 = k10 + l;
         if (k1 < K1) out[(long long)y * K1 + k1] = res[y * LS + l];
