@@ -135,7 +135,8 @@ struct Space {
     long long min_ms = 0, mout_ms = 0;  // elements per member
     int YT = 1, PPT = 1, zchunk = 1, nchunks = 1;  // x kernels: rows per block, points per thread, z chunks
     int xw = 0;                                     // > 0: warp-per-row x kernel with xw warps per block
-    int zmult = 1;                                  // x kernels: z-chunk count multiplier (autotuned)
+    int xwmb = 1;                                   // warp-per-row kernel: register cap (min blocks of 128 threads)
+    int zmult = 2;                                  // x kernels: z-chunk count multiplier in halves (autotuned)
     bool xb = false;                                // block of three warps per row (advection)
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
@@ -259,7 +260,7 @@ void x_chunks(const bld_handle* h, Space& s) {
     want = std::min(want, std::max(1, n3 / 8));
     // the autotuner may ask for more chunks (shorter streams, more blocks: a
     // smaller partial last wave), down to 4 layers per chunk
-    want = std::min(want * s.zmult, std::max(1, n3 / 4));
+    want = std::min(std::max(1, want * s.zmult / 2), std::max(1, n3 / 4));
     s.zchunk = (n3 + want - 1) / want;
     s.nchunks = (n3 + s.zchunk - 1) / s.zchunk;
 }
@@ -303,6 +304,12 @@ void tile_space(const bld_handle* h, Space& s, bool is_adv) {
 }
 
 size_t smem_y(int P2, int NL, bool fp32) { return (size_t)(P2 + 2 * P2 * NL) * csize(fp32); }
+// per-term y kernels with `lines` lines: twiddles and two line buffers for the
+// block-wide stages, or twiddles and one buffer on a line stride of lines + 1
+// for the warp transforms
+size_t smem_y_term(int P2, int lines, int wfft, bool fp32) {
+    return (size_t)(wfft ? P2 + P2 * (lines + 1) : P2 + 2 * P2 * lines) * csize(fp32);
+}
 size_t smem_adv(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 3 * s.YT * s.P1) * csize(fp32); }
 size_t smem_sgs(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 5 * s.YT * s.P1) * csize(fp32); }
 
@@ -339,7 +346,7 @@ int launch_inv_y(bld_handle* h, const Space& s, InvYArgs a, int nm) {
         k_inv_y_all<R><<<grid, c.thr, (size_t)(s.P2 + s.P2 * a.nterms * c.NL) * cs, h->stream>>>(a);
     } else {
         dim3 grid(a.nterms * nm, (h->g.K1 + c.NL - 1) / c.NL, h->g.n3);
-        const size_t sm = (size_t)(s.P2 + 2 * s.P2 * c.NL) * cs;
+        const size_t sm = smem_y_term(s.P2, c.NL, c.wfft, sizeof(R) == 4);
         switch (c.wfft) {
             case 0: k_inv_y<R, 0><<<grid, c.thr, sm, h->stream>>>(a); break;
             case 2: k_inv_y<R, 2><<<grid, c.thr, sm, h->stream>>>(a); break;
@@ -367,7 +374,7 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
         k_fwd_y_all<R><<<grid, c.thr, (size_t)(s.P2 + s.P2 * 3 * s.fsets * c.NL) * cs, h->stream>>>(a);
     } else {
         dim3 grid(a.fields * nm, (h->g.K1 + c.NL - 1) / c.NL, h->g.n3);
-        const size_t sm = (size_t)(s.P2 + 2 * s.P2 * s.fsets * c.NL) * cs;
+        const size_t sm = smem_y_term(s.P2, s.fsets * c.NL, c.wfft, sizeof(R) == 4);
         switch (c.wfft) {
             case 0: k_fwd_y<R, 0><<<grid, c.thr, sm, h->stream>>>(a); break;
             case 2: k_fwd_y<R, 2><<<grid, c.thr, sm, h->stream>>>(a); break;
@@ -432,12 +439,38 @@ int warpx_radix(int P1) {
     return (r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 9 || r == 12) ? r : 0;
 }
 
+// register caps compiled for the warp-per-row x kernel (single precision, radix >= 8)
+template <typename R>
+bool warpx_minb_ok(int r, int mb) {
+    if (mb == 1) return true;
+    return sizeof(R) == 4 && (r == 8 || r == 9 || r == 12) && (mb == 3 || mb == 4);
+}
+
 template <typename R>
 int launch_adv_xw(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     const int r = warpx_radix<R>(s.P1);
     dim3 grid((s.P2 + s.xw - 1) / s.xw, s.nchunks, nm);
     const int thr = 32 * s.xw;
     const size_t sm = ((size_t)r * 32 + (size_t)s.xw * 12 * h->g.K1) * csize(sizeof(R) == 4);
+    if constexpr (sizeof(R) == 4) {
+        if (s.xwmb > 1) {
+            if (!warpx_minb_ok<R>(r, s.xwmb)) return fail(BLD_ERR_INVALID_CONFIG, "no capped warp x kernel");
+#define BLD_XW_MB(RR)                                                                   \
+    case RR:                                                                            \
+        if (s.xwmb == 3) k_adv_xwc<R, RR, 3><<<grid, thr, sm, h->stream>>>(a);          \
+        else k_adv_xwc<R, RR, 4><<<grid, thr, sm, h->stream>>>(a);                      \
+        break;
+            switch (r) {
+                BLD_XW_MB(8)
+                BLD_XW_MB(9)
+                BLD_XW_MB(12)
+                default: return fail(BLD_ERR_INVALID_CONFIG, "no capped warp x kernel");
+            }
+#undef BLD_XW_MB
+            CUDA_TRY(cudaGetLastError());
+            return BLD_OK;
+        }
+    }
     switch (r) {
         case 2: k_adv_xw<R, 2><<<grid, thr, sm, h->stream>>>(a); break;
         case 3: k_adv_xw<R, 3><<<grid, thr, sm, h->stream>>>(a); break;
@@ -573,6 +606,12 @@ int set_smem_limits_R() {
         BLD_SET((k_adv_xw<R, 8>));
         BLD_SET((k_adv_xw<R, 9>));
         BLD_SET((k_adv_xw<R, 12>));
+        BLD_SET((k_adv_xwc<R, 8, 3>));
+        BLD_SET((k_adv_xwc<R, 9, 3>));
+        BLD_SET((k_adv_xwc<R, 12, 3>));
+        BLD_SET((k_adv_xwc<R, 8, 4>));
+        BLD_SET((k_adv_xwc<R, 9, 4>));
+        BLD_SET((k_adv_xwc<R, 12, 4>));
     }
 #undef BLD_SET
     return BLD_OK;
@@ -788,20 +827,20 @@ bool yforce_warp() {
 std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_per_nl, int all_lines_per_nl) {
     std::vector<YCfg> out;
     const size_t cs = csize(h->fp32);
-    const int nls_pt[3] = {h->fp32 ? 4 : 2, h->fp32 ? 8 : 4, h->fp32 ? 16 : 8};
+    const int nls_pt[4] = {h->fp32 ? 4 : 2, h->fp32 ? 8 : 4, h->fp32 ? 16 : 8, h->fp32 ? 32 : 16};
     for (int nl : nls_pt) {
-        if ((size_t)(s.P2 + 2 * s.P2 * lines_per_nl * nl) * cs > 150 * 1024) continue;
+        const int wr = s.P2 % 32 ? 0 : s.P2 / 32;
+        if (wfft_radix_ok(wr) && !ydisable_warp() && smem_y_term(s.P2, lines_per_nl * nl, wr, h->fp32) <= 150 * 1024) {
+            out.push_back(YCfg{0, nl, 128, wr});
+            out.push_back(YCfg{0, nl, 256, wr});
+        }
+        if (nl == nls_pt[3] || (size_t)(s.P2 + 2 * s.P2 * lines_per_nl * nl) * cs > 150 * 1024) continue;
         int thrs[3] = {y_threads(s.plan2, lines_per_nl * nl), 128, 256};
         for (int i = 0; i < 3; ++i) {
             bool dup = false;
             for (int k = 0; k < i; ++k) dup |= thrs[k] == thrs[i];
             const bool warp_possible = wfft_radix_ok(s.P2 % 32 ? 0 : s.P2 / 32);
             if (!dup && !(yforce_warp() && warp_possible)) out.push_back(YCfg{0, nl, thrs[i], 0});
-        }
-        const int wr = s.P2 % 32 ? 0 : s.P2 / 32;
-        if (wfft_radix_ok(wr) && !ydisable_warp()) {
-            out.push_back(YCfg{0, nl, 128, wr});
-            out.push_back(YCfg{0, nl, 256, wr});
         }
     }
     const int nls_all[2] = {h->fp32 ? 2 : 1, h->fp32 ? 4 : 2};
@@ -937,22 +976,35 @@ int autotune(bld_handle* h) {
         s.xr = bxr;
         s.YT = byt;
         s.PPT = bppt;
-        // z-chunk count of the chosen x kernel
+        // z-chunk count of the chosen x kernel (and, for the warp-per-row
+        // kernel, its register cap: more resident warps want more chunks)
         {
             float bz = 1e30f;
-            int bm = 1, last_chunks = -1;
-            for (int mult = 1; mult <= 8; mult *= 2) {
-                s.zmult = mult;
-                x_chunks(h, s);
-                if (s.nchunks == last_chunks) continue;
-                last_chunks = s.nchunks;
-                BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
-                if (t < bz) {
-                    bz = t;
-                    bm = mult;
+            int bm = 2, bmb = 1;
+            const int r = h->fp32 ? warpx_radix<float>(s.P1) : warpx_radix<double>(s.P1);
+            const char* mbe = getenv("BLD_XW_MINB");   // force one register cap (1, 3, 4)
+            const int mb_only = mbe && mbe[0] ? atoi(mbe) : 0;
+            for (int mb : {1, 3, 4}) {
+                if (mb > 1 && !(s.xw && (h->fp32 ? warpx_minb_ok<float>(r, mb) : warpx_minb_ok<double>(r, mb))))
+                    continue;
+                if (mb_only && s.xw && mb != mb_only) continue;
+                s.xwmb = mb;
+                int last_chunks = -1;
+                for (int mult : {2, 3, 4, 6, 8, 12, 16}) {
+                    s.zmult = mult;
+                    x_chunks(h, s);
+                    if (s.nchunks == last_chunks) continue;
+                    last_chunks = s.nchunks;
+                    BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
+                    if (t < bz) {
+                        bz = t;
+                        bm = mult;
+                        bmb = mb;
+                    }
                 }
             }
             s.zmult = bm;
+            s.xwmb = bmb;
         }
         x_chunks(h, s);
         best = 1e30f;
@@ -1939,6 +1991,8 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         char xname[96];
         if (sp == 0 && s.xb)
             snprintf(xname, sizeof xname, "k_adv_xb<%s, %d>", R, s.P1 / 32);
+        else if (sp == 0 && s.xw && s.xwmb > 1)
+            snprintf(xname, sizeof xname, "k_adv_xwc<%s, %d, %d>", R, s.P1 / 32, s.xwmb);
         else if (sp == 0 && s.xw)
             snprintf(xname, sizeof xname, "k_adv_xw<%s, %d>", R, s.P1 / 32);
         else

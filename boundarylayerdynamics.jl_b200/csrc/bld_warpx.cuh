@@ -17,8 +17,11 @@
 // copied into the warp's shared buffer (cp.async) while layer j is transformed.
 // grid (ceil(P2 / WPB), nchunks, members), block 32 * WPB; dynamic smem:
 // W_P^{-l k} as [k][32] (RAD * 32 complex), then per warp 2 x 6 rows of K1.
+// k_adv_xwc<R, RAD, MINB> is the same kernel with the registers capped at
+// 65536 / (128 MINB) per thread, so that more warps share an SM (the values of
+// the previous layer may then spill a little).
 template <typename R, int RAD>
-__global__ void __launch_bounds__(128) k_adv_xw(XArgs a) {
+__device__ __forceinline__ void adv_xw_body(const XArgs& a) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* twl_all = reinterpret_cast<C*>(smem_raw);
@@ -148,6 +151,12 @@ __global__ void __launch_bounds__(128) k_adv_xw(XArgs a) {
     }
     cp_async_wait<0>();
 }
+
+template <typename R, int RAD>
+__global__ void __launch_bounds__(128) k_adv_xw(XArgs a) { adv_xw_body<R, RAD>(a); }
+
+template <typename R, int RAD, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_adv_xwc(XArgs a) { adv_xw_body<R, RAD>(a); }
 
 // Rotation-form advection with one block of three warps per y row: each warp
 // transforms one packed line in registers (inverse: (u, v), (vort3, w),

@@ -95,6 +95,33 @@ def test_advection_x_kernel_family(oracle, BLD, res, precision, tol, family):
         assert e < tol, (res, precision, family, gm.info.adv_p1, f, e)
 
 
+@pytest.mark.parametrize("minb", ["3", "4"])
+@pytest.mark.parametrize("res", [(171, 6, 4), (192, 8, 5), (256, 6, 4)])
+def test_warp_x_kernel_register_caps(oracle, BLD, res, minb):
+    """The warp-per-row x kernel compiled with a register cap (3 or 4 blocks of
+    128 threads per SM; radices 8, 9, 12), forced, against the oracle (1e-5)."""
+    saved = {k: os.environ.get(k) for k in ("BLD_X_KERNEL", "BLD_XW_MINB")}
+    os.environ["BLD_X_KERNEL"] = "warp"
+    os.environ["BLD_XW_MINB"] = minb
+    try:
+        gm = _build(BLD, res, "mixed")
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    xk = gm.kernels()["advection"]["x"]
+    assert xk.startswith("k_adv_xwc<") and xk.endswith(", %s>" % minb), xk
+    om = _build(oracle, res)
+    st = _state(om, seed=sum(res) + int(minb))
+    ref = om.compute_rates(st)
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < 1e-5, (res, minb, f, e)
+
+
 @pytest.mark.parametrize("family", ["warp", "blockwarp"])
 def test_warp_kernel_les_mixed_trajectory(oracle, BLD, family):
     """The warp advection kernels inside a full LES step sequence (mixed form)."""
