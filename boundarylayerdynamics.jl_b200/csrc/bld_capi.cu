@@ -137,7 +137,7 @@ struct Space {
     int xw = 0;                                     // > 0: warp-per-row x kernel with xw warps per block
     int xwmb = 1;                                   // warp-per-row kernel: register cap (min blocks of 128 threads)
     int zmult = 2;                                  // x kernels: z-chunk count multiplier in halves (autotuned)
-    bool xb = false;                                // block of three warps per row (advection)
+    int xb = 0;                                     // block of warps per row (advection): 1 three warps, 2 five (pipelined)
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
@@ -502,6 +502,21 @@ template <typename R>
 int launch_adv_xb(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     const int r = xb_radix(s.P1);
     dim3 grid(s.P2, s.nchunks, nm);
+    if (s.xb == 2) {
+        const size_t smp = ((size_t)r * 32 + 5 * (size_t)s.P1 + 12 * (size_t)h->g.K1) * csize(sizeof(R) == 4);
+        switch (r) {
+            case 2: k_adv_xp<R, 2><<<grid, 160, smp, h->stream>>>(a); break;
+            case 3: k_adv_xp<R, 3><<<grid, 160, smp, h->stream>>>(a); break;
+            case 4: k_adv_xp<R, 4><<<grid, 160, smp, h->stream>>>(a); break;
+            case 6: k_adv_xp<R, 6><<<grid, 160, smp, h->stream>>>(a); break;
+            case 8: k_adv_xp<R, 8><<<grid, 160, smp, h->stream>>>(a); break;
+            case 9: k_adv_xp<R, 9><<<grid, 160, smp, h->stream>>>(a); break;
+            case 12: k_adv_xp<R, 12><<<grid, 160, smp, h->stream>>>(a); break;
+            default: return fail(BLD_ERR_INVALID_CONFIG, "no pipelined block-of-warps x kernel for P1=%d", s.P1);
+        }
+        CUDA_TRY(cudaGetLastError());
+        return BLD_OK;
+    }
     const size_t sm = ((size_t)r * 32 + 3 * (size_t)s.P1 + 12 * (size_t)h->g.K1) * csize(sizeof(R) == 4);
     switch (r) {
         case 2: k_adv_xb<R, 2><<<grid, 96, sm, h->stream>>>(a); break;
@@ -598,6 +613,13 @@ int set_smem_limits_R() {
     BLD_SET((k_adv_xb<R, 8>));
     BLD_SET((k_adv_xb<R, 9>));
     BLD_SET((k_adv_xb<R, 12>));
+    BLD_SET((k_adv_xp<R, 2>));
+    BLD_SET((k_adv_xp<R, 3>));
+    BLD_SET((k_adv_xp<R, 4>));
+    BLD_SET((k_adv_xp<R, 6>));
+    BLD_SET((k_adv_xp<R, 8>));
+    BLD_SET((k_adv_xp<R, 9>));
+    BLD_SET((k_adv_xp<R, 12>));
     BLD_SET((k_adv_xw<R, 2>));
     BLD_SET((k_adv_xw<R, 3>));
     BLD_SET((k_adv_xw<R, 4>));
@@ -877,7 +899,8 @@ int autotune(bld_handle* h) {
     // BLD_X_KERNEL=warp|block restricts the advection x kernel to one family
     const char* xk = getenv("BLD_X_KERNEL");
     const bool only_warp = xk && !strcmp(xk, "warp"), only_block = xk && !strcmp(xk, "block");
-    const bool only_bw = xk && !strcmp(xk, "blockwarp");
+    const bool only_bw3 = xk && !strcmp(xk, "blockwarp"), only_pipe = xk && !strcmp(xk, "pipe");
+    const bool only_bw = only_bw3 || only_pipe;   // a block-of-warps kernel (three warps, or five pipelined)
     const bool only_lines = xk && !strcmp(xk, "lines");   // block kernels with warp line transforms
     const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1) > 0;
     if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
@@ -890,7 +913,7 @@ int autotune(bld_handle* h) {
             x_chunks(h, h->adv);
         }
         if (only_bw && adv_bw_ok) {
-            h->adv.xb = true;
+            h->adv.xb = only_pipe ? 2 : 1;
             x_chunks(h, h->adv);
         }
         return BLD_OK;
@@ -946,66 +969,62 @@ int autotune(bld_handle* h) {
             }
             s.xr = 0;
         }
-        int bxw = 0;
-        const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw && !only_lines;
-        for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) {
-            s.xw = wpb;
+        // finalists: the best block kernel above, the warp-per-row kernel with
+        // 1, 2, 4 warps per block and the block-of-warps kernels, each timed at
+        // its best z-chunk count (and, for the warp-per-row kernel, register
+        // cap: more resident warps want more chunks)
+        struct XPick {
+            int YT, PPT, xr, xw, xwmb, xb, zmult;
+        };
+        auto get_pick = [&]() { return XPick{s.YT, s.PPT, s.xr, s.xw, s.xwmb, s.xb, s.zmult}; };
+        auto set_pick = [&](const XPick& p) {
+            s.YT = p.YT;
+            s.PPT = p.PPT;
+            s.xr = p.xr;
+            s.xw = p.xw;
+            s.xwmb = p.xwmb;
+            s.xb = p.xb;
+            s.zmult = p.zmult;
             x_chunks(h, s);
-            BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
-            if (t < best) {
-                best = t;
-                bxw = wpb;
-                bxr = 0;
-            }
-        }
-        s.xw = 0;
-        bool bxb = false;
-        if (sp == 0 && adv_bw_ok && !only_block && !only_warp && !only_lines) {
-            s.xb = true;
-            x_chunks(h, s);
-            BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
-            if (t < best) {
-                best = t;
-                bxb = true;
-                bxw = 0;
-                bxr = 0;
-            }
-        }
-        s.xb = bxb;
-        s.xw = bxw;
-        s.xr = bxr;
-        s.YT = byt;
-        s.PPT = bppt;
-        // z-chunk count of the chosen x kernel (and, for the warp-per-row
-        // kernel, its register cap: more resident warps want more chunks)
-        {
-            float bz = 1e30f;
-            int bm = 2, bmb = 1;
+        };
+        const char* mbe = getenv("BLD_XW_MINB");   // force one register cap (1, 3, 4)
+        const int mb_only = mbe && mbe[0] ? atoi(mbe) : 0;
+        float bx = 1e30f;
+        XPick bp{};
+        auto tune_chunks = [&](XPick base) -> int {
             const int r = h->fp32 ? warpx_radix<float>(s.P1) : warpx_radix<double>(s.P1);
-            const char* mbe = getenv("BLD_XW_MINB");   // force one register cap (1, 3, 4)
-            const int mb_only = mbe && mbe[0] ? atoi(mbe) : 0;
             for (int mb : {1, 3, 4}) {
-                if (mb > 1 && !(s.xw && (h->fp32 ? warpx_minb_ok<float>(r, mb) : warpx_minb_ok<double>(r, mb))))
+                if (mb > 1 && !(base.xw && (h->fp32 ? warpx_minb_ok<float>(r, mb) : warpx_minb_ok<double>(r, mb))))
                     continue;
-                if (mb_only && s.xw && mb != mb_only) continue;
-                s.xwmb = mb;
+                if (mb_only && base.xw && mb != mb_only) continue;
                 int last_chunks = -1;
                 for (int mult : {2, 3, 4, 6, 8, 12, 16}) {
-                    s.zmult = mult;
-                    x_chunks(h, s);
+                    XPick p = base;
+                    p.xwmb = mb;
+                    p.zmult = mult;
+                    set_pick(p);
                     if (s.nchunks == last_chunks) continue;
                     last_chunks = s.nchunks;
                     BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
-                    if (t < bz) {
-                        bz = t;
-                        bm = mult;
-                        bmb = mb;
+                    if (t < bx) {
+                        bx = t;
+                        bp = p;
                     }
                 }
             }
-            s.zmult = bm;
-            s.xwmb = bmb;
+            return BLD_OK;
+        };
+        const bool block_ok = best < 1e30f;   // a block kernel was timed above
+        if (block_ok) BLD_TRY(tune_chunks(XPick{byt, bppt, bxr, 0, 1, 0, 2}));
+        const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw && !only_lines;
+        for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) BLD_TRY(tune_chunks(XPick{1, 1, 0, wpb, 1, 0, 2}));
+        for (int xbk = 1; xbk <= 2; ++xbk) {
+            if (!(sp == 0 && adv_bw_ok && !only_block && !only_warp && !only_lines)) break;
+            if ((xbk == 1 && only_pipe) || (xbk == 2 && only_bw3)) continue;
+            BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2}));
         }
+        if (bx >= 1e30f) return fail(BLD_ERR_INVALID_CONFIG, "no x kernel could be timed");
+        set_pick(bp);
         x_chunks(h, s);
         best = 1e30f;
         YCfg bf = s.fwd;
@@ -1990,7 +2009,7 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         const char* xk = sp == 0 ? "k_adv_x" : "k_sgs_x";
         char xname[96];
         if (sp == 0 && s.xb)
-            snprintf(xname, sizeof xname, "k_adv_xb<%s, %d>", R, s.P1 / 32);
+            snprintf(xname, sizeof xname, "%s<%s, %d>", s.xb == 2 ? "k_adv_xp" : "k_adv_xb", R, s.P1 / 32);
         else if (sp == 0 && s.xw && s.xwmb > 1)
             snprintf(xname, sizeof xname, "k_adv_xwc<%s, %d, %d>", R, s.P1 / 32, s.xwmb);
         else if (sp == 0 && s.xw)

@@ -289,3 +289,143 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
     }
     cp_async_wait<0>();
 }
+
+// k_adv_xb with its transforms pipelined over two warp groups: five warps per y
+// row, where warps 0-2 run the inverse transforms of layer j while warps 3-4 run
+// the forward transforms of layer j - 1, then all five form the products of
+// layer j (shared memory L -> F).  Two barriers per layer instead of three, and
+// no warp idles while the forward lines run.  The staged rows of layer j + 1
+// are requested (cp.async) at the top of iteration j and waited for before the
+// barrier that ends the products.
+// grid (P2, nchunks, members), block 160; dynamic smem: W_P^{-l k} [RAD][32],
+// inverse lines L [3][P1], product lines F [2][P1], staging [2][6][K1] (complex).
+template <typename R, int RAD>
+__global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
+    using C = cplx<R>;
+    constexpr int NT = 160;
+    constexpr int PPT = (32 * RAD + NT - 1) / NT;   // product points per thread
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* twl_all = reinterpret_cast<C*>(smem_raw);
+    const int P1 = a.P1, n3 = a.g.n3, k1max = a.g.k1max, K1 = a.g.K1;
+    C* L = twl_all + RAD * 32;            // [3][P1]
+    C* F = L + 3 * P1;                    // [2][P1]
+    C* stage = F + 2 * P1;                // [2][6][K1]
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int m = a.m0 + blockIdx.z;
+    BLD_SKIP_INACTIVE(a, m);
+    for (int i = threadIdx.x; i < RAD * 32; i += blockDim.x) {
+        const int k = i >> 5, l = i & 31;
+        double s, c;
+        sincospi(-2.0 * (double)(l * k) / (double)P1, &s, &c);
+        twl_all[i] = mk<R>((R)c, (R)s);
+    }
+    const int y = blockIdx.x;
+    const C* twl = twl_all + lane;
+    LaneTw<R> lt;
+    lane_twiddles<R>(lt, lane);
+    const int brl = (int)(__brev((unsigned)lane) >> 27);
+    const int z0 = blockIdx.y * a.zchunk;
+    const int z1 = min(n3, z0 + a.zchunk);
+    const C* Min = reinterpret_cast<const C*>(a.min) + (long long)m * a.min_mstride;
+    C* Mout = reinterpret_cast<C*>(a.mout) + (long long)m * a.mout_mstride;
+    const int nb = (k1max + 32) / 32;
+    // staged rows: u, v, vort3 (C); w, vort1, vort2 (I) = terms 0, 1, 5, 2, 3, 4
+    auto issue = [&](int j, C* buf) {
+        const int nrows = (j < n3 - 1) ? 6 : 3;
+        for (int i = threadIdx.x; i < nrows * K1; i += blockDim.x) {
+            const int r = i / K1, k = i - r * K1;
+            const int t = r < 2 ? r : (r == 2 ? 5 : r - 1);
+            cp_async_elem<C>(buf + i, mrow(Min, a, t, j, y) + k);
+        }
+    };
+
+    R pu[PPT], pv[PPT], pw[PPT], po1[PPT], po2[PPT];
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) pu[i] = pv[i] = pw[i] = po1[i] = po2[i] = R(0);
+
+    const int jb = max(0, z0 - 1);
+    issue(jb, stage);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();   // staged rows of jb and the twiddle table visible
+    for (int j = jb; j <= z1; ++j) {
+        const bool inv = j < z1;
+        const bool hasI = (j < n3 - 1);
+        if (j + 1 < z1) issue(j + 1, stage + ((j + 1 - jb) & 1) * 6 * K1);
+        cp_async_commit();
+        if (wib < 3) {
+            // ---- inverse: warp t transforms line t of layer j into L[t] (physical order)
+            if (inv && wib < (hasI ? 3 : 2)) {
+                const C* cur = stage + ((j - jb) & 1) * 6 * K1;
+                C zl[RAD];
+                const C* ra = cur + (wib == 0 ? 0 : (wib == 1 ? 2 : 4)) * K1;
+                const C* rb = (wib == 1 && !hasI) ? nullptr : cur + (wib == 0 ? 1 : (wib == 1 ? 3 : 5)) * K1;
+                load_packed<R, RAD>(zl, ra, rb, lane, P1, k1max);
+                inverse_line<R, RAD>(zl, lane, twl, 32, lt);
+#pragma unroll
+                for (int k = 0; k < RAD; ++k) L[wib * P1 + k + RAD * brl] = zl[k];
+            }
+        } else {
+            // ---- forward of layer lj = j - 1: warp 3 (adv1, adv2) on C layer lj,
+            // warp 4 (adv3, 0) on I layer lj - 1
+            const int lj = j - 1, fw = wib - 3;
+            const bool emit = lj >= jb && lj >= z0 && (fw == 0 || lj >= 1);
+            if (emit) {
+                C zl[RAD];
+#pragma unroll
+                for (int k = 0; k < RAD; ++k) zl[k] = F[fw * P1 + k + RAD * brl];
+                forward_line<R, RAD>(zl, lane, twl, 32, lt);
+                C* rA = mrow_w(Mout, a, fw == 0 ? 0 : 2, fw == 0 ? lj : lj - 1, y);
+                C* rB = mrow_w(Mout, a, 1, lj, y);
+#pragma unroll
+                for (int b = 0; b < RAD; ++b) {
+                    if (b >= nb) break;
+                    const int f = lane + 32 * b;
+                    const C Zk = zl[b];
+                    const C Zr = mirror_mode<R, RAD>(zl, lane, b);
+                    if (f <= k1max) {
+                        rA[f] = mk<R>((Zk.x + Zr.x) * R(0.5), (Zk.y - Zr.y) * R(0.5));
+                        if (fw == 0) rB[f] = mk<R>((Zk.y + Zr.y) * R(0.5), -(Zk.x - Zr.x) * R(0.5));
+                    }
+                }
+            }
+        }
+        __syncthreads();   // L of layer j written; F of layer j - 1 read
+        if (inv) {
+            // ---- products at the thread's points: L -> F
+#pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+                const int x = threadIdx.x + NT * i;
+                if (x < P1) {
+                    const C c0 = L[x], c1 = L[P1 + x];
+                    const C c2 = hasI ? L[2 * P1 + x] : mk<R>(R(0), R(0));
+                    const R u = c0.x, v = c0.y, o3 = c1.x;
+                    const R w = hasI ? c1.y : R(0);
+                    const R q1 = c2.x, q2 = c2.y;
+                    R adv1, adv2;
+                    if (j == 0) {  // w below is the (zero) boundary value (:181-184,:194-197)
+                        adv1 = o3 * v - R(0.5) * (q2 * w);
+                        adv2 = R(0.5) * (q1 * w) - o3 * u;
+                    } else if (j == n3 - 1) {  // w above is the boundary value (:185-188,:198-201)
+                        adv1 = o3 * v - R(0.5) * (po2[i] * pw[i]);
+                        adv2 = R(0.5) * (po1[i] * pw[i]) - o3 * u;
+                    } else {  // (:180,:193)
+                        adv1 = o3 * v - R(0.5) * (po2[i] * pw[i] + q2 * w);
+                        adv2 = R(0.5) * (po1[i] * pw[i] + q1 * w) - o3 * u;
+                    }
+                    // adv3 on I layer j-1 (:206)
+                    const R adv3 = po2[i] * R(0.5) * (pu[i] + u) - po1[i] * R(0.5) * (pv[i] + v);
+                    F[x] = mk<R>(adv1, adv2);
+                    F[P1 + x] = mk<R>(adv3, R(0));
+                    pu[i] = u;
+                    pv[i] = v;
+                    pw[i] = w;
+                    po1[i] = q1;
+                    po2[i] = q2;
+                }
+            }
+        }
+        cp_async_wait<0>();   // this thread's copies of layer j + 1
+        __syncthreads();      // F of layer j written, L read; staged rows of j + 1 visible
+    }
+}

@@ -3,9 +3,10 @@
 The autotuner keeps whichever variant is fastest on the device, so the parity
 tests elsewhere exercise only the winners.  Here BLD_X_KERNEL forces the
 advection x pass to the warp-per-row kernel (register transforms with lane
-shuffles) or to the block kernel (shared-memory Stockham stages), and each is
-compared with the oracle at the plain form's 1e-12 and the mixed form's 1e-5,
-over every radix the warp kernel is compiled for.
+shuffles), the block kernel (shared-memory Stockham stages), the block of three
+warps per row, its pipelined five-warp form, or the block kernel with warp line
+transforms, and each is compared with the oracle at the plain form's 1e-12 and
+the mixed form's 1e-5, over every radix the warp kernel is compiled for.
 """
 
 import math
@@ -79,7 +80,7 @@ CASES = [
 
 
 @pytest.mark.parametrize("res,precision,tol", CASES)
-@pytest.mark.parametrize("family", ["warp", "block", "blockwarp", "lines"])
+@pytest.mark.parametrize("family", ["warp", "block", "blockwarp", "pipe", "lines"])
 def test_advection_x_kernel_family(oracle, BLD, res, precision, tol, family):
     if family == "warp" and precision == "fp64" and res[0] == 192:
         pytest.skip("the warp-per-row kernel is compiled for radix <= 6 in FP64 (P1 = 288 is radix 9)")
@@ -122,7 +123,7 @@ def test_warp_x_kernel_register_caps(oracle, BLD, res, minb):
         assert e < 1e-5, (res, minb, f, e)
 
 
-@pytest.mark.parametrize("family", ["warp", "blockwarp"])
+@pytest.mark.parametrize("family", ["warp", "blockwarp", "pipe"])
 def test_warp_kernel_les_mixed_trajectory(oracle, BLD, family):
     """The warp advection kernels inside a full LES step sequence (mixed form)."""
     res = (64, 64, 16)
