@@ -569,7 +569,8 @@ def run_profile(args):
     m.sync()
     torch.cuda.profiler.stop()
     return {"profile": args.config, "precision": args.precision, "steps": args.profile_steps,
-            "adv_p": [m.info.adv_p1, m.info.adv_p2], "sgs_p": [m.info.sgs_p1, m.info.sgs_p2]}
+            "adv_p": [m.info.adv_p1, m.info.adv_p2], "sgs_p": [m.info.sgs_p1, m.info.sgs_p2],
+            "kernels": m.kernels()}
 
 
 def main():

@@ -747,8 +747,17 @@ int enqueue_x_R(bld_handle* h, int sp, int m0, int nm) {
     return launch_sgs_x<R>(h, s, xa, nm);
 }
 
+// explicit stage update fused into the last forward y pass of a right-hand side:
+// sout = (cu su + ct state + cd rate) / div
+struct StageFuse {
+    const double2* su;
+    double2* sout;
+    double cu, ct, cd, div;
+};
+
 template <typename R>
-int enqueue_fwd_y_R(bld_handle* h, int sp, bool first, bool last, const double2* state, double2* du, int m0, int nm) {
+int enqueue_fwd_y_R(bld_handle* h, int sp, bool first, bool last, const double2* state, double2* du, int m0, int nm,
+                    const StageFuse* sf = nullptr) {
     Space& s = sp == 0 ? h->adv : h->sgs;
     FwdYArgs fa{};
     fa.g = h->g;
@@ -791,6 +800,16 @@ int enqueue_fwd_y_R(bld_handle* h, int sp, bool first, bool last, const double2*
     fa.active = h->mask_on ? h->active : nullptr;
     fa.plan = s.plan2;
     fa.tw = twp(h, s.P2, sizeof(R) == 4);
+    if (sf) {
+        if (s.fwd.all) return fail(BLD_ERR_INVALID_CONFIG, "stage fusion needs the per-term forward y kernel");
+        fa.fuse = 1;
+        fa.su = sf->su;
+        fa.sout = sf->sout;
+        fa.st_cu = sf->cu;
+        fa.st_ct = sf->ct;
+        fa.st_cd = sf->cd;
+        fa.st_div = sf->div;
+    }
     return launch_fwd_y<R>(h, s, fa, nm);
 }
 
@@ -818,9 +837,10 @@ int enqueue_inv_y(bld_handle* h, int sp, const double2* st, int m0, int nm) {
 int enqueue_x(bld_handle* h, int sp, int m0, int nm) {
     return h->fp32 ? enqueue_x_R<float>(h, sp, m0, nm) : enqueue_x_R<double>(h, sp, m0, nm);
 }
-int enqueue_fwd_y(bld_handle* h, int sp, bool first, bool last, const double2* st, double2* du, int m0, int nm) {
-    return h->fp32 ? enqueue_fwd_y_R<float>(h, sp, first, last, st, du, m0, nm)
-                   : enqueue_fwd_y_R<double>(h, sp, first, last, st, du, m0, nm);
+int enqueue_fwd_y(bld_handle* h, int sp, bool first, bool last, const double2* st, double2* du, int m0, int nm,
+                  const StageFuse* sf = nullptr) {
+    return h->fp32 ? enqueue_fwd_y_R<float>(h, sp, first, last, st, du, m0, nm, sf)
+                   : enqueue_fwd_y_R<double>(h, sp, first, last, st, du, m0, nm, sf);
 }
 
 int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const double2* t, const double2* du,
@@ -892,9 +912,12 @@ int time_launches(bld_handle* h, F&& fn, int iters, float* ms) {
     return st == BLD_ERR_CUDA ? fail(BLD_ERR_CUDA, "autotune timing failed") : st;
 }
 
+bool stage_fusable(const bld_handle* h);
+
 // Picks, per physical-domain space, the fastest y-pass variants and x-kernel
 // tiling by timing every candidate on the handle's own buffers.  All candidates
 // perform the same arithmetic, so the choice changes speed, not results.
+
 int autotune(bld_handle* h) {
     // BLD_X_KERNEL=warp|block restricts the advection x kernel to one family
     const char* xk = getenv("BLD_X_KERNEL");
@@ -1053,9 +1076,19 @@ int autotune(bld_handle* h) {
             if (v == 3 && h->g.n3 > 128) break;   // the tile variant holds n3 <= 128 layers
             if (only_v >= 0 && v != only_v) continue;
             h->proj_variant = v;
-            // timed as an SSP-RK33 middle stage (three inputs), the kind that dominates a step
-            BLD_TRY(time_launches(h, [&] { return enqueue_project(h, S_RK33_2, 1e-4, h->u, h->t, h->du, nullptr, h->io, 0, B); },
-                                  3, &t));
+            // timed as the projections of one SSP-RK33 step: with the stage update
+            // fused into the forward y pass, one Euler stage and two plain
+            // projections in place; otherwise an Euler stage and two middle stages
+            // (three inputs)
+            const bool fz = stage_fusable(h);
+            BLD_TRY(time_launches(h, [&] {
+                BLD_TRY(enqueue_project(h, S_EULER, 1e-4, h->u, nullptr, h->du, nullptr, h->io, 0, B));
+                for (int k = 0; k < 2; ++k) {
+                    if (fz) BLD_TRY(enqueue_project(h, S_NONE, 1e-4, h->io, nullptr, nullptr, nullptr, h->io, 0, B));
+                    else BLD_TRY(enqueue_project(h, S_RK33_2, 1e-4, h->u, h->t, h->du, nullptr, h->io, 0, B));
+                }
+                return (int)BLD_OK;
+            }, 3, &t));
             if (t < best) {
                 best = t;
                 bv = v;
@@ -1072,7 +1105,8 @@ int autotune(bld_handle* h) {
 
 // compute_rates! (src/Processes.jl:39-62): nonlinear processes in the reference's
 // process order (advection, then SGS), each rate written once with the linear terms
-int enqueue_rates_impl(bld_handle* h, const double2* state, double2* du, int m0, int nm) {
+int enqueue_rates_impl(bld_handle* h, const double2* state, double2* du, int m0, int nm,
+                       const StageFuse* sf = nullptr) {
     for (int sp = 0; sp < 2; ++sp) {
         if (!(sp == 0 ? h->adv.on : h->sgs.on)) continue;
         BLD_TRY(enqueue_inv_y(h, sp, state, m0, nm));
@@ -1082,11 +1116,24 @@ int enqueue_rates_impl(bld_handle* h, const double2* state, double2* du, int m0,
     for (int sp = 0; sp < 2; ++sp) {
         if (!(sp == 0 ? h->adv.on : h->sgs.on)) continue;
         const bool last = (sp == 1) || !h->sgs.on;
-        BLD_TRY(enqueue_fwd_y(h, sp, first, last, state, du, m0, nm));
+        BLD_TRY(enqueue_fwd_y(h, sp, first, last, state, du, m0, nm, last ? sf : nullptr));
         first = false;
     }
-    if (first) BLD_TRY(enqueue_linear(h, state, du, m0, nm));
+    if (first) {
+        if (sf) return fail(BLD_ERR_INVALID_CONFIG, "stage fusion needs a forward y pass");
+        BLD_TRY(enqueue_linear(h, state, du, m0, nm));
+    }
     return BLD_OK;
+}
+
+// The stage update can ride on the last forward y pass when that pass is the
+// per-term kernel (BLD_NO_STAGE_FUSION=1 keeps the update in the projection).
+bool stage_fusable(const bld_handle* h) {
+    const char* e = getenv("BLD_NO_STAGE_FUSION");
+    if (e && e[0] && e[0] != '0') return false;
+    if (!h->adv.on && !h->sgs.on) return false;
+    const Space& last = h->sgs.on ? h->sgs : h->adv;
+    return !last.fwd.all;
 }
 
 int enqueue_rates(bld_handle* h, const double2* state, double2* du, int m0, int nm) {
@@ -1163,16 +1210,38 @@ int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first) {
             break;
         case BLD_SSPRK22:
             BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->t, 0, B));
-            BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
-            BLD_TRY(enqueue_project(h, S_RK22_2, dt, h->u, h->t, h->du, nullptr, h->u, 0, B));
+            if (stage_fusable(h)) {
+                // u <- (u + t + dt f(t)) / 2 in the forward y pass (u is read and
+                // written element by element; the pass reads t), then project u
+                const StageFuse sf{h->u, h->u, 1.0, 1.0, dt, 2.0};
+                BLD_TRY(enqueue_rates_impl(h, h->t, h->du, 0, B, &sf));
+                BLD_TRY(enqueue_project(h, S_NONE, dt, h->u, nullptr, nullptr, nullptr, h->u, 0, B));
+            } else {
+                BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
+                BLD_TRY(enqueue_project(h, S_RK22_2, dt, h->u, h->t, h->du, nullptr, h->u, 0, B));
+            }
             BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
             break;
         case BLD_SSPRK33:
             BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->t, 0, B));
-            BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
-            BLD_TRY(enqueue_project(h, S_RK33_2, dt, h->u, h->t, h->du, nullptr, h->t, 0, B));
-            BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
-            BLD_TRY(enqueue_project(h, S_RK33_3, dt, h->u, h->t, h->du, nullptr, h->u, 0, B));
+            if (stage_fusable(h)) {
+                // second stage into du (free once the first stage consumed it; the
+                // pass reads t, so the stage value cannot overwrite t in place)
+                const StageFuse s2{h->u, h->du, 3.0, 1.0, dt, 4.0};
+                BLD_TRY(enqueue_rates_impl(h, h->t, h->du, 0, B, &s2));
+                BLD_TRY(enqueue_project(h, S_NONE, dt, h->du, nullptr, nullptr, nullptr, h->du, 0, B));
+                // third stage into u from the second-stage state held in du; the
+                // partial rates of a first forward pass (when two physical-domain
+                // spaces contribute) go to t, which the first stage left free
+                const StageFuse s3{h->u, h->u, 1.0, 2.0, 2.0 * dt, 3.0};
+                BLD_TRY(enqueue_rates_impl(h, h->du, h->t, 0, B, &s3));
+                BLD_TRY(enqueue_project(h, S_NONE, dt, h->u, nullptr, nullptr, nullptr, h->u, 0, B));
+            } else {
+                BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
+                BLD_TRY(enqueue_project(h, S_RK33_2, dt, h->u, h->t, h->du, nullptr, h->t, 0, B));
+                BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
+                BLD_TRY(enqueue_project(h, S_RK33_3, dt, h->u, h->t, h->du, nullptr, h->u, 0, B));
+            }
             BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
             break;
         case BLD_AB2: {

@@ -837,6 +837,14 @@ struct FwdYArgs {
     int check;                 // set *flag on a non-finite result
     double2* du;               // member stride g.mstride
     long long du_mstride;
+    // fused stage update (k_fwd_y, modes 0 and 1): instead of the rate d, write
+    // sout = (st_cu su + st_ct state + st_cd d) / st_div, the explicit
+    // SSP-RK stage value that the projection would otherwise form from d
+    // (src/ODEMethods.jl:143,157,164); su and sout have the member stride of du
+    int fuse;
+    const double2* su;
+    double2* sout;
+    double st_cu, st_ct, st_cd, st_div;
     const double2* state;
     Linear lin;
     const double* d1;
@@ -1143,12 +1151,15 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     const int nout = K2 * NL;
     // the epilogue with the mode and the window loads fixed at compile time, so
     // that the loads of OB outputs are straight-line code
-    auto epilogue = [&](auto mode_c, auto win_c) {
+    double2* so = a.fuse ? a.sout + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F : nullptr;
+    const double2* su = a.fuse ? a.su + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F : nullptr;
+    auto epilogue = [&](auto mode_c, auto win_c, auto fuse_c) {
         constexpr int MODE = decltype(mode_c)::value;
         constexpr bool WIN = decltype(win_c)::value;
+        constexpr bool FUSE = decltype(fuse_c)::value;
         for (int o0 = 0; o0 < nout; o0 += OB * blockDim.x) {
             double2 W[OB][3];
-            double2 old[OB];
+            double2 old[OB], U[OB], T[OB];
 #pragma unroll
             for (int q = 0; q < OB; ++q) {
                 const int o = o0 + q * blockDim.x + threadIdx.x;
@@ -1161,6 +1172,10 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
                             if (r < wn) W[q][r] = Sf[(long long)(w0 + r) * g.F + idx];
                     }
                     if constexpr (MODE == 0) old[q] = du[idx];
+                    if constexpr (FUSE) {
+                        U[q] = su[idx];
+                        if constexpr (!WIN) T[q] = Sf[(long long)z * g.F + idx];
+                    }
                 }
             }
 #pragma unroll
@@ -1192,7 +1207,20 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
                 } else {
                     v = make_double2(old[q].x + vx, old[q].y + vy);
                 }
-                du[idx] = v;
+                if constexpr (FUSE) {
+                    double2 tz;
+                    if constexpr (WIN) {
+                        const int r = z - w0;   // the window holds layer z
+                        tz = r == 0 ? W[q][0] : (r == 1 ? W[q][1] : W[q][2]);
+                    } else {
+                        tz = T[q];
+                    }
+                    const double2 uz = U[q];
+                    so[idx] = make_double2((a.st_cu * uz.x + a.st_ct * tz.x + a.st_cd * v.x) / a.st_div,
+                                           (a.st_cu * uz.y + a.st_ct * tz.y + a.st_cd * v.y) / a.st_div);
+                } else {
+                    du[idx] = v;
+                }
                 if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
             }
         }
@@ -1202,14 +1230,20 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     using I2 = std::integral_constant<int, 2>;
     using BT = std::integral_constant<bool, true>;
     using BF = std::integral_constant<bool, false>;
-    if (a.mode == 1 && need_win)
-        epilogue(I1{}, BT{});
+    if (a.fuse && a.mode == 1 && need_win)
+        epilogue(I1{}, BT{}, BT{});
+    else if (a.fuse && a.mode == 1)
+        epilogue(I1{}, BF{}, BT{});
+    else if (a.fuse && a.mode == 0)
+        epilogue(I0{}, BF{}, BT{});
+    else if (a.mode == 1 && need_win)
+        epilogue(I1{}, BT{}, BF{});
     else if (a.mode == 1)
-        epilogue(I1{}, BF{});
+        epilogue(I1{}, BF{}, BF{});
     else if (a.mode == 0)
-        epilogue(I0{}, BF{});
+        epilogue(I0{}, BF{}, BF{});
     else
-        epilogue(I2{}, BF{});
+        epilogue(I2{}, BF{}, BF{});
     if (a.check && bad) atomicOr(a.flag + m, 1);
 }
 

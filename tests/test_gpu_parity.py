@@ -170,6 +170,38 @@ def test_trajectory_parity(oracle, BLD, method):
         assert rel_l2(got[f], om.state[f]) < TRAJ_TOL, (f, rel_l2(got[f], om.state[f]))
 
 
+@pytest.mark.parametrize("method", ["SSPRK33", "SSPRK22"])
+@pytest.mark.parametrize("case", ["dns_16x16x8", "les_16x16x8", "stretched_dns", "les_24x18x7_nodamp"])
+def test_stage_fusion_matches_unfused(oracle, BLD, case, method):
+    """The SSP-RK stage update formed in the forward y pass (default) against the
+    same steps with the update in the projection (BLD_NO_STAGE_FUSION=1), and
+    both against the oracle: 20 steps, 1e-12 between the two engine paths."""
+    import os
+    res, dom, procs = CASES[case]
+    om = oracle.Model(res, dom(oracle), procs(oracle))
+    st = _random_state(om, seed=len(case), scale=2.0)
+    om.apply_projections(st)
+    runs = []
+    for off in ("0", "1"):
+        old = os.environ.get("BLD_NO_STAGE_FUSION")
+        os.environ["BLD_NO_STAGE_FUSION"] = off
+        try:
+            gm = BLD.Model(res, dom(BLD), procs(BLD))
+            gm.set_state(st)
+            gm.evolve(20 * 1e-3, 1e-3, method=getattr(BLD, method))
+            runs.append(gm.state)
+        finally:
+            if old is None:
+                del os.environ["BLD_NO_STAGE_FUSION"]
+            else:
+                os.environ["BLD_NO_STAGE_FUSION"] = old
+    om.state.update({f: v.copy() for f, v in st.items()})
+    om.evolve(20 * 1e-3, 1e-3, method=getattr(oracle, method))
+    for f in om.fields:
+        assert rel_l2(runs[0][f], runs[1][f]) < 1e-12, (f, rel_l2(runs[0][f], runs[1][f]))
+        assert rel_l2(runs[0][f], om.state[f]) < TRAJ_TOL, (f, rel_l2(runs[0][f], om.state[f]))
+
+
 def test_trajectory_parity_dns(oracle, BLD):
     spec = dict(kind="dns", resolution=(24, 24, 12), size=(4 * math.pi, 2 * math.pi, 2.0), lower=("smooth",),
                 upper=("smooth",), nu=1 / 180, forcing=1.0, sgs=None, dt=1e-4, steps=100, seed=5)
