@@ -55,6 +55,19 @@ __device__ __forceinline__ void copy_table(C* dst, const C* __restrict__ src, in
     }
 }
 
+// The twiddles of a block's transforms in shared memory: for the block-wide
+// stages (RAD = 0) the [P] table W_P^(-m) as it is; for the warp transforms
+// (P = 32 RAD) the lane-major [RAD][32] table W_P^(-l k), which lane l reads at
+// stride 32 without bank conflicts (at stride l, lanes collide for even k)
+template <int RAD, typename C>
+__device__ __forceinline__ void lane_table(C* dst, const C* __restrict__ src, int P) {
+    if constexpr (RAD > 0) {
+        for (int i = threadIdx.x; i < P; i += blockDim.x) dst[i] = src[(i >> 5) * (i & 31)];
+    } else {
+        copy_table(dst, src, P);
+    }
+}
+
 // ------------------------------------------------------------------ inverse y pass
 enum TermOp { T_DIRECT = 0, T_D1 = 1, T_D2 = 2, T_VORT1 = 3, T_VORT2 = 4, T_VORT3 = 5 };
 
@@ -178,7 +191,7 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
     const int K1 = a.g.K1, K2 = a.g.K2, k2max = a.g.k2max, P2 = a.P2;
     const int k10 = blockIdx.y * NL;
     const C* twg = reinterpret_cast<const C*>(a.tw);
-    copy_table(tw, twg, P2);
+    lane_table<RAD>(tw, twg, P2);
     const double2* S = a.state + (long long)m * a.g.mstride;
     // zero the padding band, then gather the K2*NL modes in batches of 8 per thread
     for (int i = threadIdx.x; i < (P2 - K2) * NL; i += blockDim.x) {
@@ -199,12 +212,12 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
         const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
         const int brl = (int)(__brev((unsigned)lane) >> 27);
         LaneTw<R> lt;
-        lane_twiddles_tab<R>(lt, lane, tw, P2);
+        lane_twiddles_tab<R>(lt, lane, twg, P2);
         for (int l = threadIdx.x >> 5; l < NL; l += nw) {
             C zl[RAD];
 #pragma unroll
             for (int q = 0; q < RAD; ++q) zl[q] = b0[(lane + 32 * q) * LS + l];
-            inverse_line<R, RAD>(zl, lane, tw, lane, lt);
+            inverse_line<R, RAD>(zl, lane, tw + lane, 32, lt);
 #pragma unroll
             for (int k = 0; k < RAD; ++k) b0[(k + RAD * brl) * LS + l] = zl[k];
         }
@@ -1022,7 +1035,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     C* b0 = tw + P2;
     C* b1 = b0 + P2 * nlines;
     const C* twg = reinterpret_cast<const C*>(a.tw);
-    copy_table(tw, twg, P2);
+    lane_table<RAD>(tw, twg, P2);
     const C* base = reinterpret_cast<const C*>(a.mout) + (long long)m * a.mout_mstride;
     const long long layer = (long long)P2 * K1;
     // line l < NL: A set (k1 = k10 + l); NL <= l < 2NL: B set; loads batched 4 per thread
@@ -1128,12 +1141,12 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
         const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
         const int brl = (int)(__brev((unsigned)lane) >> 27);
         LaneTw<R> lt;
-        lane_twiddles_tab<R>(lt, lane, tw, P2);
+        lane_twiddles_tab<R>(lt, lane, twg, P2);
         for (int l = threadIdx.x >> 5; l < nlines; l += nw) {
             C zl[RAD];
 #pragma unroll
             for (int k = 0; k < RAD; ++k) zl[k] = b0[(k + RAD * brl) * LS + l];
-            forward_line<R, RAD>(zl, lane, tw, lane, lt);
+            forward_line<R, RAD>(zl, lane, tw + lane, 32, lt);
 #pragma unroll
             for (int b = 0; b < RAD; ++b) b0[(lane + 32 * b) * LS + l] = zl[b];
         }
@@ -1655,6 +1668,9 @@ __device__ __forceinline__ void project_seg_body(const ProjArgs& a, double2* til
     const int j = cc / g.K1, k1 = cc - j * g.K1;
     const bool mean_mode = (c == 0);
     const double e1 = a.d1[k1], e2 = a.d2[j];
+    // a plain projection in place: the stage values are the stored values, so
+    // phase 1 need not write them out again (phase 3 reads them from u = out)
+    const bool in_place = (KIND == S_NONE) && (a.out == a.u);
     // stage value of w just below the segment, read before any thread writes `out`
     double2 wprev = make_double2(0.0, 0.0);
     if (valid && z0 > 0 && len > 0) wprev = stage_value_k<KIND>(a, o3 + (long long)(z0 - 1) * F + c);
@@ -1688,7 +1704,7 @@ __device__ __forceinline__ void project_seg_body(const ProjArgs& a, double2* til
                     tile[(0 * n + z) * LN + lane] = uz;
                     tile[(1 * n + z) * LN + lane] = vz;
                     if (z < n - 1) tile[(2 * n + z) * LN + lane] = wz;
-                } else {
+                } else if (!in_place) {
                     a.out[o1 + z * F + c] = uz;
                     a.out[o2 + z * F + c] = vz;
                     if (z < n - 1) a.out[o3 + z * F + c] = wz;
