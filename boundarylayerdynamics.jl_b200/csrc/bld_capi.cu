@@ -305,10 +305,10 @@ void tile_space(const bld_handle* h, Space& s, bool is_adv) {
 
 size_t smem_y(int P2, int NL, bool fp32) { return (size_t)(P2 + 2 * P2 * NL) * csize(fp32); }
 // per-term y kernels with `lines` lines: twiddles and two line buffers for the
-// block-wide stages, or twiddles and one buffer on a line stride of lines + 1
-// for the warp transforms
+// block-wide stages, or twiddles and one buffer of P2 + 32 (swizzled) positions
+// on a line stride of lines + 1 for the warp transforms
 size_t smem_y_term(int P2, int lines, int wfft, bool fp32) {
-    return (size_t)(wfft ? P2 + P2 * (lines + 1) : P2 + 2 * P2 * lines) * csize(fp32);
+    return (size_t)(wfft ? P2 + (P2 + 32) * (lines + 1) : P2 + 2 * P2 * lines) * csize(fp32);
 }
 size_t smem_adv(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 3 * s.YT * s.P1) * csize(fp32); }
 size_t smem_sgs(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 5 * s.YT * s.P1) * csize(fp32); }
@@ -503,7 +503,7 @@ int launch_adv_xb(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     const int r = xb_radix(s.P1);
     dim3 grid(s.P2, s.nchunks, nm);
     if (s.xb == 2) {
-        const size_t smp = ((size_t)r * 32 + 5 * (size_t)s.P1 + 12 * (size_t)h->g.K1) * csize(sizeof(R) == 4);
+        const size_t smp = ((size_t)r * 32 + 5 * (size_t)(s.P1 + 32) + 12 * (size_t)h->g.K1) * csize(sizeof(R) == 4);
         switch (r) {
             case 2: k_adv_xp<R, 2><<<grid, 160, smp, h->stream>>>(a); break;
             case 3: k_adv_xp<R, 3><<<grid, 160, smp, h->stream>>>(a); break;
@@ -517,7 +517,7 @@ int launch_adv_xb(bld_handle* h, const Space& s, const XArgs& a, int nm) {
         CUDA_TRY(cudaGetLastError());
         return BLD_OK;
     }
-    const size_t sm = ((size_t)r * 32 + 3 * (size_t)s.P1 + 12 * (size_t)h->g.K1) * csize(sizeof(R) == 4);
+    const size_t sm = ((size_t)r * 32 + 3 * (size_t)(s.P1 + 32) + 12 * (size_t)h->g.K1) * csize(sizeof(R) == 4);
     switch (r) {
         case 2: k_adv_xb<R, 2><<<grid, 96, sm, h->stream>>>(a); break;
         case 3: k_adv_xb<R, 3><<<grid, 96, sm, h->stream>>>(a); break;

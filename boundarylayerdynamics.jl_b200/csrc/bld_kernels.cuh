@@ -138,7 +138,7 @@ __device__ __forceinline__ double2 inv_term_value(const InvYArgs& a, const doubl
 // grid (ceil(K1/NL), n3, nterms*members); smem: tw[P2] + 2*P2*NL complex
 // Gather of one term's K2 x NL modes into the line buffer with the term kind
 // fixed at compile time (the loads of a batch are straight-line code).
-template <typename R, int OP>
+template <typename R, int OP, int RAD>
 __device__ __forceinline__ void gather_term(const InvYArgs& a, const double2* __restrict__ S, int f, int z, int k10,
                                             int nls, int LS, cplx<R>* b0) {
     const int NL = a.NL, K1 = a.g.K1, K2 = a.g.K2, k2max = a.g.k2max, P2 = a.P2;
@@ -161,7 +161,7 @@ __device__ __forceinline__ void gather_term(const InvYArgs& a, const double2* __
             if (i < nmodes) {
                 const int j = i >> nls, l = i & (NL - 1);
                 const int p = (j <= k2max) ? j : P2 - (K2 - j);
-                b0[p * LS + l] = mk<R>((R)v[q].x, (R)v[q].y);
+                b0[swz<cplx<R>, RAD>(p) * LS + l] = mk<R>((R)v[q].x, (R)v[q].y);
             }
         }
     }
@@ -196,15 +196,15 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
     // zero the padding band, then gather the K2*NL modes in batches of 8 per thread
     for (int i = threadIdx.x; i < (P2 - K2) * NL; i += blockDim.x) {
         const int p = k2max + 1 + (i >> nls), l = i & (NL - 1);
-        b0[p * LS + l] = mk<R>(0, 0);
+        b0[swz<C, RAD>(p) * LS + l] = mk<R>(0, 0);
     }
     switch (op) {
-        case T_DIRECT: gather_term<R, T_DIRECT>(a, S, f, z, k10, nls, LS, b0); break;
-        case T_D1: gather_term<R, T_D1>(a, S, f, z, k10, nls, LS, b0); break;
-        case T_D2: gather_term<R, T_D2>(a, S, f, z, k10, nls, LS, b0); break;
-        case T_VORT1: gather_term<R, T_VORT1>(a, S, f, z, k10, nls, LS, b0); break;
-        case T_VORT2: gather_term<R, T_VORT2>(a, S, f, z, k10, nls, LS, b0); break;
-        default: gather_term<R, T_VORT3>(a, S, f, z, k10, nls, LS, b0); break;
+        case T_DIRECT: gather_term<R, T_DIRECT, RAD>(a, S, f, z, k10, nls, LS, b0); break;
+        case T_D1: gather_term<R, T_D1, RAD>(a, S, f, z, k10, nls, LS, b0); break;
+        case T_D2: gather_term<R, T_D2, RAD>(a, S, f, z, k10, nls, LS, b0); break;
+        case T_VORT1: gather_term<R, T_VORT1, RAD>(a, S, f, z, k10, nls, LS, b0); break;
+        case T_VORT2: gather_term<R, T_VORT2, RAD>(a, S, f, z, k10, nls, LS, b0); break;
+        default: gather_term<R, T_VORT3, RAD>(a, S, f, z, k10, nls, LS, b0); break;
     }
     __syncthreads();
     C* res = b0;
@@ -216,10 +216,10 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
         for (int l = threadIdx.x >> 5; l < NL; l += nw) {
             C zl[RAD];
 #pragma unroll
-            for (int q = 0; q < RAD; ++q) zl[q] = b0[(lane + 32 * q) * LS + l];
+            for (int q = 0; q < RAD; ++q) zl[q] = b0[swz<C, RAD>(lane + 32 * q) * LS + l];
             inverse_line<R, RAD>(zl, lane, tw + lane, 32, lt);
 #pragma unroll
-            for (int k = 0; k < RAD; ++k) b0[(k + RAD * brl) * LS + l] = zl[k];
+            for (int k = 0; k < RAD; ++k) b0[swz<C, RAD>(k + RAD * brl) * LS + l] = zl[k];
         }
         __syncthreads();
     } else {
@@ -234,7 +234,8 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
             for (int i = threadIdx.x; i < P2 * half; i += blockDim.x) {
                 const int y = i >> (nls - 1), l = 2 * (i & (half - 1)), k1 = k10 + l;
                 if (k1 < K1) {
-                    const C v0 = res[y * LS + l], v1 = res[y * LS + l + 1];
+                    const int ry = swz<C, RAD>(y) * LS;
+                    const C v0 = res[ry + l], v1 = res[ry + l + 1];
                     *reinterpret_cast<float4*>(out + (long long)y * K1 + k1) = make_float4(v0.x, v0.y, v1.x, v1.y);
                 }
             }
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(256) k_inv_y(InvYArgs a) {
     }
     for (int i = threadIdx.x; i < P2 * NL; i += blockDim.x) {
         const int y = i >> nls, l = i & (NL - 1), k1 = k10 + l;
-        if (k1 < K1) out[(long long)y * K1 + k1] = res[y * LS + l];
+        if (k1 < K1) out[(long long)y * K1 + k1] = res[swz<C, RAD>(y) * LS + l];
     }
 }
 
@@ -1060,7 +1061,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
                 const int i = i0 + q * blockDim.x + threadIdx.x;
                 if (i < nval) {
                     const int y = i >> nlsl, l = i & (nlines - 1);
-                    b0[y * LS + l] = v[q];
+                    b0[swz<C, RAD>(y) * LS + l] = v[q];
                 }
             }
         }
@@ -1094,7 +1095,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
                 const int i = i0 + q * blockDim.x + threadIdx.x;
                 if (i < nval) {
                     const int y = i >> nlsl, l = i & (nlines - 1);
-                    b0[y * LS + l] = v[q];
+                    b0[swz<C, RAD>(y) * LS + l] = v[q];
                 }
             }
         }
@@ -1131,7 +1132,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
             const int i = i0 + q * blockDim.x + threadIdx.x;
             if (i < nval) {
                 const int y = i >> nlsl, l = i & (nlines - 1);
-                b0[y * LS + l] = v[q];
+                b0[swz<C, RAD>(y) * LS + l] = v[q];
             }
         }
     }
@@ -1145,10 +1146,10 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
         for (int l = threadIdx.x >> 5; l < nlines; l += nw) {
             C zl[RAD];
 #pragma unroll
-            for (int k = 0; k < RAD; ++k) zl[k] = b0[(k + RAD * brl) * LS + l];
+            for (int k = 0; k < RAD; ++k) zl[k] = b0[swz<C, RAD>(k + RAD * brl) * LS + l];
             forward_line<R, RAD>(zl, lane, tw + lane, 32, lt);
 #pragma unroll
-            for (int b = 0; b < RAD; ++b) b0[(lane + 32 * b) * LS + l] = zl[b];
+            for (int b = 0; b < RAD; ++b) b0[swz<C, RAD>(lane + 32 * b) * LS + l] = zl[b];
         }
         __syncthreads();
     } else {
@@ -1196,7 +1197,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
                 const int o = o0 + q * blockDim.x + threadIdx.x;
                 const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
                 if (o >= nout || k1 >= K1) continue;
-                const int pos = (j <= k2max) ? j : P2 - (K2 - j);
+                const int pos = swz<C, RAD>((j <= k2max) ? j : P2 - (K2 - j));
                 const C X = res[pos * LS + l];
                 double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
                 if (hasB) {

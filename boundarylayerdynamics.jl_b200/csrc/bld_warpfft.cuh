@@ -183,6 +183,25 @@ __device__ __forceinline__ cplx<R> mirror_mode(const cplx<R> (&z)[RAD], int lane
 }
 
 
+// Shared-memory buffers that hold lines in physical order after a warp
+// transform (lane l holds points k + RAD brev5(l)) store point p at position
+// swz(p) = p + (p / RAD) >> SH, on a padded extent P + 32.  Without it the lanes
+// of one shared-memory wavefront (8 lanes for 16-byte complex values, 16 for
+// 8-byte ones) land in the same banks, up to 8-way for even RAD; the pad adds the
+// bits of brev5(l) that RAD brev5(l) does not spread over the banks, and
+// consecutive points stay consecutive between pads.
+__host__ __device__ constexpr int ctz_c(int v) { return (v & 1) ? 0 : 1 + ctz_c(v >> 1); }
+template <typename C, int RAD>
+__device__ __forceinline__ int swz(int p) {
+    if constexpr (RAD == 0) {
+        return p;
+    } else {
+        constexpr int a = ctz_c(RAD) < 3 ? ctz_c(RAD) : 3;
+        constexpr int SH = sizeof(C) == 16 ? ((RAD & 1) ? 3 : 2) : 4 - a;
+        return p + ((p / RAD) >> SH);
+    }
+}
+
 __device__ __forceinline__ int brev5(int lane) { return (int)(__brev((unsigned)lane) >> 27); }
 
 // In-place transforms of `nlines` contiguous lines of P = 32 RAD points in shared

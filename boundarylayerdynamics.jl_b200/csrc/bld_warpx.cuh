@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(128, MINB) k_adv_xwc(XArgs a) { adv_xw_body<R,
 // stages, and only one line in registers per thread, so the FP64 form fits.
 // The six input rows of layer j+1 are staged with cp.async while layer j runs.
 // grid (P2, nchunks, members), block 96; dynamic smem: W_P^{-l k} [RAD][32],
-// lines [3][P1], staging [2][6][K1] (complex).
+// lines [3][P1 + 32], staging [2][6][K1] (complex).
 template <typename R, int RAD>
 __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
     using C = cplx<R>;
@@ -176,7 +176,8 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
     C* twl_all = reinterpret_cast<C*>(smem_raw);
     const int P1 = a.P1, n3 = a.g.n3, k1max = a.g.k1max, K1 = a.g.K1;
     C* L = twl_all + RAD * 32;            // [3][P1]
-    C* stage = L + 3 * P1;                // [2][6][K1]
+    const int LP = P1 + 32;               // padded line stride (see swz)
+    C* stage = L + 3 * LP;                // [2][6][K1]
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int m = a.m0 + blockIdx.z;
     BLD_SKIP_INACTIVE(a, m);
@@ -228,7 +229,7 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
             load_packed<R, RAD>(zl, ra, rb, lane, P1, k1max);
             inverse_line<R, RAD>(zl, lane, twl, 32, lt);
 #pragma unroll
-            for (int k = 0; k < RAD; ++k) L[wib * P1 + k + RAD * brl] = zl[k];
+            for (int k = 0; k < RAD; ++k) L[wib * LP + swz<C, RAD>(k + RAD * brl)] = zl[k];
         }
         __syncthreads();
         // ---- products at the thread's points; outputs overwrite L[0] and L[1]
@@ -238,8 +239,9 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
         for (int i = 0; i < PPT; ++i) {
             const int x = threadIdx.x + 96 * i;
             if (x < P1) {
-                const C c0 = L[x], c1 = L[P1 + x];
-                const C c2 = hasI ? L[2 * P1 + x] : mk<R>(R(0), R(0));
+                const int xs = swz<C, RAD>(x);
+                const C c0 = L[xs], c1 = L[LP + xs];
+                const C c2 = hasI ? L[2 * LP + xs] : mk<R>(R(0), R(0));
                 const R u = c0.x, v = c0.y, o3 = c1.x;
                 const R w = hasI ? c1.y : R(0);
                 const R q1 = c2.x, q2 = c2.y;
@@ -256,8 +258,8 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
                 }
                 // adv3 on I layer j-1 (:206)
                 const R adv3 = po2[i] * R(0.5) * (pu[i] + u) - po1[i] * R(0.5) * (pv[i] + v);
-                L[x] = mk<R>(adv1, adv2);
-                L[P1 + x] = mk<R>(adv3, R(0));
+                L[xs] = mk<R>(adv1, adv2);
+                L[LP + xs] = mk<R>(adv3, R(0));
                 pu[i] = u;
                 pv[i] = v;
                 pw[i] = w;
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
         if (wib < 2 && (wib == 0 ? emitC : emitI)) {
             C zl[RAD];
 #pragma unroll
-            for (int k = 0; k < RAD; ++k) zl[k] = L[wib * P1 + k + RAD * brl];
+            for (int k = 0; k < RAD; ++k) zl[k] = L[wib * LP + swz<C, RAD>(k + RAD * brl)];
             forward_line<R, RAD>(zl, lane, twl, 32, lt);
             C* rA = mrow_w(Mout, a, wib == 0 ? 0 : 2, wib == 0 ? j : j - 1, y);
             C* rB = mrow_w(Mout, a, 1, j, y);
@@ -298,7 +300,7 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
 // are requested (cp.async) at the top of iteration j and waited for before the
 // barrier that ends the products.
 // grid (P2, nchunks, members), block 160; dynamic smem: W_P^{-l k} [RAD][32],
-// inverse lines L [3][P1], product lines F [2][P1], staging [2][6][K1] (complex).
+// inverse lines L [3][P1 + 32], product lines F [2][P1 + 32], staging [2][6][K1] (complex).
 template <typename R, int RAD>
 __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
     using C = cplx<R>;
@@ -308,8 +310,9 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
     C* twl_all = reinterpret_cast<C*>(smem_raw);
     const int P1 = a.P1, n3 = a.g.n3, k1max = a.g.k1max, K1 = a.g.K1;
     C* L = twl_all + RAD * 32;            // [3][P1]
-    C* F = L + 3 * P1;                    // [2][P1]
-    C* stage = F + 2 * P1;                // [2][6][K1]
+    const int LP = P1 + 32;               // padded line stride (see swz)
+    C* F = L + 3 * LP;                    // [2][LP]
+    C* stage = F + 2 * LP;                // [2][6][K1]
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int m = a.m0 + blockIdx.z;
     BLD_SKIP_INACTIVE(a, m);
@@ -363,7 +366,7 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
                 load_packed<R, RAD>(zl, ra, rb, lane, P1, k1max);
                 inverse_line<R, RAD>(zl, lane, twl, 32, lt);
 #pragma unroll
-                for (int k = 0; k < RAD; ++k) L[wib * P1 + k + RAD * brl] = zl[k];
+                for (int k = 0; k < RAD; ++k) L[wib * LP + swz<C, RAD>(k + RAD * brl)] = zl[k];
             }
         } else {
             // ---- forward of layer lj = j - 1: warp 3 (adv1, adv2) on C layer lj,
@@ -373,7 +376,7 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
             if (emit) {
                 C zl[RAD];
 #pragma unroll
-                for (int k = 0; k < RAD; ++k) zl[k] = F[fw * P1 + k + RAD * brl];
+                for (int k = 0; k < RAD; ++k) zl[k] = F[fw * LP + swz<C, RAD>(k + RAD * brl)];
                 forward_line<R, RAD>(zl, lane, twl, 32, lt);
                 C* rA = mrow_w(Mout, a, fw == 0 ? 0 : 2, fw == 0 ? lj : lj - 1, y);
                 C* rB = mrow_w(Mout, a, 1, lj, y);
@@ -397,8 +400,9 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
             for (int i = 0; i < PPT; ++i) {
                 const int x = threadIdx.x + NT * i;
                 if (x < P1) {
-                    const C c0 = L[x], c1 = L[P1 + x];
-                    const C c2 = hasI ? L[2 * P1 + x] : mk<R>(R(0), R(0));
+                    const int xs = swz<C, RAD>(x);
+                    const C c0 = L[xs], c1 = L[LP + xs];
+                    const C c2 = hasI ? L[2 * LP + xs] : mk<R>(R(0), R(0));
                     const R u = c0.x, v = c0.y, o3 = c1.x;
                     const R w = hasI ? c1.y : R(0);
                     const R q1 = c2.x, q2 = c2.y;
@@ -415,8 +419,8 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
                     }
                     // adv3 on I layer j-1 (:206)
                     const R adv3 = po2[i] * R(0.5) * (pu[i] + u) - po1[i] * R(0.5) * (pv[i] + v);
-                    F[x] = mk<R>(adv1, adv2);
-                    F[P1 + x] = mk<R>(adv3, R(0));
+                    F[xs] = mk<R>(adv1, adv2);
+                    F[LP + xs] = mk<R>(adv3, R(0));
                     pu[i] = u;
                     pv[i] = v;
                     pw[i] = w;
