@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
     const int z1 = min(n3, z0 + a.zchunk);
     const int nthr = blockDim.x;
     const C* twg = reinterpret_cast<const C*>(a.tw);
-    copy_table(tw, twg, P1);
+    lane_table<RAD>(tw, twg, P1);
     const C* Min = reinterpret_cast<const C*>(a.min) + (long long)m * a.min_mstride;
     C* Mout = reinterpret_cast<C*>(a.mout) + (long long)m * a.mout_mstride;
 
@@ -495,11 +495,11 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
         __syncthreads();
         C* phys = bufA;
         if constexpr (RAD > 0) {
-            warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw);
+            warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw, twg);
             __syncthreads();
         } else {
             if constexpr (RAD > 0) {
-                warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw);
+                warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw, twg);
                 __syncthreads();
             } else {
                 phys = fft_big<R, +1>(bufA, bufB, NLin, P1, 1, true, a.plan, tw);
@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
             __syncthreads();
             C* r2 = outb;
             if constexpr (RAD > 0) {
-                warp_lines_inplace<R, RAD, -1>(outb, NLout, P1, tw);
+                warp_lines_inplace<R, RAD, -1>(outb, NLout, P1, tw, twg);
                 __syncthreads();
             } else {
                 r2 = fft_big<R, -1>(outb, phys, NLout, P1, 1, true, a.plan, tw);
@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
     const int z1 = min(n3, z0 + a.zchunk);
     const int nthr = blockDim.x;
     const C* twg = reinterpret_cast<const C*>(a.tw);
-    copy_table(tw, twg, P1);
+    lane_table<RAD>(tw, twg, P1);
     const C* Min = reinterpret_cast<const C*>(a.min) + (long long)m * a.min_mstride;
     C* Mout = reinterpret_cast<C*>(a.mout) + (long long)m * a.mout_mstride;
     const double* lcm = a.lc + (long long)m * n3;
@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
             }
             __syncthreads();
             if constexpr (RAD > 0) {
-                warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw);
+                warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw, twg);
                 __syncthreads();
             } else {
                 phys = fft_big<R, +1>(bufA, bufB, NLin, P1, 1, true, a.plan, tw);
@@ -788,7 +788,7 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
             __syncthreads();
             C* r2 = outb;
             if constexpr (RAD > 0) {
-                warp_lines_inplace<R, RAD, -1>(outb, NLout, P1, tw);
+                warp_lines_inplace<R, RAD, -1>(outb, NLout, P1, tw, twg);
                 __syncthreads();
             } else {
                 r2 = fft_big<R, -1>(outb, phys, NLout, P1, 1, true, a.plan, tw);
