@@ -5,6 +5,7 @@ csrc/).  It links the CUDA runtime statically, so the only run-time
 dependency is the NVIDIA driver.
 """
 
+import glob
 import os
 import shutil
 import subprocess
@@ -15,7 +16,7 @@ REPO = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libbld.so")
 SOURCES = [os.path.join(HERE, "csrc", "bld_capi.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("bld_fft.cuh", "bld_kernels.cuh")] + [
+DEPS = SOURCES + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [
     os.path.join(REPO, "include", "bld.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
