@@ -1136,6 +1136,14 @@ bool stage_fusable(const bld_handle* h) {
     return !last.fwd.all;
 }
 
+// steps of one call may be chained (BLD_NO_STEP_CHAIN=1 keeps every step whole)
+bool chain_ok(const bld_handle* h, int method) {
+    if (method != BLD_SSPRK33 && method != BLD_SSPRK22) return false;
+    const char* e = getenv("BLD_NO_STEP_CHAIN");
+    if (e && e[0] && e[0] != '0') return false;
+    return stage_fusable(h);
+}
+
 int enqueue_rates(bld_handle* h, const double2* state, double2* du, int m0, int nm) {
     return enqueue_rates_impl(h, state, du, m0, nm);
 }
@@ -1196,7 +1204,25 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
 }
 
 // one time step of `method` (perform_step! + the trailing rate!, src/ODEMethods.jl:217-234)
-int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first) {
+// the right-hand side of the new state at the end of a step: f(u) into du, or
+// (CHAIN_LEAVE) the next step's first stage value u + dt f(u) into t
+int enqueue_trailing_rates(bld_handle* h, double dt, int chain) {
+    if (chain & 2) {
+        const StageFuse sf{nullptr, h->t, 0.0, 1.0, dt, 1.0};
+        return enqueue_rates_impl(h, h->u, h->du, 0, h->B, &sf);
+    }
+    return enqueue_rates(h, h->u, h->du, 0, h->B);
+}
+
+// chain (SSPRK22 / SSPRK33 with the stage update fused, steps inside one
+// multi-step call): CHAIN_ENTER = the step starts from t = u + dt f(u) formed by
+// the previous step's trailing forward pass, so its first stage is a plain
+// projection of t in place; CHAIN_LEAVE = the trailing right-hand side writes
+// t = u + dt f(u) for the next step instead of f(u).  The last step of a call
+// never leaves, so du holds f(u) between calls.
+enum { CHAIN_ENTER = 1, CHAIN_LEAVE = 2 };
+
+int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first, int chain = 0) {
     const int B = h->B;
     struct MaskScope {
         bld_handle* h;
@@ -1209,7 +1235,10 @@ int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first) {
             BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
             break;
         case BLD_SSPRK22:
-            BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->t, 0, B));
+            if (chain & CHAIN_ENTER)
+                BLD_TRY(enqueue_project(h, S_NONE, dt, h->t, nullptr, nullptr, nullptr, h->t, 0, B));
+            else
+                BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->t, 0, B));
             if (stage_fusable(h)) {
                 // u <- (u + t + dt f(t)) / 2 in the forward y pass (u is read and
                 // written element by element; the pass reads t), then project u
@@ -1220,10 +1249,13 @@ int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first) {
                 BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
                 BLD_TRY(enqueue_project(h, S_RK22_2, dt, h->u, h->t, h->du, nullptr, h->u, 0, B));
             }
-            BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
+            BLD_TRY(enqueue_trailing_rates(h, dt, chain));
             break;
         case BLD_SSPRK33:
-            BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->t, 0, B));
+            if (chain & CHAIN_ENTER)
+                BLD_TRY(enqueue_project(h, S_NONE, dt, h->t, nullptr, nullptr, nullptr, h->t, 0, B));
+            else
+                BLD_TRY(enqueue_project(h, S_EULER, dt, h->u, nullptr, h->du, nullptr, h->t, 0, B));
             if (stage_fusable(h)) {
                 // second stage into du (free once the first stage consumed it; the
                 // pass reads t, so the stage value cannot overwrite t in place)
@@ -1242,7 +1274,7 @@ int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first) {
                 BLD_TRY(enqueue_rates(h, h->t, h->du, 0, B));
                 BLD_TRY(enqueue_project(h, S_RK33_3, dt, h->u, h->t, h->du, nullptr, h->u, 0, B));
             }
-            BLD_TRY(enqueue_rates(h, h->u, h->du, 0, B));
+            BLD_TRY(enqueue_trailing_rates(h, dt, chain));
             break;
         case BLD_AB2: {
             const size_t bytes = (size_t)B * h->g.mstride * sizeof(double2);
@@ -1792,12 +1824,12 @@ static int enqueue_profile_sample(bld_handle* h, double w) {
 
 // captures one step of `method` (regular steps; AB2 after its start-up step) into
 // a CUDA graph, kept as source graph and instantiated executable
-static int step_graph(bld_handle* h, int method, double dt) {
-    const auto key = std::make_pair(gkey(h, method), dt);
+static int step_graph(bld_handle* h, int method, double dt, int chain = 0) {
+    const auto key = std::make_pair(gkey(h, method) + 32 * chain, dt);
     if (h->graphs.count(key)) return BLD_OK;
     cudaGraph_t graph;
     CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int st = enqueue_step(h, method, dt, false);
+    int st = enqueue_step(h, method, dt, false, chain);
     if (st == BLD_OK && h->prof_on) {
         h->mask_on = true;
         st = enqueue_profile_sample(h, 0.5 * dt);
@@ -1852,13 +1884,32 @@ static int step_impl(bld_handle* h, int64_t nsteps, double dt, int32_t method) {
         }
     }
     if (done < nsteps) {
-        const auto key = std::make_pair(gkey(h, method), dt);
-        auto it = h->graphs.find(key);
-        if (it == h->graphs.end()) {
-            BLD_TRY(step_graph(h, method, dt));
-            it = h->graphs.find(key);
+        // chained steps: the first leaves the next step's first stage value in t,
+        // the middle ones enter and leave, the last one enters and ends with f(u)
+        const bool chain = nsteps - done >= 2 && chain_ok(h, method);
+        auto graph_for = [&](int c, cudaGraphExec_t* g) -> int {
+            const auto key = std::make_pair(gkey(h, method) + 32 * c, dt);
+            auto it = h->graphs.find(key);
+            if (it == h->graphs.end()) {
+                BLD_TRY(step_graph(h, method, dt, c));
+                it = h->graphs.find(key);
+            }
+            *g = it->second;
+            return BLD_OK;
+        };
+        if (!chain) {
+            cudaGraphExec_t g;
+            BLD_TRY(graph_for(0, &g));
+            for (; done < nsteps; ++done) CUDA_TRY(cudaGraphLaunch(g, h->stream));
+        } else {
+            cudaGraphExec_t gfirst, gmid, glast;
+            BLD_TRY(graph_for(CHAIN_LEAVE, &gfirst));
+            BLD_TRY(graph_for(CHAIN_ENTER | CHAIN_LEAVE, &gmid));
+            BLD_TRY(graph_for(CHAIN_ENTER, &glast));
+            const int64_t last = nsteps - 1;
+            for (; done < nsteps; ++done)
+                CUDA_TRY(cudaGraphLaunch(done == 0 ? gfirst : (done == last ? glast : gmid), h->stream));
         }
-        for (; done < nsteps; ++done) CUDA_TRY(cudaGraphLaunch(it->second, h->stream));
     }
     return BLD_OK;
 }

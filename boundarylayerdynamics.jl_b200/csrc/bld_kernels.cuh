@@ -854,7 +854,8 @@ struct FwdYArgs {
     // fused stage update (k_fwd_y, modes 0 and 1): instead of the rate d, write
     // sout = (st_cu su + st_ct state + st_cd d) / st_div, the explicit
     // SSP-RK stage value that the projection would otherwise form from d
-    // (src/ODEMethods.jl:143,157,164); su and sout have the member stride of du
+    // (src/ODEMethods.jl:101,143,157,164); su (NULL: no su term, st_ct = st_div = 1)
+    // and sout have the member stride of du
     int fuse;
     const double2* su;
     double2* sout;
@@ -1166,11 +1167,13 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     // the epilogue with the mode and the window loads fixed at compile time, so
     // that the loads of OB outputs are straight-line code
     double2* so = a.fuse ? a.sout + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F : nullptr;
-    const double2* su = a.fuse ? a.su + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F : nullptr;
+    const double2* su = (a.fuse && a.su) ? a.su + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F : nullptr;
     auto epilogue = [&](auto mode_c, auto win_c, auto fuse_c) {
         constexpr int MODE = decltype(mode_c)::value;
         constexpr bool WIN = decltype(win_c)::value;
-        constexpr bool FUSE = decltype(fuse_c)::value;
+        // 0: the rate; 1: (cu su + ct state + cd rate) / div; 2: state + cd rate
+        constexpr int FZ = decltype(fuse_c)::value;
+        constexpr bool FUSE = FZ != 0;
         for (int o0 = 0; o0 < nout; o0 += OB * blockDim.x) {
             double2 W[OB][3];
             double2 old[OB], U[OB], T[OB];
@@ -1186,10 +1189,8 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
                             if (r < wn) W[q][r] = Sf[(long long)(w0 + r) * g.F + idx];
                     }
                     if constexpr (MODE == 0) old[q] = du[idx];
-                    if constexpr (FUSE) {
-                        U[q] = su[idx];
-                        if constexpr (!WIN) T[q] = Sf[(long long)z * g.F + idx];
-                    }
+                    if constexpr (FZ == 1) U[q] = su[idx];
+                    if constexpr (FUSE && !WIN) T[q] = Sf[(long long)z * g.F + idx];
                 }
             }
 #pragma unroll
@@ -1229,9 +1230,13 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
                     } else {
                         tz = T[q];
                     }
-                    const double2 uz = U[q];
-                    so[idx] = make_double2((a.st_cu * uz.x + a.st_ct * tz.x + a.st_cd * v.x) / a.st_div,
-                                           (a.st_cu * uz.y + a.st_ct * tz.y + a.st_cd * v.y) / a.st_div);
+                    if constexpr (FZ == 1) {
+                        const double2 uz = U[q];
+                        so[idx] = make_double2((a.st_cu * uz.x + a.st_ct * tz.x + a.st_cd * v.x) / a.st_div,
+                                               (a.st_cu * uz.y + a.st_ct * tz.y + a.st_cd * v.y) / a.st_div);
+                    } else {   // Euler stage: state + dt rate (src/ODEMethods.jl:101)
+                        so[idx] = make_double2(tz.x + a.st_cd * v.x, tz.y + a.st_cd * v.y);
+                    }
                 } else {
                     du[idx] = v;
                 }
@@ -1244,20 +1249,27 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     using I2 = std::integral_constant<int, 2>;
     using BT = std::integral_constant<bool, true>;
     using BF = std::integral_constant<bool, false>;
-    if (a.fuse && a.mode == 1 && need_win)
-        epilogue(I1{}, BT{}, BT{});
-    else if (a.fuse && a.mode == 1)
-        epilogue(I1{}, BF{}, BT{});
-    else if (a.fuse && a.mode == 0)
-        epilogue(I0{}, BF{}, BT{});
+    const int fz = a.fuse ? (a.su ? 1 : 2) : 0;
+    if (fz == 1 && a.mode == 1 && need_win)
+        epilogue(I1{}, BT{}, I1{});
+    else if (fz == 1 && a.mode == 1)
+        epilogue(I1{}, BF{}, I1{});
+    else if (fz == 1 && a.mode == 0)
+        epilogue(I0{}, BF{}, I1{});
+    else if (fz == 2 && a.mode == 1 && need_win)
+        epilogue(I1{}, BT{}, I2{});
+    else if (fz == 2 && a.mode == 1)
+        epilogue(I1{}, BF{}, I2{});
+    else if (fz == 2 && a.mode == 0)
+        epilogue(I0{}, BF{}, I2{});
     else if (a.mode == 1 && need_win)
-        epilogue(I1{}, BT{}, BF{});
+        epilogue(I1{}, BT{}, I0{});
     else if (a.mode == 1)
-        epilogue(I1{}, BF{}, BF{});
+        epilogue(I1{}, BF{}, I0{});
     else if (a.mode == 0)
-        epilogue(I0{}, BF{}, BF{});
+        epilogue(I0{}, BF{}, I0{});
     else
-        epilogue(I2{}, BF{}, BF{});
+        epilogue(I2{}, BF{}, I0{});
     if (a.check && bad) atomicOr(a.flag + m, 1);
 }
 

@@ -173,22 +173,30 @@ def test_trajectory_parity(oracle, BLD, method):
 @pytest.mark.parametrize("method", ["SSPRK33", "SSPRK22"])
 @pytest.mark.parametrize("case", ["dns_16x16x8", "les_16x16x8", "stretched_dns", "les_24x18x7_nodamp"])
 def test_stage_fusion_matches_unfused(oracle, BLD, case, method):
-    """The SSP-RK stage update formed in the forward y pass (default) against the
-    same steps with the update in the projection (BLD_NO_STAGE_FUSION=1), and
-    both against the oracle: 20 steps, 1e-12 between the two engine paths."""
+    """The SSP-RK stage update formed in the forward y pass, with the steps of one
+    call chained (the trailing right-hand side forms the next step's Euler stage),
+    against the same 20 steps with the update in the projection
+    (BLD_NO_STAGE_FUSION=1) and against one step per call (no chaining): 1e-12
+    between the engine paths, and the oracle's trajectory tolerance."""
     import os
     res, dom, procs = CASES[case]
     om = oracle.Model(res, dom(oracle), procs(oracle))
     st = _random_state(om, seed=len(case), scale=2.0)
     om.apply_projections(st)
+    meth = getattr(BLD, method)
     runs = []
-    for off in ("0", "1"):
+    for off, per_call in (("0", 20), ("1", 20), ("0", 1)):
         old = os.environ.get("BLD_NO_STAGE_FUSION")
         os.environ["BLD_NO_STAGE_FUSION"] = off
         try:
             gm = BLD.Model(res, dom(BLD), procs(BLD))
             gm.set_state(st)
-            gm.evolve(20 * 1e-3, 1e-3, method=getattr(BLD, method))
+            if per_call == 20:
+                gm.evolve(20 * 1e-3, 1e-3, method=meth)
+            else:
+                gm.evolve(1e-3, 1e-3, method=meth)
+                for _ in range(19):
+                    gm.step(1, 1e-3, meth)
             runs.append(gm.state)
         finally:
             if old is None:
@@ -198,7 +206,8 @@ def test_stage_fusion_matches_unfused(oracle, BLD, case, method):
     om.state.update({f: v.copy() for f, v in st.items()})
     om.evolve(20 * 1e-3, 1e-3, method=getattr(oracle, method))
     for f in om.fields:
-        assert rel_l2(runs[0][f], runs[1][f]) < 1e-12, (f, rel_l2(runs[0][f], runs[1][f]))
+        for r in runs[1:]:
+            assert rel_l2(runs[0][f], r[f]) < 1e-12, (f, rel_l2(runs[0][f], r[f]))
         assert rel_l2(runs[0][f], om.state[f]) < TRAJ_TOL, (f, rel_l2(runs[0][f], om.state[f]))
 
 
