@@ -310,8 +310,14 @@ size_t smem_y(int P2, int NL, bool fp32) { return (size_t)(P2 + 2 * P2 * NL) * c
 size_t smem_y_term(int P2, int lines, int wfft, bool fp32) {
     return (size_t)(wfft ? P2 + (P2 + 32) * (lines + 1) : P2 + 2 * P2 * lines) * csize(fp32);
 }
-size_t smem_adv(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 3 * s.YT * s.P1) * csize(fp32); }
-size_t smem_sgs(const Space& s, bool fp32) { return (size_t)(s.P1 + 2 * 5 * s.YT * s.P1) * csize(fp32); }
+// block x kernels: twiddles and two buffers of (3 or 5) YT lines, on a line stride
+// P1 + 32 (swizzled positions) with warp line transforms (xr > 0)
+size_t smem_adv(const Space& s, bool fp32) {
+    return (size_t)(s.P1 + 2 * 3 * s.YT * (s.P1 + (s.xr ? 32 : 0))) * csize(fp32);
+}
+size_t smem_sgs(const Space& s, bool fp32) {
+    return (size_t)(s.P1 + 2 * 5 * s.YT * (s.P1 + (s.xr ? 32 : 0))) * csize(fp32);
+}
 
 // ------------------------------------------------------------------ kernel dispatch
 // threads for an in-place transform of `lines` lines (one task per thread for
@@ -976,7 +982,7 @@ int autotune(bld_handle* h) {
         const int xrr = s.P1 % 32 ? 0 : s.P1 / 32;
         if (xr_radix_ok(xrr) && !(sp == 0 && (only_warp || only_bw)) && !only_block && !xdisable_wlines()) {
             for (int yt = 1; yt <= 2; ++yt) {
-                const size_t smx = (size_t)(s.P1 + 2 * (sp == 0 ? 3 : 5) * yt * s.P1) * csize(h->fp32);
+                const size_t smx = (size_t)(s.P1 + 2 * (sp == 0 ? 3 : 5) * yt * (s.P1 + 32)) * csize(h->fp32);
                 if (s.P2 % yt || smx > 150 * 1024 || yt * s.P1 / xr_ppt(xrr) > 256) continue;
                 s.xr = xrr;
                 s.YT = yt;

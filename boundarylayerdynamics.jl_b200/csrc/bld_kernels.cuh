@@ -406,21 +406,24 @@ __device__ __forceinline__ void build_packed(cplx<R>* line, const cplx<R>* rowA,
     }
 }
 
-template <typename R>
+// RAD > 0: the line is stored on swizzled positions (swz, bld_warpfft.cuh)
+template <typename R, int RAD = 0>
 __device__ __forceinline__ void put_packed(cplx<R>* line, cplx<R> A, cplx<R> B, int k, int P1) {
+    using C = cplx<R>;
     if (k == 0) {
         line[0] = mk<R>(A.x, B.x);
     } else {
-        line[k] = mk<R>(A.x - B.y, A.y + B.x);
-        line[P1 - k] = mk<R>(A.x + B.y, -A.y + B.x);
+        line[swz<C, RAD>(k)] = mk<R>(A.x - B.y, A.y + B.x);
+        line[swz<C, RAD>(P1 - k)] = mk<R>(A.x + B.y, -A.y + B.x);
     }
 }
 
 // Unpack forward FFT Z of a + ib: A[k] = (Z[k] + conj(Z[-k]))/2, B[k] = (Z[k] - conj(Z[-k]))/(2i)
-template <typename R>
+template <typename R, int RAD = 0>
 __device__ __forceinline__ void unpack_pair(const cplx<R>* line, int k, int P1, cplx<R>& A, cplx<R>& B) {
-    const cplx<R> Zk = line[k];
-    const cplx<R> Zr = line[k == 0 ? 0 : P1 - k];
+    using C = cplx<R>;
+    const cplx<R> Zk = line[swz<C, RAD>(k)];
+    const cplx<R> Zr = line[swz<C, RAD>(k == 0 ? 0 : P1 - k)];
     A = mk<R>((Zk.x + Zr.x) * R(0.5), (Zk.y - Zr.y) * R(0.5));
     const R dx = Zk.x - Zr.x, dy = Zk.y + Zr.y;
     B = mk<R>(dy * R(0.5), -dx * R(0.5));
@@ -437,10 +440,12 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P1 = a.P1, YT = a.YT, n3 = a.g.n3, k1max = a.g.k1max;
     const int NLin = 3 * YT, NLout = YT + (YT + 1) / 2;
-    // two line buffers of NLin lines: inputs/physical values and outputs ping-pong between them
+    // two line buffers of NLin lines: inputs/physical values and outputs ping-pong
+    // between them; RAD > 0: swizzled positions on a line stride P1 + 32
+    const int LP = RAD ? P1 + 32 : P1;
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* bufA = tw + P1;
-    C* bufB = bufA + NLin * P1;
+    C* bufB = bufA + NLin * LP;
     const int y0 = blockIdx.x * YT;
     const int m = a.m0 + blockIdx.z;
     BLD_SKIP_INACTIVE(a, m);
@@ -464,7 +469,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
         const int nk = k1max + 1;
         for (int i = threadIdx.x; i < NLin * (P1 - 2 * k1max - 1); i += nthr) {
             const int line = i / (P1 - 2 * k1max - 1), k = k1max + 1 + i % (P1 - 2 * k1max - 1);
-            cur[line * P1 + k] = mk<R>(0, 0);
+            cur[line * LP + swz<C, RAD>(k)] = mk<R>(0, 0);
         }
         for (int i0 = 0; i0 < NLin * nk; i0 += 4 * nthr) {
             C va[4], vb[4];
@@ -488,7 +493,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
                 const int i = i0 + q * nthr + threadIdx.x;
                 if (i < NLin * nk) {
                     const int line = i / nk, k = i - line * nk;
-                    put_packed<R>(cur + line * P1, va[q], vb[q], k, P1);
+                    put_packed<R, RAD>(cur + line * LP, va[q], vb[q], k, P1);
                 }
             }
         }
@@ -512,9 +517,10 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
         for (int i = 0; i < PPT; ++i) {
             const int p = threadIdx.x + i * nthr;
             const int yl = p / P1, x = p - yl * P1;
-            const C c0 = phys[(yl * 3 + 0) * P1 + x];
-            const C c1 = phys[(yl * 3 + 1) * P1 + x];
-            const C c2 = phys[(yl * 3 + 2) * P1 + x];
+            const int xs = swz<C, RAD>(x);
+            const C c0 = phys[(yl * 3 + 0) * LP + xs];
+            const C c1 = phys[(yl * 3 + 1) * LP + xs];
+            const C c2 = phys[(yl * 3 + 2) * LP + xs];
             const R u = c0.x, v = c0.y, o3 = c1.x;
             const R w = hasI ? c1.y : R(0);
             const R o1 = hasI ? c2.x : R(0);
@@ -531,11 +537,11 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
                     adv1 = o3 * v - R(0.5) * (po2[i] * pw[i] + o2 * w);
                     adv2 = R(0.5) * (po1[i] * pw[i] + o1 * w) - o3 * u;
                 }
-                outb[yl * P1 + x] = mk<R>(adv1, adv2);
+                outb[yl * LP + xs] = mk<R>(adv1, adv2);
             }
             if (emitI) {  // adv3 on I layer j-1 (:206)
                 const R adv3 = po2[i] * R(0.5) * (pu[i] + u) - po1[i] * R(0.5) * (pv[i] + v);
-                C* o = outb + (YT + yl / 2) * P1 + x;
+                C* o = outb + (YT + yl / 2) * LP + xs;
                 if (yl & 1) {
                     o->y = adv3;
                 } else {
@@ -562,7 +568,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
             for (int i = threadIdx.x; i < NLout * nk; i += nthr) {
                 const int line = i / nk, k = i - line * nk;
                 C A, B;
-                unpack_pair<R>(r2 + line * P1, k, P1, A, B);
+                unpack_pair<R, RAD>(r2 + line * LP, k, P1, A, B);
                 if (line < YT) {
                     const int y = y0 + line;
                     mrow_w(Mout, a, 0, j, y)[k] = A;
@@ -595,9 +601,10 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P1 = a.P1, YT = a.YT, n3 = a.g.n3, k1max = a.g.k1max;
     const int NLin = 5 * YT, NLout = 4 * YT;
+    const int LP = RAD ? P1 + 32 : P1;   // RAD > 0: swizzled positions on a padded line stride
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* bufA = tw + P1;
-    C* bufB = bufA + NLin * P1;
+    C* bufB = bufA + NLin * LP;
     const int y0 = blockIdx.x * YT;
     const int m = a.m0 + blockIdx.z;
     BLD_SKIP_INACTIVE(a, m);
@@ -633,7 +640,7 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
             const int nk = k1max + 1;
             for (int i = threadIdx.x; i < NLin * (P1 - 2 * k1max - 1); i += nthr) {
                 const int line = i / (P1 - 2 * k1max - 1), k = k1max + 1 + i % (P1 - 2 * k1max - 1);
-                cur[line * P1 + k] = mk<R>(0, 0);
+                cur[line * LP + swz<C, RAD>(k)] = mk<R>(0, 0);
             }
             for (int i0 = 0; i0 < NLin * nk; i0 += 4 * nthr) {
                 C va[4], vb[4];
@@ -657,7 +664,7 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
                     const int i = i0 + q * nthr + threadIdx.x;
                     if (i < NLin * nk) {
                         const int line = i / nk, k = i - line * nk;
-                        put_packed<R>(cur + line * P1, va[q], vb[q], k, P1);
+                        put_packed<R, RAD>(cur + line * LP, va[q], vb[q], k, P1);
                     }
                 }
             }
@@ -679,12 +686,13 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
             const int p = threadIdx.x + i * nthr;
             const int yl = p / P1, x = p - yl * P1;
             R u = 0, v = 0, u1 = 0, u2 = 0, v1 = 0, v2 = 0, w = whi, w1 = 0, w2 = 0;
+            const int xs = swz<C, RAD>(x);
             if (hasC) {
-                const C c0 = phys[(yl * 5 + 0) * P1 + x], c1 = phys[(yl * 5 + 1) * P1 + x];
-                const C c2 = phys[(yl * 5 + 2) * P1 + x];
+                const C c0 = phys[(yl * 5 + 0) * LP + xs], c1 = phys[(yl * 5 + 1) * LP + xs];
+                const C c2 = phys[(yl * 5 + 2) * LP + xs];
                 u = c0.x; v = c0.y; u1 = c1.x; u2 = c1.y; v1 = c2.x; v2 = c2.y;
                 if (hasI) {
-                    const C c3 = phys[(yl * 5 + 3) * P1 + x], c4 = phys[(yl * 5 + 4) * P1 + x];
+                    const C c3 = phys[(yl * 5 + 3) * LP + xs], c4 = phys[(yl * 5 + 4) * LP + xs];
                     w = c3.x; w1 = c3.y; w2 = c4.x;
                 }
             }
@@ -769,7 +777,7 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
             }
             if (doC || do5) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) outb[(yl * 4 + q) * P1 + x] = mk<R>(o[2 * q], o[2 * q + 1]);
+                for (int q = 0; q < 4; ++q) outb[(yl * 4 + q) * LP + xs] = mk<R>(o[2 * q], o[2 * q + 1]);
             }
             // (d) carry
             if (j >= 1 && j <= n3 - 1) {
@@ -798,7 +806,7 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
                 const int line = i / nk, k = i - line * nk;
                 const int yl = line / 4, q = line - yl * 4, y = y0 + yl;
                 C A, B;
-                unpack_pair<R>(r2 + line * P1, k, P1, A, B);
+                unpack_pair<R, RAD>(r2 + line * LP, k, P1, A, B);
                 // pairs (0,1) (2,3) (4,5) (6,7)
                 const int ta = 2 * q, tb = 2 * q + 1;
                 if (ta <= 4) {

@@ -204,11 +204,12 @@ __device__ __forceinline__ int swz(int p) {
 
 __device__ __forceinline__ int brev5(int lane) { return (int)(__brev((unsigned)lane) >> 27); }
 
-// In-place transforms of `nlines` contiguous lines of P = 32 RAD points in shared
-// memory, natural order in and out, one line per warp at a time (the block-wide
-// Stockham stages replaced by register work).  `tw` is the lane-major [RAD][32]
-// table W_P^(-l k) in shared memory, `twg` the [P] table W_P^(-m) in global memory.
-// The caller synchronises the block before and after.
+// In-place transforms of `nlines` lines of P = 32 RAD points in shared memory,
+// natural order in and out, one line per warp at a time (the block-wide Stockham
+// stages replaced by register work).  Line l starts at lines + l (P + 32) and
+// holds point p at swz(p).  `tw` is the lane-major [RAD][32] table W_P^(-l k) in
+// shared memory, `twg` the [P] table W_P^(-m) in global memory.  The caller
+// synchronises the block before and after.
 template <typename R, int RAD, int DIR>
 __device__ __forceinline__ void warp_lines_inplace(cplx<R>* lines, int nlines, int P, const cplx<R>* __restrict__ tw,
                                                    const cplx<R>* __restrict__ twg) {
@@ -217,20 +218,21 @@ __device__ __forceinline__ void warp_lines_inplace(cplx<R>* lines, int nlines, i
     LaneTw<R> lt;
     lane_twiddles_tab<R>(lt, lane, twg, P);
     for (int l = threadIdx.x >> 5; l < nlines; l += nw) {
-        cplx<R>* L = lines + (size_t)l * P;
-        cplx<R> z[RAD];
+        using C = cplx<R>;
+        C* L = lines + (size_t)l * (P + 32);
+        C z[RAD];
         if constexpr (DIR > 0) {
 #pragma unroll
-            for (int m = 0; m < RAD; ++m) z[m] = L[lane + 32 * m];
+            for (int m = 0; m < RAD; ++m) z[m] = L[swz<C, RAD>(lane + 32 * m)];
             inverse_line<R, RAD>(z, lane, tw + lane, 32, lt);
 #pragma unroll
-            for (int k = 0; k < RAD; ++k) L[k + RAD * brl] = z[k];
+            for (int k = 0; k < RAD; ++k) L[swz<C, RAD>(k + RAD * brl)] = z[k];
         } else {
 #pragma unroll
-            for (int k = 0; k < RAD; ++k) z[k] = L[k + RAD * brl];
+            for (int k = 0; k < RAD; ++k) z[k] = L[swz<C, RAD>(k + RAD * brl)];
             forward_line<R, RAD>(z, lane, tw + lane, 32, lt);
 #pragma unroll
-            for (int b = 0; b < RAD; ++b) L[lane + 32 * b] = z[b];
+            for (int b = 0; b < RAD; ++b) L[swz<C, RAD>(lane + 32 * b)] = z[b];
         }
     }
 }
