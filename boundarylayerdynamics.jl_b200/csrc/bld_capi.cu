@@ -498,15 +498,18 @@ int launch_adv_xw(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     return BLD_OK;
 }
 
-int xb_radix(int P1) {
+// radix of the block-of-warps x kernels for P1 = 32 * radix (16 and 24 in single
+// precision only: one line of 24 FP64 complex values per lane would spill), or 0
+int xb_radix(int P1, bool fp32) {
     if (P1 % 32) return 0;
     const int r = P1 / 32;
+    if (fp32 && (r == 16 || r == 24)) return r;
     return (r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 9 || r == 12) ? r : 0;
 }
 
 template <typename R>
 int launch_adv_xb(bld_handle* h, const Space& s, const XArgs& a, int nm) {
-    const int r = xb_radix(s.P1);
+    const int r = xb_radix(s.P1, sizeof(R) == 4);
     dim3 grid(s.P2, s.nchunks, nm);
     if (s.xb == 2) {
         const size_t smp = ((size_t)r * 32 + 5 * (size_t)(s.P1 + 32) + 12 * (size_t)h->g.K1) * csize(sizeof(R) == 4);
@@ -518,7 +521,12 @@ int launch_adv_xb(bld_handle* h, const Space& s, const XArgs& a, int nm) {
             case 8: k_adv_xp<R, 8><<<grid, 160, smp, h->stream>>>(a); break;
             case 9: k_adv_xp<R, 9><<<grid, 160, smp, h->stream>>>(a); break;
             case 12: k_adv_xp<R, 12><<<grid, 160, smp, h->stream>>>(a); break;
-            default: return fail(BLD_ERR_INVALID_CONFIG, "no pipelined block-of-warps x kernel for P1=%d", s.P1);
+            default:
+                if constexpr (sizeof(R) == 4) {
+                    if (r == 16) { k_adv_xp<R, 16><<<grid, 160, smp, h->stream>>>(a); break; }
+                    if (r == 24) { k_adv_xp<R, 24><<<grid, 160, smp, h->stream>>>(a); break; }
+                }
+                return fail(BLD_ERR_INVALID_CONFIG, "no pipelined block-of-warps x kernel for P1=%d", s.P1);
         }
         CUDA_TRY(cudaGetLastError());
         return BLD_OK;
@@ -532,7 +540,12 @@ int launch_adv_xb(bld_handle* h, const Space& s, const XArgs& a, int nm) {
         case 8: k_adv_xb<R, 8><<<grid, 96, sm, h->stream>>>(a); break;
         case 9: k_adv_xb<R, 9><<<grid, 96, sm, h->stream>>>(a); break;
         case 12: k_adv_xb<R, 12><<<grid, 96, sm, h->stream>>>(a); break;
-        default: return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", s.P1);
+        default:
+            if constexpr (sizeof(R) == 4) {
+                if (r == 16) { k_adv_xb<R, 16><<<grid, 96, sm, h->stream>>>(a); break; }
+                if (r == 24) { k_adv_xb<R, 24><<<grid, 96, sm, h->stream>>>(a); break; }
+            }
+            return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", s.P1);
     }
     CUDA_TRY(cudaGetLastError());
     return BLD_OK;
@@ -626,6 +639,12 @@ int set_smem_limits_R() {
     BLD_SET((k_adv_xp<R, 8>));
     BLD_SET((k_adv_xp<R, 9>));
     BLD_SET((k_adv_xp<R, 12>));
+    if constexpr (sizeof(R) == 4) {
+        BLD_SET((k_adv_xb<R, 16>));
+        BLD_SET((k_adv_xb<R, 24>));
+        BLD_SET((k_adv_xp<R, 16>));
+        BLD_SET((k_adv_xp<R, 24>));
+    }
     BLD_SET((k_adv_xw<R, 2>));
     BLD_SET((k_adv_xw<R, 3>));
     BLD_SET((k_adv_xw<R, 4>));
@@ -931,7 +950,7 @@ int autotune(bld_handle* h) {
     const bool only_bw3 = xk && !strcmp(xk, "blockwarp"), only_pipe = xk && !strcmp(xk, "pipe");
     const bool only_bw = only_bw3 || only_pipe;   // a block-of-warps kernel (three warps, or five pipelined)
     const bool only_lines = xk && !strcmp(xk, "lines");   // block kernels with warp line transforms
-    const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1) > 0;
+    const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1, h->fp32) > 0;
     if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
     const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
     if (only_warp && !adv_warp_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no warp x kernel for P1=%d", h->adv.P1);

@@ -76,6 +76,8 @@ CASES = [
     ((192, 8, 5), "mixed", 1e-5),
     ((256, 6, 4), "mixed", 1e-5),
     ((171, 6, 4), "mixed", 1e-5),       # k1max = 85: P1 = 256, radix 8
+    ((341, 4, 4), "mixed", 1e-5),       # k1max = 170: P1 = 512, radix 16
+    ((512, 4, 4), "mixed", 1e-5),       # k1max = 255: P1 = 768, radix 24
 ]
 
 
@@ -84,6 +86,8 @@ CASES = [
 def test_advection_x_kernel_family(oracle, BLD, res, precision, tol, family):
     if family == "warp" and precision == "fp64" and res[0] == 192:
         pytest.skip("the warp-per-row kernel is compiled for radix <= 6 in FP64 (P1 = 288 is radix 9)")
+    if family == "warp" and res[0] in (341, 512):
+        pytest.skip("the warp-per-row kernel is compiled for radix <= 12 (P1 = 512, 768 are radix 16, 24)")
     om = _build(oracle, res)
     gm = _forced(BLD, family, res, precision)
     if family != "block":
