@@ -123,7 +123,10 @@ struct YCfg {
 };
 
 // radices of the warp y transforms compiled for the per-term y kernels
-bool wfft_radix_ok(int r) { return r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 9 || r == 12 || r == 16; }
+// (24 in single precision only)
+bool wfft_radix_ok(int r, bool fp32) {
+    return r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 9 || r == 12 || r == 16 || (fp32 && r == 24);
+}
 
 struct Space {
     bool on = false;
@@ -363,6 +366,12 @@ int launch_inv_y(bld_handle* h, const Space& s, InvYArgs a, int nm) {
             case 9: k_inv_y<R, 9><<<grid, c.thr, sm, h->stream>>>(a); break;
             case 12: k_inv_y<R, 12><<<grid, c.thr, sm, h->stream>>>(a); break;
             case 16: k_inv_y<R, 16><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 24:
+                if constexpr (sizeof(R) == 4) {
+                    k_inv_y<R, 24><<<grid, c.thr, sm, h->stream>>>(a);
+                    break;
+                }
+                return fail(BLD_ERR_INVALID_CONFIG, "no warp y transform of radix %d", c.wfft);
             default: return fail(BLD_ERR_INVALID_CONFIG, "no warp y transform of radix %d", c.wfft);
         }
     }
@@ -391,6 +400,12 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
             case 9: k_fwd_y<R, 9><<<grid, c.thr, sm, h->stream>>>(a); break;
             case 12: k_fwd_y<R, 12><<<grid, c.thr, sm, h->stream>>>(a); break;
             case 16: k_fwd_y<R, 16><<<grid, c.thr, sm, h->stream>>>(a); break;
+            case 24:
+                if constexpr (sizeof(R) == 4) {
+                    k_fwd_y<R, 24><<<grid, c.thr, sm, h->stream>>>(a);
+                    break;
+                }
+                return fail(BLD_ERR_INVALID_CONFIG, "no warp y transform of radix %d", c.wfft);
             default: return fail(BLD_ERR_INVALID_CONFIG, "no warp y transform of radix %d", c.wfft);
         }
     }
@@ -602,6 +617,10 @@ int set_smem_limits_R() {
     BLD_SET((k_fwd_y<R, 12>));
     BLD_SET((k_inv_y<R, 16>));
     BLD_SET((k_fwd_y<R, 16>));
+    if constexpr (sizeof(R) == 4) {
+        BLD_SET((k_inv_y<R, 24>));
+        BLD_SET((k_fwd_y<R, 24>));
+    }
     BLD_SET((k_inv_y_all<R>));
     BLD_SET((k_fwd_y_all<R>));
     BLD_SET((k_adv_x<R, 1, 0>));
@@ -897,7 +916,7 @@ std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_pe
     const int nls_pt[4] = {h->fp32 ? 4 : 2, h->fp32 ? 8 : 4, h->fp32 ? 16 : 8, h->fp32 ? 32 : 16};
     for (int nl : nls_pt) {
         const int wr = s.P2 % 32 ? 0 : s.P2 / 32;
-        if (wfft_radix_ok(wr) && !ydisable_warp() && smem_y_term(s.P2, lines_per_nl * nl, wr, h->fp32) <= 150 * 1024) {
+        if (wfft_radix_ok(wr, h->fp32) && !ydisable_warp() && smem_y_term(s.P2, lines_per_nl * nl, wr, h->fp32) <= 150 * 1024) {
             out.push_back(YCfg{0, nl, 128, wr});
             out.push_back(YCfg{0, nl, 256, wr});
         }
@@ -906,7 +925,7 @@ std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_pe
         for (int i = 0; i < 3; ++i) {
             bool dup = false;
             for (int k = 0; k < i; ++k) dup |= thrs[k] == thrs[i];
-            const bool warp_possible = wfft_radix_ok(s.P2 % 32 ? 0 : s.P2 / 32);
+            const bool warp_possible = wfft_radix_ok(s.P2 % 32 ? 0 : s.P2 / 32, h->fp32);
             if (!dup && !(yforce_warp() && warp_possible)) out.push_back(YCfg{0, nl, thrs[i], 0});
         }
     }

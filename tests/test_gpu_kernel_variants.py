@@ -159,7 +159,7 @@ def _forced_y(BLD, family, res, precision, les):
             os.environ["BLD_Y_KERNEL"] = old
 
 
-# y-pass sizes P2 = 96 (3), 288 (9), 384 (12), 64 (2), 192 (6), 128 (4), 256 (8), 512 (16)
+# y-pass sizes P2 = 96 (3), 288 (9), 384 (12), 64 (2), 192 (6), 128 (4), 256 (8), 512 (16), 768 (24)
 Y_CASES = [
     ((16, 64, 6), "fp64", False, 1e-12),
     ((16, 192, 5), "fp64", False, 1e-12),
@@ -169,6 +169,7 @@ Y_CASES = [
     ((16, 128, 6), "mixed", True, 1e-5),
     ((12, 256, 4), "fp64", True, 1e-12),
     ((8, 512, 4), "fp64", True, 1e-12),
+    ((8, 512, 4), "mixed", False, 1e-5),    # advection P2 = 768: radix 24 (single precision)
 ]
 
 
