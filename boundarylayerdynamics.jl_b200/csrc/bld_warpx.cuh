@@ -207,9 +207,12 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
         }
     };
 
-    R pu[PPT], pv[PPT], pw[PPT], po1[PPT], po2[PPT];
+    R pu[PPT], pv[PPT], pw[PPT], po1[PPT], po2[PPT], pa3[PPT];
 #pragma unroll
-    for (int i = 0; i < PPT; ++i) pu[i] = pv[i] = pw[i] = po1[i] = po2[i] = R(0);
+    for (int i = 0; i < PPT; ++i) pu[i] = pv[i] = pw[i] = po1[i] = po2[i] = pa3[i] = R(0);
+    // adv3 lines of consecutive I layers are forward-transformed in pairs
+    // (adv3(i - 1) + i adv3(i)): the chunk emits I layers first_e..last_e
+    const int first_e = max(z0, 1) - 1, last_e = z1 - 2;
 
     const int jb = max(0, z0 - 1);
     issue(jb, stage);
@@ -235,6 +238,9 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
         // ---- products at the thread's points; outputs overwrite L[0] and L[1]
         const bool emitC = (j >= z0);
         const bool emitI = (j >= z0) && (j >= 1);
+        const int i3 = j - 1;                                  // I layer of this layer's adv3
+        const bool odd3 = ((i3 - first_e) & 1) != 0;           // second of a pair
+        const bool single3 = !odd3 && i3 == last_e;            // unpaired last one
 #pragma unroll
         for (int i = 0; i < PPT; ++i) {
             const int x = threadIdx.x + 96 * i;
@@ -259,7 +265,11 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
                 // adv3 on I layer j-1 (:206)
                 const R adv3 = po2[i] * R(0.5) * (pu[i] + u) - po1[i] * R(0.5) * (pv[i] + v);
                 L[xs] = mk<R>(adv1, adv2);
-                L[LP + xs] = mk<R>(adv3, R(0));
+                if (emitI) {
+                    if (odd3) L[LP + xs] = mk<R>(pa3[i], adv3);
+                    else if (single3) L[LP + xs] = mk<R>(adv3, R(0));
+                    pa3[i] = adv3;
+                }
                 pu[i] = u;
                 pv[i] = v;
                 pw[i] = w;
@@ -268,14 +278,16 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
             }
         }
         __syncthreads();
-        // ---- forward: warp 0 (adv1, adv2) on C layer j, warp 1 (adv3, 0) on I layer j-1
-        if (wib < 2 && (wib == 0 ? emitC : emitI)) {
+        // ---- forward: warp 0 (adv1, adv2) on C layer j; warp 1 (adv3(j - 2), adv3(j - 1))
+        // of I layers j - 2, j - 1 once a pair is complete, or the unpaired last one
+        if (wib < 2 && (wib == 0 ? emitC : (emitI && (odd3 || single3)))) {
             C zl[RAD];
 #pragma unroll
             for (int k = 0; k < RAD; ++k) zl[k] = L[wib * LP + swz<C, RAD>(k + RAD * brl)];
             forward_line<R, RAD>(zl, lane, twl, 32, lt);
-            C* rA = mrow_w(Mout, a, wib == 0 ? 0 : 2, wib == 0 ? j : j - 1, y);
-            C* rB = mrow_w(Mout, a, 1, j, y);
+            const bool two = wib == 0 || odd3;
+            C* rA = mrow_w(Mout, a, wib == 0 ? 0 : 2, wib == 0 ? j : (odd3 ? i3 - 1 : i3), y);
+            C* rB = mrow_w(Mout, a, wib == 0 ? 1 : 2, wib == 0 ? j : i3, y);
 #pragma unroll
             for (int b = 0; b < RAD; ++b) {
                 if (b >= nb) break;
@@ -284,7 +296,7 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
                 const C Zr = mirror_mode<R, RAD>(zl, lane, b);
                 if (f <= k1max) {
                     rA[f] = mk<R>((Zk.x + Zr.x) * R(0.5), (Zk.y - Zr.y) * R(0.5));
-                    if (wib == 0) rB[f] = mk<R>((Zk.y + Zr.y) * R(0.5), -(Zk.x - Zr.x) * R(0.5));
+                    if (two) rB[f] = mk<R>((Zk.y + Zr.y) * R(0.5), -(Zk.x - Zr.x) * R(0.5));
                 }
             }
         }
