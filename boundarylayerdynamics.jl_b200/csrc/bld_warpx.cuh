@@ -354,9 +354,12 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
         }
     };
 
-    R pu[PPT], pv[PPT], pw[PPT], po1[PPT], po2[PPT];
+    R pu[PPT], pv[PPT], pw[PPT], po1[PPT], po2[PPT], pa3[PPT];
 #pragma unroll
-    for (int i = 0; i < PPT; ++i) pu[i] = pv[i] = pw[i] = po1[i] = po2[i] = R(0);
+    for (int i = 0; i < PPT; ++i) pu[i] = pv[i] = pw[i] = po1[i] = po2[i] = pa3[i] = R(0);
+    // adv3 lines of consecutive I layers are forward-transformed in pairs (as in
+    // k_adv_xb): the chunk emits I layers first_e..last_e
+    const int first_e = max(z0, 1) - 1, last_e = z1 - 2;
 
     const int jb = max(0, z0 - 1);
     issue(jb, stage);
@@ -384,14 +387,17 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
             // ---- forward of layer lj = j - 1: warp 3 (adv1, adv2) on C layer lj,
             // warp 4 (adv3, 0) on I layer lj - 1
             const int lj = j - 1, fw = wib - 3;
-            const bool emit = lj >= jb && lj >= z0 && (fw == 0 || lj >= 1);
+            const int i3 = lj - 1;                                   // I layer of lj's adv3
+            const bool odd3 = ((i3 - first_e) & 1) != 0, single3 = !odd3 && i3 == last_e;
+            const bool emit = lj >= jb && lj >= z0 && (fw == 0 || (lj >= 1 && (odd3 || single3)));
             if (emit) {
                 C zl[RAD];
 #pragma unroll
                 for (int k = 0; k < RAD; ++k) zl[k] = F[fw * LP + swz<C, RAD>(k + RAD * brl)];
                 forward_line<R, RAD>(zl, lane, twl, 32, lt);
-                C* rA = mrow_w(Mout, a, fw == 0 ? 0 : 2, fw == 0 ? lj : lj - 1, y);
-                C* rB = mrow_w(Mout, a, 1, lj, y);
+                const bool two = fw == 0 || odd3;
+                C* rA = mrow_w(Mout, a, fw == 0 ? 0 : 2, fw == 0 ? lj : (odd3 ? i3 - 1 : i3), y);
+                C* rB = mrow_w(Mout, a, fw == 0 ? 1 : 2, fw == 0 ? lj : i3, y);
 #pragma unroll
                 for (int b = 0; b < RAD; ++b) {
                     if (b >= nb) break;
@@ -400,7 +406,7 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
                     const C Zr = mirror_mode<R, RAD>(zl, lane, b);
                     if (f <= k1max) {
                         rA[f] = mk<R>((Zk.x + Zr.x) * R(0.5), (Zk.y - Zr.y) * R(0.5));
-                        if (fw == 0) rB[f] = mk<R>((Zk.y + Zr.y) * R(0.5), -(Zk.x - Zr.x) * R(0.5));
+                        if (two) rB[f] = mk<R>((Zk.y + Zr.y) * R(0.5), -(Zk.x - Zr.x) * R(0.5));
                     }
                 }
             }
@@ -432,7 +438,12 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
                     // adv3 on I layer j-1 (:206)
                     const R adv3 = po2[i] * R(0.5) * (pu[i] + u) - po1[i] * R(0.5) * (pv[i] + v);
                     F[xs] = mk<R>(adv1, adv2);
-                    F[LP + xs] = mk<R>(adv3, R(0));
+                    if (j >= z0 && j >= 1) {   // adv3 of I layer j - 1 is emitted
+                        const bool odd = ((j - 1 - first_e) & 1) != 0;
+                        if (odd) F[LP + xs] = mk<R>(pa3[i], adv3);
+                        else if (j - 1 == last_e) F[LP + xs] = mk<R>(adv3, R(0));
+                        pa3[i] = adv3;
+                    }
                     pu[i] = u;
                     pv[i] = v;
                     pw[i] = w;
