@@ -33,7 +33,7 @@ METRIC = "grid-pt updates/s (plain FP64 vs mixed) @192^2x96"
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the x-pass
 # kernel the autotuner picks at 192^2x96, from one ncu capture of a step
 # (profiles/step_kernels_dns192_fp64.md, profiles/step_kernels_dns192_mixed.md)
-TRAFFIC = {("dns192", "k_adv_xb<double, 9>"): (258.8 + 95.85) * 1e6,
+TRAFFIC = {("dns192", "k_adv_xb<double, 9>"): (258.7 + 94.14) * 1e6,
            ("dns192", "k_adv_xp<double, 9>"): (255.0 + 97.5) * 1e6,
            ("dns192", "k_adv_xwc<float, 9, 3>"): (133.4 + 33.06) * 1e6,
            ("dns192", "k_adv_xw<float, 9>"): (130.8 + 36.81) * 1e6}
