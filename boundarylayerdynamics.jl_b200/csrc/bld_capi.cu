@@ -1248,16 +1248,6 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
 }
 
 // one time step of `method` (perform_step! + the trailing rate!, src/ODEMethods.jl:217-234)
-// the right-hand side of the new state at the end of a step: f(u) into du, or
-// (CHAIN_LEAVE) the next step's first stage value u + dt f(u) into t
-int enqueue_trailing_rates(bld_handle* h, double dt, int chain) {
-    if (chain & 2) {
-        const StageFuse sf{nullptr, h->t, 0.0, 1.0, dt, 1.0};
-        return enqueue_rates_impl(h, h->u, h->du, 0, h->B, &sf);
-    }
-    return enqueue_rates(h, h->u, h->du, 0, h->B);
-}
-
 // chain (SSPRK22 / SSPRK33 with the stage update fused, steps inside one
 // multi-step call): CHAIN_ENTER = the step starts from t = u + dt f(u) formed by
 // the previous step's trailing forward pass, so its first stage is a plain
@@ -1265,6 +1255,16 @@ int enqueue_trailing_rates(bld_handle* h, double dt, int chain) {
 // t = u + dt f(u) for the next step instead of f(u).  The last step of a call
 // never leaves, so du holds f(u) between calls.
 enum { CHAIN_ENTER = 1, CHAIN_LEAVE = 2 };
+
+// the right-hand side of the new state at the end of a step: f(u) into du, or
+// (CHAIN_LEAVE) the next step's first stage value u + dt f(u) into t
+int enqueue_trailing_rates(bld_handle* h, double dt, int chain) {
+    if (chain & CHAIN_LEAVE) {
+        const StageFuse sf{nullptr, h->t, 0.0, 1.0, dt, 1.0};
+        return enqueue_rates_impl(h, h->u, h->du, 0, h->B, &sf);
+    }
+    return enqueue_rates(h, h->u, h->du, 0, h->B);
+}
 
 int enqueue_step(bld_handle* h, int method, double dt, bool ab2_first, int chain = 0) {
     const int B = h->B;
