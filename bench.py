@@ -37,7 +37,14 @@ TRAFFIC = {("dns192", "k_adv_xb<double, 9>"): (258.7 + 94.14) * 1e6,
            ("dns192", "k_adv_xp<double, 9>"): (255.0 + 97.5) * 1e6,
            ("dns192", "k_adv_xwc<float, 9, 3>"): (133.4 + 33.06) * 1e6,
            ("dns192", "k_adv_xw<float, 9>"): (130.8 + 36.81) * 1e6}
+TRAFFIC_SOURCE = "ncu capture of one step in profiles/ (a fixed figure, not measured in this run)"
 UNIT = "grid-pt updates/s"
+# the workload both arms report under "config" (identical dicts); how the engine
+# runs it goes under "config_notes"
+CONFIG = {"workload": "closed-channel DNS 192x192x96, 4pi x 2pi x 2, nu=1/180, SSPRK33 dt=1e-4"}
+# seconds of the same step loop run untimed before and after the timed steps,
+# inside the clock-sampling window (nvidia-smi samples every 200 ms)
+CLOCK_WINDOW_S = 2.5
 
 
 def parse():
@@ -72,7 +79,8 @@ def dist_env():
 
 # ------------------------------------------------------------------- clock sampling
 class Clocks:
-    """Samples nvidia-smi every 200 ms on one GPU while the timed region runs."""
+    """Samples nvidia-smi every 200 ms on one GPU over a window that holds the
+    timed steps and CLOCK_WINDOW_S seconds of the same step loop on either side."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -114,7 +122,8 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(self.rows),
+                "window": f"the timed steps plus {CLOCK_WINDOW_S} s of the same step loop before and after"}
 
 
 def peaks():
@@ -190,16 +199,27 @@ def run_b200(args):
         sp = ctypes.c_void_p()
         _capi.check(lib.bld_get_stream(m._h, ctypes.byref(sp)))
         stream = torch.cuda.ExternalStream(sp.value)
+        # warm-up steps, timed only to size the untimed roll before and after the timed steps
+        w0e, w1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0e.record(stream)
         m.step(W, dt)
+        w1e.record(stream)
+        w1e.synchronize()
+        roll = max(1, int(CLOCK_WINDOW_S * 1e3 / max(w0e.elapsed_time(w1e) / W, 1e-3)))
         pt = _capi.BldPhaseTimes()
-        barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # the clock sampler covers the timed steps and the same step loop before
+        # and after them, so that it sees the load for several seconds
         with Clocks(local) as clk:
+            m.step(roll, dt)
+            barrier()
             e0.record(stream)
             _capi.check(lib.bld_step_async(m._h, K, dt, _capi.SSPRK33))
             e1.record(stream)
             e1.synchronize()
-        m.sync()
+            m.sync()
+            m.step(roll, dt)
+            m.sync()
         ms = max_over_ranks(e0.elapsed_time(e1))
         barrier()
         _capi.check(lib.bld_time_phases(m._h, 20, _capi.SSPRK33, ctypes.byref(pt)))
@@ -261,38 +281,44 @@ def run_b200(args):
     fp, mx = res["fp64"], res["mixed"]
     value = ws * npts / (fp["ms_per_step"] / 1e3)
     peak, peak_kind = peaks()
-    # dominant kernel of the FP64 form by time share per step
     lps = fp["launches_per_step"]
     ph = fp["phases"]
-    counts = {"inv_y": 3, "adv_x": 3, "fwd_y": 3, "project": 3}
-    share = {k: ph[k] * counts[k] for k in ph}
-    dom = max(share, key=share.get)
-    pb = phase_bytes(m, "fp64")
-    ach = pb[dom] / (ph[dom] * 1e-3) / 1e9
-    names = {"inv_y": "inv_y", "adv_x": "x", "fwd_y": "fwd_y"}
+    names ={"inv_y": "inv_y", "adv_x": "x", "fwd_y": "fwd_y"}
 
     def kname(kern, phase):
         return kern["projection"] if phase == "project" else kern["advection"][names[phase]]
 
     def roofline(prec, phases):
+        """The dominant kernel against the HBM roofline.  `achieved` divides the
+        algorithmic bytes of one SSP-RK stage, B_alg / 3 = 8 S / 3 (the stage reads
+        its input and u^n and writes its output; S = the FP64 state), by one launch
+        of that kernel (one launch per stage): the fraction of the step's
+        compulsory traffic this kernel would need at the device's peak.  The
+        kernel's own input and output bytes (intermediates included) divided by
+        the same time are kept as `own_bytes_*`."""
         share = {k: phases[k] for k in phases}
         d = max(share, key=share.get)
-        b = phase_bytes(models[prec][0], prec)[d]
-        a = b / (phases[d] * 1e-3) / 1e9
+        mm = models[prec][0]
+        b_alg = 8 * state_bytes(mm) / 3
+        own = phase_bytes(mm, prec)[d]
+        t = phases[d] * 1e-3
+        a = b_alg / t / 1e9
         kn = kname(res[prec]["kernels"], d)
         tr = TRAFFIC.get((args.config, kn))
         return {"bound": "hbm", "kernel": kn, "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
-                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b, "avg_launch_ms": phases[d],
-                "traffic": tr}
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b_alg, "avg_launch_ms": phases[d],
+                "own_bytes_per_launch": own, "own_bytes_achieved": own / t / 1e9,
+                "own_bytes_frac": own / t / 1e9 / peak,
+                "traffic": tr, "traffic_source": (TRAFFIC_SOURCE if tr is not None else None)}
     step_ach = 8 * sbytes / (fp["ms_per_step"] * 1e-3) / 1e9
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
         "ms_per_step": fp["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded laminar profile + Gaussian noise)",
-        "config": {"workload": "closed-channel DNS 192x192x96, 4pi x 2pi x 2, nu=1/180, SSPRK33 dt=1e-4",
-                   "padding": f"{m.info.adv_p1}x{m.info.adv_p2} (reference {m.info.adv_ref_p1}x{m.info.adv_ref_p2})",
-                   "l2": "working set (~0.5 GB per step) larger than the 126 MB L2; no flush",
-                   "parallelism": f"replicas x{ws}"},
+        "config": dict(CONFIG),
+        "config_notes": {"padding": f"{m.info.adv_p1}x{m.info.adv_p2} (reference {m.info.adv_ref_p1}x{m.info.adv_ref_p2})",
+                         "l2": "working set (~0.5 GB per step) larger than the 126 MB L2; no flush",
+                         "parallelism": f"replicas x{ws}"},
         "mixed": {"value": ws * npts / (mx["ms_per_step"] / 1e3), "ms_per_step": mx["ms_per_step"],
                   "speedup_vs_fp64": fp["ms_per_step"] / mx["ms_per_step"], "dtype": "f32 transforms/products, f64 state+pressure",
                   "error_vs_fp64": err, "clocks": mx["clocks"]},
@@ -547,7 +573,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "steps_timed": nk, "warmup": args.warmup, "ms_per_step": el / nk * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "closed-channel DNS 192x192x96, 4pi x 2pi x 2, nu=1/180, SSPRK33 dt=1e-4"},
+        "config": dict(CONFIG),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

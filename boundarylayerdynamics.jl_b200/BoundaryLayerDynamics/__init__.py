@@ -40,29 +40,29 @@ FIELDS = ("vel1", "vel2", "vel3")
 
 # ----------------------------------------------------------------- domain (src/Domains.jl)
 class SmoothWall:
-    """No-slip, no-penetration wall (src/Domains.jl:316-322)."""
+    """No-slip, no-penetration wall (src/Domains.jl:173-179)."""
 
 
 class RoughWall:
-    """Rough wall with roughness length z0 (src/Domains.jl:324-335)."""
+    """Rough wall with roughness length z0 (src/Domains.jl:181-192)."""
 
     def __init__(self, roughness, von_karman_constant=0.4):
         self.roughness, self.von_karman_constant = float(roughness), float(von_karman_constant)
 
 
 class FreeSlipBoundary:
-    """No-penetration boundary with vanishing tangential gradients (src/Domains.jl:337-343)."""
+    """No-penetration boundary with vanishing tangential gradients (src/Domains.jl:194-200)."""
 
 
 class CustomBoundary:
-    """Explicit BCs: ``CustomBoundary(vel1=("dirichlet", 1.0), vel3="dirichlet")`` (src/Domains.jl:345-363)."""
+    """Explicit BCs: ``CustomBoundary(vel1=("dirichlet", 1.0), vel3="dirichlet")`` (src/Domains.jl:202-220)."""
 
     def __init__(self, **behaviors):
         self.behaviors = behaviors
 
 
 class SinusoidalMapping:
-    """Vertical grid stretching (src/Domains.jl:214-238)."""
+    """Vertical grid stretching (src/Domains.jl:72-130)."""
 
     def __init__(self, eta, variant="auto"):
         if not 0 < eta < 1:
@@ -83,7 +83,7 @@ def _f(z):
 
 
 class Domain:
-    """``Domain(dims, lower_boundary, upper_boundary, mapping=None)`` (src/Domains.jl:173-190,240-278)."""
+    """``Domain(dims, lower_boundary, upper_boundary, mapping=None)`` (src/Domains.jl:30-47,97-135)."""
 
     def __init__(self, dims, lower_boundary, upper_boundary, mapping=None):
         self.hsize = (float(dims[0]), float(dims[1]))
@@ -132,7 +132,7 @@ class Domain:
 
 
 def _bctype(boundary, field):
-    """(kind, value) per src/boundary_conditions.jl:296-338."""
+    """(kind, value) per src/boundary_conditions.jl:85-95,53-59."""
     if isinstance(boundary, CustomBoundary):
         b = boundary.behaviors[field]
         kind, val = (b, 0.0) if isinstance(b, str) else (b[0], float(b[1]))

@@ -1623,7 +1623,7 @@ int32_t bld_create(const bld_config* cfg, bld_handle** out) {
     for (int m = 0; m < h->B; ++m) h->flag_host[m] = 0;
     h->diverged.assign(h->B, 0);
 
-    // ---- wavenumber factors (src/Domains.jl:285-288, src/derivatives.jl:21-27)
+    // ---- wavenumber factors (src/Domains.jl:142-145, src/derivatives.jl:21-27)
     const double TWO_PI = 2.0 * M_PI;
     std::vector<double> d1(K1), d2(K2), DD1(K1), DD2(K2);
     const double c1 = TWO_PI / cfg->l1, c2 = TWO_PI / cfg->l2;
@@ -1642,7 +1642,7 @@ int32_t bld_create(const bld_config* cfg, bld_handle** out) {
     for (int i = 0; i <= n3; ++i) aext[i] = (double)n3 / cfg->dx3_i[i];
     for (int i = 0; i < n3 - 1; ++i) ai[i] = aext[i + 1];
     const double L3 = cfg->x3_max - cfg->x3_min;
-    for (int i = 0; i < n3; ++i) mw[i] = 1.0 / ac[i] / L3;  // ConstantMean weight (src/processes/sources.jl:62)
+    for (int i = 0; i < n3; ++i) mw[i] = 1.0 / ac[i] / L3;  // ConstantMean weight (src/processes/sources.jl:64)
     H_TRY(upload(h, &h->d1, d1));
     H_TRY(upload(h, &h->d2, d2));
     H_TRY(upload(h, &h->DD1, DD1));
@@ -1695,7 +1695,7 @@ int32_t bld_create(const bld_config* cfg, bld_handle** out) {
         for (int s = 0; s < 2; ++s) {
             L.bc_kind[f][s] = cfg->bc_kind[f][s];
             L.bc_val[f][s] = cfg->bc_value[f][s];
-            // ConstantGradient.difference = gradient * Dvmap(zeta_wall) / N3 (src/boundary_conditions.jl:299-320)
+            // ConstantGradient.difference = gradient * Dvmap(zeta_wall) / N3 (src/boundary_conditions.jl:56-57,69,76)
             L.bc_diff[f][s] = cfg->bc_value[f][s] * (cfg->dx3_i[s == 0 ? 0 : n3] / (double)n3);
         }
     }
@@ -2413,24 +2413,34 @@ int32_t bld_ldlt_solve_real_device(const double* gamma, const double* beta, doub
 }  // extern "C"
 
 // ---------------------------------------------------------------- no-alloc projection
-// Scratch of bld_project_noalloc: one fixed array per device, looked up once per
-// device with cudaGetSymbolAddress (host code may not use the symbol as an address).
+// Scratch of bld_project_noalloc: one fixed array per device, whose device
+// address host code gets from cudaGetSymbolAddress (the symbol itself is not an
+// address in host code).
 static __device__ __align__(256) double2 g_noalloc_scratch[BLD_NOALLOC_MAX_VALUES];
 
 namespace {
 std::mutex g_noalloc_mutex;
 std::map<int, void*> g_noalloc_ptr;  // device ordinal -> device address of g_noalloc_scratch
 
-int noalloc_scratch(void** out) {
+// The device address of the scratch array on the current device.  Outside a
+// stream capture it is looked up on every call, so an address recorded before a
+// device reset or under an earlier primary context is never reused; during a
+// capture (where the lookup could load the module) the address recorded by an
+// earlier call on this device is used.
+int noalloc_scratch(cudaStream_t stream, void** out) {
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(stream, &cap));
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    auto it = g_noalloc_ptr.find(dev);
-    if (it == g_noalloc_ptr.end()) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* ptr = nullptr;
         CUDA_TRY(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-        it = g_noalloc_ptr.emplace(dev, ptr).first;
+        g_noalloc_ptr[dev] = ptr;
     }
+    auto it = g_noalloc_ptr.find(dev);
+    if (it == g_noalloc_ptr.end())
+        return fail(BLD_ERR_ARGUMENT, "bld_project_noalloc: the first call on a device must come before any stream capture");
     *out = it->second;
     return BLD_OK;
 }
@@ -2441,13 +2451,17 @@ extern "C" int32_t bld_project_noalloc(int32_t k1max, int32_t k2max, int32_t n3,
                                        const double* d2, double w_lo, double w_hi, void* state, void* stream) {
     if (!gamma || !alpha_c || !alpha_i || !d1 || !d2 || !state) return fail(BLD_ERR_ARGUMENT, "null argument");
     if (k1max < 0 || k2max < 0 || n3 < 3) return fail(BLD_ERR_INVALID_CONFIG, "invalid grid size");
-    const long long F = (long long)(k1max + 1) * (2 * k2max + 1);
-    if ((long long)n3 * F > (long long)BLD_NOALLOC_MAX_VALUES)
+    // the regular projection's check (src/processes/pressure.jl:357)
+    if (w_lo != w_hi) return fail(BLD_ERR_UNSUPPORTED_BC, "The mean flow must be equal at both vertical boundaries.");
+    // sizes in 64 bits before any product, so that none wraps past the limit
+    const long long F = ((long long)k1max + 1) * (2LL * k2max + 1);
+    const long long values = F > (long long)BLD_NOALLOC_MAX_VALUES ? F : (long long)n3 * F;
+    if (values > (long long)BLD_NOALLOC_MAX_VALUES)
         return fail(BLD_ERR_INVALID_CONFIG,
                     "bld_project_noalloc: n3*(k1max+1)*(2*k2max+1) = %lld exceeds the fixed scratch of %d values",
-                    (long long)n3 * F, BLD_NOALLOC_MAX_VALUES);
+                    values, BLD_NOALLOC_MAX_VALUES);
     void* scratch = nullptr;
-    BLD_TRY(noalloc_scratch(&scratch));
+    BLD_TRY(noalloc_scratch((cudaStream_t)stream, &scratch));
     ProjArgs a{};
     a.g.k1max = k1max;
     a.g.k2max = k2max;

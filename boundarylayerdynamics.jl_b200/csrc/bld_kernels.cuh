@@ -92,7 +92,7 @@ struct InvYArgs {
 };
 
 // value of spectral term `op` at (z, j, k1); D1 = i*d1, D2 = i*d2
-// (src/derivatives.jl:67-80,228-230; src/Domains.jl:285-288)
+// (src/derivatives.jl:67-80,228-230; src/Domains.jl:142-145)
 __device__ __forceinline__ double2 inv_term_value(const InvYArgs& a, const double2* __restrict__ S, int op, int f,
                                                   int z, int j, int k1) {
     const Geo& g = a.g;
@@ -884,7 +884,7 @@ struct FwdYArgs {
 };
 
 // Frequency-domain Laplacian with ghost layers (src/processes/molecular_diffusion.jl:57-72,
-// src/boundary_conditions.jl:506-602) and the constant source (src/processes/sources.jl:30-35).
+// src/boundary_conditions.jl:254-359) and the constant source (src/processes/sources.jl:32-35).
 __device__ __forceinline__ double2 linear_terms(const Geo& g, const Linear& L, const double2* __restrict__ S, int f,
                                                 int z, int j, int k1, int m) {
     double2 val = make_double2(0.0, 0.0);
@@ -933,7 +933,7 @@ __device__ __forceinline__ double2 linear_terms(const Geo& g, const Linear& L, c
             A = L.alpha_c[z];
             B = L.alpha_i[z];
             Cc = L.alpha_c[z + 1];
-            // Dirichlet values enter every mode (src/boundary_conditions.jl:506-517)
+            // Dirichlet values enter every mode (src/boundary_conditions.jl:263-273)
             qm = (z == 0) ? make_double2(L.bc_val[2][0], 0.0) : Sf[(long long)(z - 1) * g.F + mo];
             qp = (z == n - 1) ? make_double2(L.bc_val[2][1], 0.0) : Sf[(long long)(z + 1) * g.F + mo];
         }
@@ -1531,7 +1531,7 @@ __device__ __forceinline__ double2 stage_value_k(const ProjArgs& a, long long id
 
 // One thread per (k1, k2) column: stage update, divergence (div!, src/processes/pressure.jl:368-378),
 // forward/backward Thomas (:106-165), gradient (add_gradient!, :405-426), then ConstantMean
-// (src/processes/sources.jl:69-77) on the (0,0) column.  grid (ceil(F/128), members)
+// (src/processes/sources.jl:71-77) on the (0,0) column.  grid (ceil(F/128), members)
 __global__ void __launch_bounds__(128) k_project(ProjArgs a) {
     const Geo& g = a.g;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1875,7 +1875,7 @@ __device__ __forceinline__ void project_seg_body(const ProjArgs& a, double2* til
             }
         }
     }
-    // ConstantMean on the (0,0) column (src/processes/sources.jl:69-77)
+    // ConstantMean on the (0,0) column (src/processes/sources.jl:71-77)
     __syncthreads();
     if (c == 0 && s == 0) {
         for (int f = 0; f < 2; ++f) {

@@ -39,7 +39,7 @@ typedef enum {
                                      (src/processes/pressure.jl:338-339,357); advection
                                      needs w = 0 (src/processes/momentum_advection.jl:182);
                                      SGS needs rough-wall / free-slip walls
-                                     (src/processes/static_smagorinsky.jl:298-304)           */
+                                     (src/processes/static_smagorinsky.jl:92-98)           */
     BLD_ERR_CUDA = -5,            /* a CUDA runtime call failed (see bld_last_error)         */
     BLD_ERR_TIMEOUT = -6,         /* a bounded device wait expired                           */
     BLD_ERR_ARGUMENT = -7,        /* null pointer / out-of-range argument                    */
@@ -48,7 +48,7 @@ typedef enum {
 
 typedef enum { BLD_BC_DIRICHLET = 0, BLD_BC_NEUMANN = 1 } bld_bc_kind;
 
-/* wall types used by the SGS wall model (src/Domains.jl:322-343) */
+/* wall types used by the SGS wall model (src/Domains.jl:181-200) */
 typedef enum { BLD_WALL_OTHER = 0, BLD_WALL_ROUGH = 1, BLD_WALL_FREESLIP = 2 } bld_wall_kind;
 
 typedef enum { BLD_FP64 = 0, BLD_MIXED = 1 } bld_precision;
@@ -62,7 +62,7 @@ typedef enum { BLD_DEALIAS_NONE = 0, BLD_DEALIAS_QUADRATIC = 1, BLD_DEALIAS_EXPL
 /*
  * Model description (Model(resolution, domain, processes), src/BoundaryLayerDynamics.jl:72-97).
  * The vertical mapping is passed as tables the caller evaluates from its Domain
- * (src/Domains.jl:240-278): dx3/dzeta at the C nodes and at the n3+1 I
+ * (src/Domains.jl:97-135): dx3/dzeta at the C nodes and at the n3+1 I
  * positions zeta = 0, 1/n3, ..., 1, and x3 at the C and interior I nodes.
  * Arrays are copied by bld_create; the caller keeps ownership.
  */
@@ -76,7 +76,7 @@ typedef struct {
     const double* x3_c;            /* [n3]    vmap at C nodes                              */
     const double* x3_i;            /* [n3-1]  vmap at interior I nodes                     */
     /* boundary conditions per field (vel1, vel2, vel3) and side (lower, upper);
-       for Neumann the value is the gradient d/dx3 (src/boundary_conditions.jl:296-302) */
+       for Neumann the value is the gradient d/dx3 (src/boundary_conditions.jl:40-43,55-57) */
     int32_t bc_kind[3][2];
     double bc_value[3][2];
     int32_t wall_kind[2];          /* lower/upper wall type for the SGS wall model         */
@@ -277,11 +277,17 @@ int32_t bld_ldlt_solve_real_device(const double* gamma, const double* beta, doub
    in one fixed device array inside the library of BLD_NOALLOC_MAX_VALUES
    complex doubles (16 MiB), which every GPU that loads the library holds until
    the process exits; n3 * (k1max+1) * (2*k2max+1) above that limit is rejected
-   with BLD_ERR_INVALID_CONFIG.  The first call on a device looks up the array's
-   device address and should come before any stream capture.  All calls share
-   the array: calls that overlap on the GPU (other streams, other threads) race,
-   so serialise them.  The solve writes every scratch value before reading it,
-   so no clearing is needed between calls. */
+   with BLD_ERR_INVALID_CONFIG.  `w_lo` and `w_hi` are the Dirichlet values of
+   vel3 at the lower and upper boundary; like the regular projection, unequal
+   values are rejected with BLD_ERR_UNSUPPORTED_BC ("The mean flow must be equal
+   at both vertical boundaries.").  Every call outside a stream capture looks up
+   the array's device address on the current device (so a device reset does not
+   leave a stale address behind); a call during a capture uses the address an
+   earlier call on that device found, so the first call on a device must come
+   before any stream capture.  All calls share the array: calls that overlap on
+   the GPU (other streams, other threads) race, so serialise them.  The solve
+   writes every scratch value before reading it, so no clearing is needed
+   between calls. */
 #define BLD_NOALLOC_MAX_VALUES (1 << 20)
 int32_t bld_project_noalloc(int32_t k1max, int32_t k2max, int32_t n3,
                             const double* gamma, const double* alpha_c, const double* alpha_i,

@@ -145,7 +145,7 @@ class CustomBoundary:
         self.behaviors = behaviors
 
 
-def _hasboundarylayer(b):                                               # src/Domains.jl:365-367
+def _hasboundarylayer(b):                                               # src/Domains.jl:222-224
     if isinstance(b, (RoughWall, SmoothWall)):
         return True
     if isinstance(b, FreeSlipBoundary):
@@ -154,7 +154,7 @@ def _hasboundarylayer(b):                                               # src/Do
 
 
 class SinusoidalMapping:
-    """Grid stretching x3 = sin(zeta*eta*pi/2)/sin(eta*pi/2) (src/Domains.jl:234-273)."""
+    """Grid stretching x3 = sin(zeta*eta*pi/2)/sin(eta*pi/2) (src/Domains.jl:72-130)."""
 
     def __init__(self, eta, variant="auto"):
         assert 0 < eta < 1
@@ -166,7 +166,7 @@ def _as_float(z):
 
 
 class Domain:
-    """``Domain(dims, lower, upper, mapping)`` (src/Domains.jl:173-190,240-278)."""
+    """``Domain(dims, lower, upper, mapping)`` (src/Domains.jl:30-47,97-135)."""
 
     def __init__(self, dims, lower_boundary, upper_boundary, mapping=None):
         self.hsize = (float(dims[0]), float(dims[1]))
@@ -178,7 +178,7 @@ class Domain:
             x3min, x3max = 0.0, float(dims[2])
         self.lower_boundary, self.upper_boundary = lower_boundary, upper_boundary
         self.mapping = mapping
-        if mapping is None:                                             # :275-276
+        if mapping is None:                                             # src/Domains.jl:132-133
             l3 = x3max - x3min
             self._vmap = lambda z: x3min + _as_float(z) * l3
             self._dvmap = lambda z: x3max - x3min
@@ -214,7 +214,7 @@ class Domain:
     def Dvmap(self, zeta):
         return float(self._dvmap(zeta))
 
-    def size3(self):                                                    # :193-197
+    def size3(self):                                                    # src/Domains.jl:50-54
         return self.vmap(Fraction(1)) - self.vmap(Fraction(0))
 
     def extrema3(self):
@@ -222,7 +222,7 @@ class Domain:
 
 
 def bctype(boundary, field):
-    """(kind, value) for ``field`` at ``boundary`` (src/boundary_conditions.jl:328-338,296-302)."""
+    """(kind, value) for ``field`` at ``boundary`` (src/boundary_conditions.jl:85-95,53-59)."""
     if isinstance(boundary, CustomBoundary):
         b = boundary.behaviors[field]
         if isinstance(b, str):
@@ -236,7 +236,7 @@ def bctype(boundary, field):
 
 
 def init_bcs(field, domain, grid):
-    """Lower/upper BCs; Neumann keeps gradient*dx3 (src/boundary_conditions.jl:304-322)."""
+    """Lower/upper BCs; Neumann keeps gradient*dx3 (src/boundary_conditions.jl:53-79)."""
     out = []
     for b, zeta in ((domain.lower_boundary, 0), (domain.upper_boundary, 1)):
         kind, val = bctype(b, field)
@@ -250,7 +250,7 @@ def init_bcs(field, domain, grid):
     return tuple(out)
 
 
-def dx1factors(domain, grid):                                           # src/Domains.jl:285-288
+def dx1factors(domain, grid):                                           # src/Domains.jl:142-145
     return 1j * grid.wavenumbers(1) * (2 * math.pi / domain.hsize[0])
 
 
@@ -413,7 +413,7 @@ class MeanProfiles:
 
     def step(self, state, t):
         """prepare_samples! + log_state! + process_log! for a checkpoint at t."""
-        w = (t - self.timespan[1]) / 2                                  # :372
+        w = (t - self.timespan[1]) / 2                                  # :373
         for f in self.means:
             self.means[f] += w * self.samples[f]
         self.sample_state(state)
@@ -427,7 +427,7 @@ class MeanProfiles:
         return {f: v / dt for f, v in self.means.items()}
 
 
-def h1range(P, centered=False):                                         # :64-65
+def h1range(P, centered=False):                                         # src/physical_space.jl:64-65
     return [Fraction(2 * i + (1 if centered else 0), 2 * P) for i in range(P)]
 
 
@@ -518,7 +518,7 @@ def incompressible_flow(viscosity, sgs_model=None, constant_forcing=None, consta
 
 class _DiscretizedDiffusion:
     """src/processes/molecular_diffusion.jl:31-72 with layers_expand_full
-    (src/boundary_conditions.jl:497-602) and second_derivatives (src/derivatives.jl:21-27)."""
+    (src/boundary_conditions.jl:254-359) and second_derivatives (src/derivatives.jl:21-27)."""
 
     kind = "linear"
 
@@ -532,7 +532,7 @@ class _DiscretizedDiffusion:
         self.DD3 = dx3factors(domain, grid, self.ns, neighbors=True)
 
     def _expanded(self, q):
-        """Layers (below, q..., above) (src/boundary_conditions.jl:506-602)."""
+        """Layers (below, q..., above) (src/boundary_conditions.jl:263-359)."""
         lower, upper = self.bcs
         n = q.shape[0]
         if self.ns == "I":
@@ -541,16 +541,16 @@ class _DiscretizedDiffusion:
                     raise ValueError("I-node diffusion supports Dirichlet boundaries only")
             return lower[1], list(q), upper[1]          # scalar values, broadcast to every mode
         if lower[0] == "dirichlet":
-            below = (-15 * q[0] + 5 * q[1] - q[2]) / 5                  # :537-538
+            below = (-15 * q[0] + 5 * q[1] - q[2]) / 5                  # src/boundary_conditions.jl:294-295
             below[0, 0] += 16 * lower[1] / 5
         else:
-            below = (21 * q[0] + 3 * q[1] - q[2]) / 23                  # :573-574
+            below = (21 * q[0] + 3 * q[1] - q[2]) / 23                  # src/boundary_conditions.jl:330-331
             below[0, 0] -= 24 * lower[2] / 23
         if upper[0] == "dirichlet":
-            above = (-15 * q[n - 1] + 5 * q[n - 2] - q[n - 3]) / 5      # :555-556
+            above = (-15 * q[n - 1] + 5 * q[n - 2] - q[n - 3]) / 5      # src/boundary_conditions.jl:312-313
             above[0, 0] += 16 * upper[1] / 5
         else:
-            above = (21 * q[n - 1] + 3 * q[n - 2] - q[n - 3]) / 23      # :591-592
+            above = (21 * q[n - 1] + 3 * q[n - 2] - q[n - 3]) / 23      # src/boundary_conditions.jl:348-349
             above[0, 0] -= 24 * (-upper[2]) / 23
         return below, list(q), above
 
@@ -559,14 +559,14 @@ class _DiscretizedDiffusion:
         below, layers, above = self._expanded(q)
         ext = [below] + layers + [above]
         out = rates[self.field]
-        for i in range(q.shape[0]):                                     # src/processes/molecular_diffusion.jl:495-498
+        for i in range(q.shape[0]):                                     # src/processes/molecular_diffusion.jl:59-61
             a, b, c = self.DD3[i]
             out[i] += self.nu * (a * b * ext[i] + (self.DD1 + self.DD2 - a * b - b * c) * ext[i + 1]
                                  + b * c * ext[i + 2])
 
 
 class _DiscretizedSource:
-    """ConstantSource.add_rates! (src/processes/sources.jl:30-35)."""
+    """ConstantSource.add_rates! (src/processes/sources.jl:32-35)."""
 
     kind = "linear"
 
@@ -641,7 +641,7 @@ class _DiscretizedPressure:
         d3g3[1:] -= ai_ext[1:n]
         d3g3[:n - 1] -= ai_ext[1:n]
         k1, k2 = grid.wavenumbers(1), grid.wavenumbers(2)
-        s1, s2 = 1 / domain.hsize[0], 1 / domain.hsize[1]               # scalefactor (src/Domains.jl:303-307)
+        s1, s2 = 1 / domain.hsize[0], 1 / domain.hsize[1]               # scalefactor (src/Domains.jl:160-171)
         K2, K1 = grid.K2, grid.K1
         diag = np.empty((K2, K1, n))
         for j in range(K2):
@@ -755,14 +755,14 @@ class _DiscretizedSmagorinsky:
     def __init__(self, d, domain, grid):
         self.dims = pdsize(grid, d.dealiasing)
         n = grid.n3global
-        d1 = domain.hsize[0] / (2 * grid.k1max + 2)                     # :60-61
+        d1 = domain.hsize[0] / (2 * grid.k1max + 2)                     # src/processes/static_smagorinsky.jl:54-55
         d2 = domain.hsize[1] / (2 * grid.k2max + 2)
         zc, zi = grid.vrange("C"), grid.vrange("I")
-        d3c = np.array([domain.Dvmap(z) for z in zc]) / n               # :62-63
+        d3c = np.array([domain.Dvmap(z) for z in zc]) / n               # src/processes/static_smagorinsky.jl:56-57
         d3i = np.array([domain.Dvmap(z) for z in zi]) / n
-        lc = d.model_constant * np.cbrt(d1 * d2 * d3c)                  # :64-65
+        lc = d.model_constant * np.cbrt(d1 * d2 * d3c)                  # src/processes/static_smagorinsky.jl:58-59
         li = d.model_constant * np.cbrt(d1 * d2 * d3i)
-        if d.wall_damping:                                              # :68-93
+        if d.wall_damping:                                              # src/processes/static_smagorinsky.jl:61-85
             x3c = np.array([domain.vmap(z) for z in zc])
             x3i = np.array([domain.vmap(z) for z in zi])
             x3min, x3max = domain.extrema3()
@@ -773,12 +773,12 @@ class _DiscretizedSmagorinsky:
             li = (li ** (-N) + liw ** (-N)) ** (-1 / N)
         self.lc, self.li = lc.reshape(-1, 1, 1), li.reshape(-1, 1, 1)
         x3min, x3max = domain.extrema3()
-        dx3_below = domain.vmap(zc[0]) - x3min                          # :305-306
+        dx3_below = domain.vmap(zc[0]) - x3min                          # src/processes/static_smagorinsky.jl:99-100
         dx3_above = x3max - domain.vmap(zc[-1])
         lw = self._init_wall(domain.lower_boundary, dx3_below)
         uw = self._init_wall(domain.upper_boundary, dx3_above)
         self.wall_dynamic = (lw[0], uw[0])
-        self.factors_strain = (lw[1], -uw[1])                           # :312-313
+        self.factors_strain = (lw[1], -uw[1])                           # src/processes/static_smagorinsky.jl:106-107
         self.factors_stress = (lw[2], -uw[2])
         self.D3c = dx3factors(domain, grid, "C")
         self.D3i = dx3factors(domain, grid, "I")
@@ -797,7 +797,7 @@ class _DiscretizedSmagorinsky:
         return min(ml(x3 - x3min, domain.lower_boundary), ml(x3max - x3, domain.upper_boundary))
 
     @staticmethod
-    def _init_wall(boundary, dx3):                                      # :298-304
+    def _init_wall(boundary, dx3):                                      # src/processes/static_smagorinsky.jl:92-98
         if isinstance(boundary, RoughWall):
             lg = math.log(dx3 / boundary.roughness)
             return (True, 1 / (2 * dx3 * lg), -boundary.von_karman_constant ** 2 / lg ** 2)
