@@ -96,6 +96,11 @@ class Clocks:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to print its first sample: start the
+            # sampled work only once it does (at most 10 s)
+            t0 = time.time()
+            while not self.rows and self.proc.poll() is None and time.time() - t0 < 10:
+                time.sleep(0.05)
         except OSError:
             self.proc = None
         return self

@@ -120,6 +120,9 @@ struct YCfg {
     int NL = 4;    // k1 lines per term (per field and line set)
     int thr = 256;
     int wfft = 0;  // per-term kernels: radix of the warp transform (P2 = 32 wfft), 0 = block stages
+    int tp = 0;    // 1: two-pass kernels (k_inv_y2 / k_fwd_y2), BLD_Y2_NL lines, P2 = A * B;
+                   // 2: inverse pass with TMA-staged tiles (k_inv_y3), BLD_Y3_NL lines
+    int zc = 1;    // tp 2: layer chunks (blocks along z)
 };
 
 // radices of the warp y transforms compiled for the per-term y kernels
@@ -345,11 +348,142 @@ int y_threads(const FftPlan& pl, int lines) {
     return std::min(256, std::max(64, (tasks + 31) / 32 * 32));
 }
 
+// two-pass y kernels: compiled for P2 with a factorisation y2_radix_a/b (single
+// precision up to 768, double up to 288) and their registers per block count
+bool y2_ok(int P2, bool fp32) { return y2_radix_a(P2) > 0 && (fp32 || P2 <= 288); }
+size_t smem_y2(int P2, int lines, bool fp32) { return (size_t)P2 * (1 + lines) * csize(fp32); }
+
+template <typename R, int P>
+int launch_y2_p(bld_handle* h, bool inverse, const void* args, dim3 grid, size_t sm) {
+    constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
+    constexpr int MINB = y2_min_blocks<R>(B * BLD_Y2_NL);
+    if (inverse)
+        k_inv_y2<R, A, B, MINB><<<grid, B * BLD_Y2_NL, sm, h->stream>>>(*static_cast<const InvYArgs*>(args));
+    else
+        k_fwd_y2<R, A, B, MINB><<<grid, B * BLD_Y2_NL, sm, h->stream>>>(*static_cast<const FwdYArgs*>(args));
+    return BLD_OK;
+}
+
+template <typename R>
+int launch_y2(bld_handle* h, int P2, bool inverse, const void* args, dim3 grid, size_t sm) {
+    switch (P2) {
+        case 64: return launch_y2_p<R, 64>(h, inverse, args, grid, sm);
+        case 96: return launch_y2_p<R, 96>(h, inverse, args, grid, sm);
+        case 128: return launch_y2_p<R, 128>(h, inverse, args, grid, sm);
+        case 144: return launch_y2_p<R, 144>(h, inverse, args, grid, sm);
+        case 192: return launch_y2_p<R, 192>(h, inverse, args, grid, sm);
+        case 256: return launch_y2_p<R, 256>(h, inverse, args, grid, sm);
+        case 288: return launch_y2_p<R, 288>(h, inverse, args, grid, sm);
+        default: break;
+    }
+    if constexpr (sizeof(R) == 4) {
+        switch (P2) {
+            case 384: return launch_y2_p<R, 384>(h, inverse, args, grid, sm);
+            case 512: return launch_y2_p<R, 512>(h, inverse, args, grid, sm);
+            case 768: return launch_y2_p<R, 768>(h, inverse, args, grid, sm);
+            default: break;
+        }
+    }
+    return fail(BLD_ERR_INVALID_CONFIG, "no two-pass y transform for P2=%d", P2);
+}
+
+// cuTensorMapEncodeTiled from the driver, found through the runtime (the
+// library links only the static CUDA runtime)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// the members' states from `base` as a float64 tensor (2 K1, K2, 3 n3 - 1, members)
+// with the box (2 NL, K2, 1, 1) of k_inv_y3
+int state_tmap(const bld_handle* h, const void* base, int nl, CUtensorMap* out) {
+    const Geo& g = h->g;
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return fail(BLD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const cuuint64_t dims[4] = {(cuuint64_t)(2 * g.K1), (cuuint64_t)g.K2, (cuuint64_t)(3 * g.n3 - 1), (cuuint64_t)h->B};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.K1 * 16, (cuuint64_t)g.F * 16, (cuuint64_t)g.mstride * 16};
+    const cuuint32_t box[4] = {(cuuint32_t)(2 * nl), (cuuint32_t)g.K2, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(BLD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return BLD_OK;
+}
+
+// k_inv_y3 applies: a two-pass factorisation, whole K2 columns in one TMA box
+// (K2 <= 256) and the staged tiles within the shared memory of a block
+bool y3_ok(const bld_handle* h, int P2) {
+    return y2_ok(P2, h->fp32) && h->g.K2 <= 256 &&
+           y3_smem(P2, h->g.K2, (int)csize(h->fp32)) <= 227 * 1024 && encode_tiled() != nullptr;
+}
+
+template <typename R, int P>
+int launch_y3_p(bld_handle* h, const InvYArgs& a, const CUtensorMap& map, dim3 grid) {
+    constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
+    const size_t sm = y3_smem(P, h->g.K2, (int)sizeof(cplx<R>));
+    k_inv_y3<R, A, B><<<grid, B * BLD_Y3_NL, sm, h->stream>>>(a, map);
+    return BLD_OK;
+}
+
+template <typename R>
+int launch_inv_y3(bld_handle* h, const Space& s, InvYArgs a, int nm) {
+    CUtensorMap map;
+    BLD_TRY(state_tmap(h, a.state, BLD_Y3_NL, &map));
+    a.NL = BLD_Y3_NL;
+    a.zchunk = (h->g.n3 + s.inv.zc - 1) / s.inv.zc;
+    a.flag = h->flag;
+    dim3 grid(a.nterms * nm, (h->g.K1 + BLD_Y3_NL - 1) / BLD_Y3_NL, (h->g.n3 + a.zchunk - 1) / a.zchunk);
+    switch (s.P2) {
+        case 64: return launch_y3_p<R, 64>(h, a, map, grid);
+        case 96: return launch_y3_p<R, 96>(h, a, map, grid);
+        case 128: return launch_y3_p<R, 128>(h, a, map, grid);
+        case 144: return launch_y3_p<R, 144>(h, a, map, grid);
+        case 192: return launch_y3_p<R, 192>(h, a, map, grid);
+        case 256: return launch_y3_p<R, 256>(h, a, map, grid);
+        case 288: return launch_y3_p<R, 288>(h, a, map, grid);
+        default: break;
+    }
+    if constexpr (sizeof(R) == 4) {
+        switch (s.P2) {
+            case 384: return launch_y3_p<R, 384>(h, a, map, grid);
+            case 512: return launch_y3_p<R, 512>(h, a, map, grid);
+            case 768: return launch_y3_p<R, 768>(h, a, map, grid);
+            default: break;
+        }
+    }
+    return fail(BLD_ERR_INVALID_CONFIG, "no TMA y transform for P2=%d", s.P2);
+}
+
 template <typename R>
 int launch_inv_y(bld_handle* h, const Space& s, InvYArgs a, int nm) {
     const YCfg& c = s.inv;
     a.NL = c.NL;
     const size_t cs = csize(sizeof(R) == 4);
+    if (c.tp == 2) {
+        BLD_TRY(launch_inv_y3<R>(h, s, a, nm));
+        CUDA_TRY(cudaGetLastError());
+        return BLD_OK;
+    }
+    if (c.tp) {
+        a.NL = BLD_Y2_NL;
+        dim3 grid(a.nterms * nm, (h->g.K1 + BLD_Y2_NL - 1) / BLD_Y2_NL, h->g.n3);
+        BLD_TRY(launch_y2<R>(h, s.P2, true, &a, grid, smem_y2(s.P2, BLD_Y2_NL, sizeof(R) == 4)));
+        CUDA_TRY(cudaGetLastError());
+        return BLD_OK;
+    }
     if (c.all) {
         dim3 grid((h->g.K1 + c.NL - 1) / c.NL, h->g.n3, nm);
         k_inv_y_all<R><<<grid, c.thr, (size_t)(s.P2 + s.P2 * a.nterms * c.NL) * cs, h->stream>>>(a);
@@ -384,6 +518,13 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
     const YCfg& c = s.fwd;
     a.NL = c.NL;
     const size_t cs = csize(sizeof(R) == 4);
+    if (c.tp) {
+        a.NL = BLD_Y2_NL;
+        dim3 grid(a.fields * nm, (h->g.K1 + BLD_Y2_NL - 1) / BLD_Y2_NL, h->g.n3);
+        BLD_TRY(launch_y2<R>(h, s.P2, false, &a, grid, smem_y2(s.P2, s.fsets * BLD_Y2_NL, sizeof(R) == 4)));
+        CUDA_TRY(cudaGetLastError());
+        return BLD_OK;
+    }
     if (c.all) {
         dim3 grid((h->g.K1 + c.NL - 1) / c.NL, h->g.n3, nm);
         k_fwd_y_all<R><<<grid, c.thr, (size_t)(s.P2 + s.P2 * 3 * s.fsets * c.NL) * cs, h->stream>>>(a);
@@ -590,7 +731,7 @@ int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
 
 template <typename R>
 int set_smem_limits_R() {
-    const int lim = 200 * 1024;
+    const int lim = 227 * 1024;   // the largest dynamic shared memory a B200 block may opt into
     // large dynamic shared memory, and the largest shared-memory carveout so the
     // per-SM block count is set by the kernel's real footprint
 #define BLD_SET(K)                                                                           \
@@ -623,6 +764,36 @@ int set_smem_limits_R() {
     }
     BLD_SET((k_inv_y_all<R>));
     BLD_SET((k_fwd_y_all<R>));
+#define BLD_SET_Y2(P)                                                                                  \
+    BLD_SET((k_inv_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks<R>(y2_radix_b(P) * BLD_Y2_NL)>)); \
+    BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks<R>(y2_radix_b(P) * BLD_Y2_NL)>));
+    BLD_SET_Y2(64)
+    BLD_SET_Y2(96)
+    BLD_SET_Y2(128)
+    BLD_SET_Y2(144)
+    BLD_SET_Y2(192)
+    BLD_SET_Y2(256)
+    BLD_SET_Y2(288)
+    if constexpr (sizeof(R) == 4) {
+        BLD_SET_Y2(384)
+        BLD_SET_Y2(512)
+        BLD_SET_Y2(768)
+    }
+#undef BLD_SET_Y2
+#define BLD_SET_Y3(P) BLD_SET((k_inv_y3<R, y2_radix_a(P), y2_radix_b(P)>));
+    BLD_SET_Y3(64)
+    BLD_SET_Y3(96)
+    BLD_SET_Y3(128)
+    BLD_SET_Y3(144)
+    BLD_SET_Y3(192)
+    BLD_SET_Y3(256)
+    BLD_SET_Y3(288)
+    if constexpr (sizeof(R) == 4) {
+        BLD_SET_Y3(384)
+        BLD_SET_Y3(512)
+        BLD_SET_Y3(768)
+    }
+#undef BLD_SET_Y3
     BLD_SET((k_adv_x<R, 1, 0>));
     BLD_SET((k_adv_x<R, 2, 0>));
     BLD_SET((k_adv_x<R, 3, 0>));
@@ -906,12 +1077,55 @@ bool yforce_warp() {
     const char* e = getenv("BLD_Y_KERNEL");
     return e && !strcmp(e, "warp");
 }
+// BLD_Y_KERNEL=twopass keeps only the two-pass y kernels (where compiled);
+// BLD_Y_KERNEL=tma the inverse pass with TMA-staged tiles (forward: two-pass)
+bool yforce_twopass() {
+    const char* e = getenv("BLD_Y_KERNEL");
+    return e && !strcmp(e, "twopass");
+}
+bool yforce_tma() {
+    const char* e = getenv("BLD_Y_KERNEL");
+    return e && !strcmp(e, "tma");
+}
 
 // y-pass candidates: per-term blocks (two-buffer FFT) with several line counts
 // and block sizes, and all-terms blocks (in-place FFT); lines * element size of
 // at least 32 bytes keeps global accesses sector-sized
-std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_per_nl, int all_lines_per_nl) {
+std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_per_nl, int all_lines_per_nl,
+                               bool inverse) {
     std::vector<YCfg> out;
+    // inverse pass with TMA-staged tiles: one candidate per z-chunk count
+    if (inverse && y3_ok(h, s.P2) && (getenv("BLD_Y_KERNEL") == nullptr || yforce_tma())) {
+        const int n3 = h->g.n3;
+        int last = -1;
+        for (int zc : {1, 2, 3, 4, 6, 8, 12}) {
+            const int zchunk = (n3 + zc - 1) / zc;
+            if (zchunk == last || (zc > 1 && zchunk < 4)) continue;
+            last = zchunk;
+            YCfg c{};
+            c.NL = BLD_Y3_NL;
+            c.thr = y2_radix_b(s.P2) * BLD_Y3_NL;
+            c.tp = 2;
+            c.zc = zc;
+            out.push_back(c);
+        }
+        if (yforce_tma()) return out;
+    }
+    const bool tp_ok = y2_ok(s.P2, h->fp32) && smem_y2(s.P2, lines_per_nl * BLD_Y2_NL, h->fp32) <= 200 * 1024;
+    if (tp_ok && !yforce_warp() && getenv("BLD_Y_KERNEL") == nullptr) {
+        YCfg c{};
+        c.NL = BLD_Y2_NL;
+        c.thr = y2_radix_b(s.P2) * BLD_Y2_NL;
+        c.tp = 1;
+        out.push_back(c);
+    }
+    if (tp_ok && (yforce_twopass() || (yforce_tma() && !inverse))) {
+        YCfg c{};
+        c.NL = BLD_Y2_NL;
+        c.thr = y2_radix_b(s.P2) * BLD_Y2_NL;
+        c.tp = 1;
+        return {c};
+    }
     const size_t cs = csize(h->fp32);
     const int nls_pt[4] = {h->fp32 ? 4 : 2, h->fp32 ? 8 : 4, h->fp32 ? 16 : 8, h->fp32 ? 32 : 16};
     for (int nl : nls_pt) {
@@ -991,7 +1205,7 @@ int autotune(bld_handle* h) {
         if (!s.on) continue;
         float best = 1e30f, t = 0;
         YCfg bi = s.inv;
-        for (const YCfg& c : y_candidates(h, s, 1, s.ntin)) {
+        for (const YCfg& c : y_candidates(h, s, 1, s.ntin, true)) {
             s.inv = c;
             BLD_TRY(time_launches(h, [&] { return enqueue_inv_y(h, sp, h->u, 0, B); }, 3, &t));
             if (t < best) {
@@ -1095,7 +1309,7 @@ int autotune(bld_handle* h) {
         x_chunks(h, s);
         best = 1e30f;
         YCfg bf = s.fwd;
-        for (const YCfg& c : y_candidates(h, s, s.fsets, 3 * s.fsets)) {
+        for (const YCfg& c : y_candidates(h, s, s.fsets, 3 * s.fsets, false)) {
             s.fwd = c;
             BLD_TRY(time_launches(h, [&] { return enqueue_fwd_y(h, sp, true, false, h->u, h->io2, 0, B); }, 3, &t));
             if (t < best) {
@@ -1379,16 +1593,18 @@ int ldlt_launch(const double* gamma, const double* beta, T* rhs, long long nsys,
 int check_flag(bld_handle* h) {
     CUDA_TRY(cudaMemcpyAsync(h->flag_host, h->flag, h->B * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
-    bool any = false;
+    bool any = false, timeout = false;
     for (int m = 0; m < h->B; ++m)
         if (h->flag_host[m]) {
             any = true;
-            h->diverged[m] = 1;
+            if (h->flag_host[m] & BLD_FLAG_TIMEOUT) timeout = true;
+            if (h->flag_host[m] & BLD_FLAG_NONFINITE) h->diverged[m] = 1;
             h->flag_host[m] = 0;
         }
     if (any) {
         CUDA_TRY(cudaMemsetAsync(h->flag, 0, h->B * sizeof(int), h->stream));
         CUDA_TRY(cudaStreamSynchronize(h->stream));
+        if (timeout) return fail(BLD_ERR_TIMEOUT, "a bounded device wait expired (a TMA copy did not complete)");
         return fail(BLD_ERR_DIVERGED, "The simulation has diverged.");
     }
     return BLD_OK;
@@ -2181,9 +2397,12 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         else
             snprintf(xname, sizeof xname, "%s<%s, %d, %d>", xk, R, s.PPT, s.xr);
         char iname[64], fname[64];
-        if (s.inv.all) snprintf(iname, sizeof iname, "k_inv_y_all<%s>", R);
+        if (s.inv.tp == 2) snprintf(iname, sizeof iname, "k_inv_y3<%s, %d, %d>", R, y2_radix_a(s.P2), y2_radix_b(s.P2));
+        else if (s.inv.tp) snprintf(iname, sizeof iname, "k_inv_y2<%s, %d, %d>", R, y2_radix_a(s.P2), y2_radix_b(s.P2));
+        else if (s.inv.all) snprintf(iname, sizeof iname, "k_inv_y_all<%s>", R);
         else snprintf(iname, sizeof iname, "k_inv_y<%s, %d>", R, s.inv.wfft);
-        if (s.fwd.all) snprintf(fname, sizeof fname, "k_fwd_y_all<%s>", R);
+        if (s.fwd.tp) snprintf(fname, sizeof fname, "k_fwd_y2<%s, %d, %d>", R, y2_radix_a(s.P2), y2_radix_b(s.P2));
+        else if (s.fwd.all) snprintf(fname, sizeof fname, "k_fwd_y_all<%s>", R);
         else snprintf(fname, sizeof fname, "k_fwd_y<%s, %d>", R, s.fwd.wfft);
         snprintf(tmp, sizeof tmp,
                  "%s\"%s\": {\"P\": [%d, %d], \"inv_y\": \"%s\", \"x\": \"%s\", \"fwd_y\": \"%s\", "

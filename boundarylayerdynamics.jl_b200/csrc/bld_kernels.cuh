@@ -80,6 +80,8 @@ struct InvYArgs {
     int isI[BLD_MAXT];
     int m0;                      // first member
     int NL;                      // k1 lines per block
+    int zchunk;                  // layers per block (k_inv_y3)
+    int* flag;                   // [members] error flags (k_inv_y3: a bounded wait expired)
     const int* active;           // [members] 0 = skip the member (NULL: all active)
     const double2* state;
     void* mixed;
@@ -1019,6 +1021,133 @@ __device__ __forceinline__ double2 linear_terms_w(const Geo& g, const Linear& L,
     return val;
 }
 
+// Epilogue of the forward y pass: the transformed lines `res` (position p of
+// line l at res[swz(p) * LS + l]; B lines at l + NL) give the truncated, scaled
+// rate of field f at layer z, summed with the linear terms, written as the rate
+// or as the fused stage value (see FwdYArgs), with the non-finite check.
+template <typename R, int RAD, int OB = 4>
+__device__ __forceinline__ void fwd_y_epilogue(const FwdYArgs& a, const cplx<R>* __restrict__ res, int LS, int m,
+                                               int f, int z, int nz, int k10, int NL, int nls, bool hasB) {
+    using C = cplx<R>;
+    const Geo& g = a.g;
+    const int K1 = g.K1, K2 = g.K2, k2max = g.k2max, P2 = a.P2;
+    double2* du = a.du + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F;
+    const double2* Sf = a.state ? a.state + (long long)m * g.mstride + fld_off(g, f) : nullptr;
+    const bool need_win = (a.mode == 1) && a.lin.diff_on[f];
+    const int w0 = lin_window_start(z, nz);
+    const int wn = min(3, nz);
+    bool bad = false;
+    // OB: outputs per thread whose loads are issued together
+    const int nout = K2 * NL;
+    // the epilogue with the mode and the window loads fixed at compile time, so
+    // that the loads of OB outputs are straight-line code
+    double2* so = a.fuse ? a.sout + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F : nullptr;
+    const double2* su = (a.fuse && a.su) ? a.su + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F : nullptr;
+    auto epilogue = [&](auto mode_c, auto win_c, auto fuse_c) {
+        constexpr int MODE = decltype(mode_c)::value;
+        constexpr bool WIN = decltype(win_c)::value;
+        // 0: the rate; 1: (cu su + ct state + cd rate) / div; 2: state + cd rate
+        constexpr int FZ = decltype(fuse_c)::value;
+        constexpr bool FUSE = FZ != 0;
+        for (int o0 = 0; o0 < nout; o0 += OB * blockDim.x) {
+            double2 W[OB][3];
+            double2 old[OB], U[OB], T[OB];
+#pragma unroll
+            for (int q = 0; q < OB; ++q) {
+                const int o = o0 + q * blockDim.x + threadIdx.x;
+                const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
+                if (o < nout && k1 < K1) {
+                    const long long idx = (long long)j * K1 + k1;
+                    if constexpr (WIN) {
+#pragma unroll
+                        for (int r = 0; r < 3; ++r)
+                            if (r < wn) W[q][r] = Sf[(long long)(w0 + r) * g.F + idx];
+                    }
+                    if constexpr (MODE == 0) old[q] = du[idx];
+                    if constexpr (FZ == 1) U[q] = su[idx];
+                    if constexpr (FUSE && !WIN) T[q] = Sf[(long long)z * g.F + idx];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < OB; ++q) {
+                const int o = o0 + q * blockDim.x + threadIdx.x;
+                const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
+                if (o >= nout || k1 >= K1) continue;
+                const int pos = swz<C, RAD>((j <= k2max) ? j : P2 - (K2 - j));
+                const C X = res[pos * LS + l];
+                double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
+                if (hasB) {
+                    const C Y = res[pos * LS + NL + l];
+                    const double d = a.d2[j];
+                    const double bx = (double)Y.x * a.inv_n, by = (double)Y.y * a.inv_n;
+                    vx += -d * by;
+                    vy += d * bx;
+                }
+                const long long idx = (long long)j * K1 + k1;
+                double2 v;
+                if constexpr (MODE == 1) {
+                    double2 lin;
+                    if constexpr (WIN)
+                        lin = linear_terms_w(g, a.lin, W[q], w0, f, z, j, k1, m);
+                    else
+                        lin = linear_terms(g, a.lin, nullptr, f, z, j, k1, m);
+                    v = make_double2(lin.x + vx, lin.y + vy);
+                } else if constexpr (MODE == 2) {
+                    v = make_double2(vx, vy);
+                } else {
+                    v = make_double2(old[q].x + vx, old[q].y + vy);
+                }
+                if constexpr (FUSE) {
+                    double2 tz;
+                    if constexpr (WIN) {
+                        const int r = z - w0;   // the window holds layer z
+                        tz = r == 0 ? W[q][0] : (r == 1 ? W[q][1] : W[q][2]);
+                    } else {
+                        tz = T[q];
+                    }
+                    if constexpr (FZ == 1) {
+                        const double2 uz = U[q];
+                        so[idx] = make_double2((a.st_cu * uz.x + a.st_ct * tz.x + a.st_cd * v.x) / a.st_div,
+                                               (a.st_cu * uz.y + a.st_ct * tz.y + a.st_cd * v.y) / a.st_div);
+                    } else {   // Euler stage: state + dt rate (src/ODEMethods.jl:101)
+                        so[idx] = make_double2(tz.x + a.st_cd * v.x, tz.y + a.st_cd * v.y);
+                    }
+                } else {
+                    du[idx] = v;
+                }
+                if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
+            }
+        }
+    };
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    using I2 = std::integral_constant<int, 2>;
+    using BT = std::integral_constant<bool, true>;
+    using BF = std::integral_constant<bool, false>;
+    const int fz = a.fuse ? (a.su ? 1 : 2) : 0;
+    if (fz == 1 && a.mode == 1 && need_win)
+        epilogue(I1{}, BT{}, I1{});
+    else if (fz == 1 && a.mode == 1)
+        epilogue(I1{}, BF{}, I1{});
+    else if (fz == 1 && a.mode == 0)
+        epilogue(I0{}, BF{}, I1{});
+    else if (fz == 2 && a.mode == 1 && need_win)
+        epilogue(I1{}, BT{}, I2{});
+    else if (fz == 2 && a.mode == 1)
+        epilogue(I1{}, BF{}, I2{});
+    else if (fz == 2 && a.mode == 0)
+        epilogue(I0{}, BF{}, I2{});
+    else if (a.mode == 1 && need_win)
+        epilogue(I1{}, BT{}, I0{});
+    else if (a.mode == 1)
+        epilogue(I1{}, BF{}, I0{});
+    else if (a.mode == 0)
+        epilogue(I0{}, BF{}, I0{});
+    else
+        epilogue(I2{}, BF{}, I0{});
+    if (a.check && bad) atomicOr(a.flag + m, 1);
+}
+
 // grid (fields*members, ceil(K1/NL), n3); smem tw[P2] + 2*P2*nlines complex (nlines = NL or 2NL)
 // RAD > 0: one line per warp in registers on a padded line stride (see k_inv_y)
 template <typename R, int RAD>
@@ -1164,121 +1293,7 @@ __global__ void __launch_bounds__(256) k_fwd_y(FwdYArgs a) {
     } else {
         res = fft_big<R, -1>(b0, b1, nlines, 1, nlines, false, a.plan, tw);
     }
-    double2* du = a.du + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F;
-    const double2* Sf = a.state ? a.state + (long long)m * g.mstride + fld_off(g, f) : nullptr;
-    const bool need_win = (a.mode == 1) && a.lin.diff_on[f];
-    const int w0 = lin_window_start(z, nz);
-    const int wn = min(3, nz);
-    bool bad = false;
-    constexpr int OB = 4;  // outputs per thread whose loads are issued together
-    const int nout = K2 * NL;
-    // the epilogue with the mode and the window loads fixed at compile time, so
-    // that the loads of OB outputs are straight-line code
-    double2* so = a.fuse ? a.sout + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F : nullptr;
-    const double2* su = (a.fuse && a.su) ? a.su + (long long)m * a.du_mstride + fld_off(g, f) + (long long)z * g.F : nullptr;
-    auto epilogue = [&](auto mode_c, auto win_c, auto fuse_c) {
-        constexpr int MODE = decltype(mode_c)::value;
-        constexpr bool WIN = decltype(win_c)::value;
-        // 0: the rate; 1: (cu su + ct state + cd rate) / div; 2: state + cd rate
-        constexpr int FZ = decltype(fuse_c)::value;
-        constexpr bool FUSE = FZ != 0;
-        for (int o0 = 0; o0 < nout; o0 += OB * blockDim.x) {
-            double2 W[OB][3];
-            double2 old[OB], U[OB], T[OB];
-#pragma unroll
-            for (int q = 0; q < OB; ++q) {
-                const int o = o0 + q * blockDim.x + threadIdx.x;
-                const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
-                if (o < nout && k1 < K1) {
-                    const long long idx = (long long)j * K1 + k1;
-                    if constexpr (WIN) {
-#pragma unroll
-                        for (int r = 0; r < 3; ++r)
-                            if (r < wn) W[q][r] = Sf[(long long)(w0 + r) * g.F + idx];
-                    }
-                    if constexpr (MODE == 0) old[q] = du[idx];
-                    if constexpr (FZ == 1) U[q] = su[idx];
-                    if constexpr (FUSE && !WIN) T[q] = Sf[(long long)z * g.F + idx];
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < OB; ++q) {
-                const int o = o0 + q * blockDim.x + threadIdx.x;
-                const int j = o >> nls, l = o & (NL - 1), k1 = k10 + l;
-                if (o >= nout || k1 >= K1) continue;
-                const int pos = swz<C, RAD>((j <= k2max) ? j : P2 - (K2 - j));
-                const C X = res[pos * LS + l];
-                double vx = (double)X.x * a.inv_n, vy = (double)X.y * a.inv_n;
-                if (hasB) {
-                    const C Y = res[pos * LS + NL + l];
-                    const double d = a.d2[j];
-                    const double bx = (double)Y.x * a.inv_n, by = (double)Y.y * a.inv_n;
-                    vx += -d * by;
-                    vy += d * bx;
-                }
-                const long long idx = (long long)j * K1 + k1;
-                double2 v;
-                if constexpr (MODE == 1) {
-                    double2 lin;
-                    if constexpr (WIN)
-                        lin = linear_terms_w(g, a.lin, W[q], w0, f, z, j, k1, m);
-                    else
-                        lin = linear_terms(g, a.lin, nullptr, f, z, j, k1, m);
-                    v = make_double2(lin.x + vx, lin.y + vy);
-                } else if constexpr (MODE == 2) {
-                    v = make_double2(vx, vy);
-                } else {
-                    v = make_double2(old[q].x + vx, old[q].y + vy);
-                }
-                if constexpr (FUSE) {
-                    double2 tz;
-                    if constexpr (WIN) {
-                        const int r = z - w0;   // the window holds layer z
-                        tz = r == 0 ? W[q][0] : (r == 1 ? W[q][1] : W[q][2]);
-                    } else {
-                        tz = T[q];
-                    }
-                    if constexpr (FZ == 1) {
-                        const double2 uz = U[q];
-                        so[idx] = make_double2((a.st_cu * uz.x + a.st_ct * tz.x + a.st_cd * v.x) / a.st_div,
-                                               (a.st_cu * uz.y + a.st_ct * tz.y + a.st_cd * v.y) / a.st_div);
-                    } else {   // Euler stage: state + dt rate (src/ODEMethods.jl:101)
-                        so[idx] = make_double2(tz.x + a.st_cd * v.x, tz.y + a.st_cd * v.y);
-                    }
-                } else {
-                    du[idx] = v;
-                }
-                if (!(isfinite(v.x) && isfinite(v.y))) bad = true;
-            }
-        }
-    };
-    using I0 = std::integral_constant<int, 0>;
-    using I1 = std::integral_constant<int, 1>;
-    using I2 = std::integral_constant<int, 2>;
-    using BT = std::integral_constant<bool, true>;
-    using BF = std::integral_constant<bool, false>;
-    const int fz = a.fuse ? (a.su ? 1 : 2) : 0;
-    if (fz == 1 && a.mode == 1 && need_win)
-        epilogue(I1{}, BT{}, I1{});
-    else if (fz == 1 && a.mode == 1)
-        epilogue(I1{}, BF{}, I1{});
-    else if (fz == 1 && a.mode == 0)
-        epilogue(I0{}, BF{}, I1{});
-    else if (fz == 2 && a.mode == 1 && need_win)
-        epilogue(I1{}, BT{}, I2{});
-    else if (fz == 2 && a.mode == 1)
-        epilogue(I1{}, BF{}, I2{});
-    else if (fz == 2 && a.mode == 0)
-        epilogue(I0{}, BF{}, I2{});
-    else if (a.mode == 1 && need_win)
-        epilogue(I1{}, BT{}, I0{});
-    else if (a.mode == 1)
-        epilogue(I1{}, BF{}, I0{});
-    else if (a.mode == 0)
-        epilogue(I0{}, BF{}, I0{});
-    else
-        epilogue(I2{}, BF{}, I0{});
-    if (a.check && bad) atomicOr(a.flag + m, 1);
+    fwd_y_epilogue<R, RAD>(a, res, LS, m, f, z, nz, k10, NL, nls, hasB);
 }
 
 // Forward y pass of all three rate fields at one layer: one block per (k1 tile,
@@ -2126,3 +2141,5 @@ __global__ void __launch_bounds__(128) k_profile_sample(Geo g, const double2* __
         Pv[i] = v;
     }
 }
+
+#include "bld_ypass2.cuh"

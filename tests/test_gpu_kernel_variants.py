@@ -173,17 +173,64 @@ Y_CASES = [
 ]
 
 
+def _y3_fits(p2, n2, precision):
+    """The TMA inverse y kernel runs where a TMA box holds whole k2 columns
+    (K2 <= 256) and its staged tiles fit a block's shared memory."""
+    k2 = 2 * ((n2 - 1) // 2) + 1
+    al = lambda b: (b + 127) // 128 * 128
+    cs = 8 if precision == "mixed" else 16
+    return k2 <= 256 and 128 + al(p2 * cs) + al(p2 * 8 * cs) + 6 * al(k2 * 8 * 16) <= 227 * 1024
+
+
+# P2 with a two-pass y kernel: both precisions, and single precision only
+Y2_SIZES = {64, 96, 128, 144, 192, 256, 288}
+Y2_SIZES_FP32 = {384, 512, 768}
+
+
 @pytest.mark.parametrize("res,precision,les,tol", Y_CASES)
-@pytest.mark.parametrize("family", ["warp", "block"])
+@pytest.mark.parametrize("family", ["warp", "block", "twopass", "tma"])
 def test_y_kernel_family(oracle, BLD, res, precision, les, tol, family):
     om = _build(oracle, res, les=les)
     gm = _forced_y(BLD, family, res, precision, les)
+    if family in ("twopass", "tma"):   # the forced family is the one that runs where it is compiled
+        inv = "k_inv_y2<" if family == "twopass" else "k_inv_y3<"
+        for space in gm.kernels().values():
+            if not isinstance(space, dict):
+                continue
+            p2 = space["P"][1]
+            if family == "tma" and not _y3_fits(p2, res[1], precision):
+                continue
+            if p2 in Y2_SIZES or (precision == "mixed" and p2 in Y2_SIZES_FP32):
+                assert space["inv_y"].startswith(inv) and space["fwd_y"].startswith("k_fwd_y2<"), space
     st = _state(om, seed=sum(res) + 1)
     ref = om.compute_rates(st)
     got = gm.compute_rates(st)
     for f in om.fields:
         e = rel_l2(got[f], ref[f])
         assert e < tol, (res, precision, family, f, e)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
+def test_twopass_y_trajectory(oracle, BLD, precision, tol):
+    """20 SSP-RK33 steps of an LES with both spaces on the two-pass y kernels
+    (advection P2 = 96, SGS P2 = 64): the forward pass forms the fused stage
+    values and the chained Euler stages, checked against the oracle."""
+    res = (32, 64, 8)
+    om = _build(oracle, res, les=True)
+    gm = _forced_y(BLD, "twopass", res, precision, True)
+    for space in gm.kernels().values():
+        if isinstance(space, dict):
+            assert space["fwd_y"].startswith("k_fwd_y2<"), space
+    st = _state(om, seed=77)
+    om.apply_projections(st)
+    gm.set_state(st)
+    om.state.update({f: v.copy() for f, v in st.items()})
+    om.evolve(20 * 1e-4, 1e-4)
+    gm.evolve(20 * 1e-4, 1e-4)
+    got = gm.state
+    for f in om.fields:
+        e = rel_l2(got[f], om.state[f])
+        assert e < tol, (precision, f, e)
 
 
 # LES: the SGS x kernel (block Stockham or warp line transforms) with the advection
