@@ -18,6 +18,7 @@
 #include "bld.h"
 #include "bld_kernels.cuh"
 #include "bld_warpx.cuh"
+#include "bld_advx2.cuh"
 
 double2 h_wtab64[BLD_WTAB_SIZE];
 float2 h_wtab32[BLD_WTAB_SIZE];
@@ -144,6 +145,7 @@ struct Space {
     int xwmb = 1;                                   // warp-per-row kernel: register cap (min blocks of 128 threads)
     int zmult = 2;                                  // x kernels: z-chunk count multiplier in halves (autotuned)
     int xb = 0;                                     // block of warps per row (advection): 1 three warps, 2 five (pipelined)
+    int x2 = 0;                                     // 1: two-pass shared-memory x kernel (advection, BLD_X2_NR rows)
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
@@ -260,7 +262,7 @@ int pick_y(int P2, bool fp32, int sets) {
 // fill the GPU a few times over, at least 8 layers per chunk
 void x_chunks(const bld_handle* h, Space& s) {
     const int n3 = h->g.n3;
-    const int rows = s.xb ? 1 : (s.xw ? s.xw : s.YT);
+    const int rows = s.x2 ? BLD_X2_NR : (s.xb ? 1 : (s.xw ? s.xw : s.YT));
     const long long blocks_per_chunk = (long long)((s.P2 + rows - 1) / rows) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
     want = std::min(want, std::max(1, n3 / 8));
@@ -554,6 +556,44 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
     return BLD_OK;
 }
 
+// two-pass advection x kernel: compiled for P1 with a two-pass factorisation
+// (single precision up to 768, double up to 288), whole row pairs per block
+bool x2_ok(const bld_handle* h, const Space& s) {
+    return y2_ok(s.P1, h->fp32) && s.P2 % BLD_X2_NR == 0 &&
+           x2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, (int)csize(h->fp32)) <= 227 * 1024;
+}
+
+template <typename R, int P>
+int launch_x2_p(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
+    dim3 grid(s.P2 / BLD_X2_NR, s.nchunks, nm);
+    const size_t sm = x2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>));
+    k_adv_x2<R, A, B><<<grid, x2_threads(B), sm, h->stream>>>(a, h->flag);
+    return BLD_OK;
+}
+
+template <typename R>
+int launch_adv_x2(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    switch (s.P1) {
+        case 64: BLD_TRY((launch_x2_p<R, 64>(h, s, a, nm))); break;
+        case 96: BLD_TRY((launch_x2_p<R, 96>(h, s, a, nm))); break;
+        case 128: BLD_TRY((launch_x2_p<R, 128>(h, s, a, nm))); break;
+        case 144: BLD_TRY((launch_x2_p<R, 144>(h, s, a, nm))); break;
+        case 192: BLD_TRY((launch_x2_p<R, 192>(h, s, a, nm))); break;
+        case 256: BLD_TRY((launch_x2_p<R, 256>(h, s, a, nm))); break;
+        case 288: BLD_TRY((launch_x2_p<R, 288>(h, s, a, nm))); break;
+        default:
+            if constexpr (sizeof(R) == 4) {
+                if (s.P1 == 384) { BLD_TRY((launch_x2_p<R, 384>(h, s, a, nm))); break; }
+                if (s.P1 == 512) { BLD_TRY((launch_x2_p<R, 512>(h, s, a, nm))); break; }
+                if (s.P1 == 768) { BLD_TRY((launch_x2_p<R, 768>(h, s, a, nm))); break; }
+            }
+            return fail(BLD_ERR_INVALID_CONFIG, "no two-pass x kernel for P1=%d", s.P1);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
 // radices of the warp line transforms compiled into the block x kernels, and the
 // points per thread that go with each (so that YT * 32 RAD / PPT threads are whole warps)
 bool xr_radix_ok(int r) { return r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 9 || r == 12 || r == 16 || r == 24; }
@@ -794,6 +834,20 @@ int set_smem_limits_R() {
         BLD_SET_Y3(768)
     }
 #undef BLD_SET_Y3
+#define BLD_SET_X2(P) BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P)>));
+    BLD_SET_X2(64)
+    BLD_SET_X2(96)
+    BLD_SET_X2(128)
+    BLD_SET_X2(144)
+    BLD_SET_X2(192)
+    BLD_SET_X2(256)
+    BLD_SET_X2(288)
+    if constexpr (sizeof(R) == 4) {
+        BLD_SET_X2(384)
+        BLD_SET_X2(512)
+        BLD_SET_X2(768)
+    }
+#undef BLD_SET_X2
     BLD_SET((k_adv_x<R, 1, 0>));
     BLD_SET((k_adv_x<R, 2, 0>));
     BLD_SET((k_adv_x<R, 3, 0>));
@@ -956,6 +1010,7 @@ int enqueue_x_R(bld_handle* h, int sp, int m0, int nm) {
     xa.w_hi = h->w_hi;
     xa.active = h->mask_on ? h->active : nullptr;
     if (sp == 0) {
+        if (s.x2) return launch_adv_x2<R>(h, s, xa, nm);
         if (s.xb) return launch_adv_xb<R>(h, s, xa, nm);
         return s.xw ? launch_adv_xw<R>(h, s, xa, nm) : launch_adv_x<R>(h, s, xa, nm);
     }
@@ -1183,6 +1238,7 @@ int autotune(bld_handle* h) {
     const bool only_bw3 = xk && !strcmp(xk, "blockwarp"), only_pipe = xk && !strcmp(xk, "pipe");
     const bool only_bw = only_bw3 || only_pipe;   // a block-of-warps kernel (three warps, or five pipelined)
     const bool only_lines = xk && !strcmp(xk, "lines");   // block kernels with warp line transforms
+    const bool only_x2 = xk && !strcmp(xk, "twopass");     // the two-pass shared-memory x kernel
     const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1, h->fp32) > 0;
     if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
     const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
@@ -1255,9 +1311,9 @@ int autotune(bld_handle* h) {
         // its best z-chunk count (and, for the warp-per-row kernel, register
         // cap: more resident warps want more chunks)
         struct XPick {
-            int YT, PPT, xr, xw, xwmb, xb, zmult;
+            int YT, PPT, xr, xw, xwmb, xb, zmult, x2;
         };
-        auto get_pick = [&]() { return XPick{s.YT, s.PPT, s.xr, s.xw, s.xwmb, s.xb, s.zmult}; };
+        auto get_pick = [&]() { return XPick{s.YT, s.PPT, s.xr, s.xw, s.xwmb, s.xb, s.zmult, s.x2}; };
         auto set_pick = [&](const XPick& p) {
             s.YT = p.YT;
             s.PPT = p.PPT;
@@ -1266,6 +1322,7 @@ int autotune(bld_handle* h) {
             s.xwmb = p.xwmb;
             s.xb = p.xb;
             s.zmult = p.zmult;
+            s.x2 = p.x2;
             x_chunks(h, s);
         };
         const char* mbe = getenv("BLD_XW_MINB");   // force one register cap (1, 3, 4)
@@ -1296,14 +1353,15 @@ int autotune(bld_handle* h) {
             return BLD_OK;
         };
         const bool block_ok = best < 1e30f;   // a block kernel was timed above
-        if (block_ok) BLD_TRY(tune_chunks(XPick{byt, bppt, bxr, 0, 1, 0, 2}));
-        const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw && !only_lines;
-        for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) BLD_TRY(tune_chunks(XPick{1, 1, 0, wpb, 1, 0, 2}));
+        if (block_ok && (sp == 1 || !only_x2)) BLD_TRY(tune_chunks(XPick{byt, bppt, bxr, 0, 1, 0, 2, 0}));
+        const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw && !only_lines && !only_x2;
+        for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) BLD_TRY(tune_chunks(XPick{1, 1, 0, wpb, 1, 0, 2, 0}));
         for (int xbk = 1; xbk <= 2; ++xbk) {
-            if (!(sp == 0 && adv_bw_ok && !only_block && !only_warp && !only_lines)) break;
+            if (!(sp == 0 && adv_bw_ok && !only_block && !only_warp && !only_lines && !only_x2)) break;
             if ((xbk == 1 && only_pipe) || (xbk == 2 && only_bw3)) continue;
-            BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2}));
+            BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2, 0}));
         }
+        if (sp == 0 && x2_ok(h, s) && (only_x2 || !xk)) BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1}));
         if (bx >= 1e30f) return fail(BLD_ERR_INVALID_CONFIG, "no x kernel could be timed");
         set_pick(bp);
         x_chunks(h, s);
@@ -2388,7 +2446,9 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         char tmp[768];
         const char* xk = sp == 0 ? "k_adv_x" : "k_sgs_x";
         char xname[96];
-        if (sp == 0 && s.xb)
+        if (sp == 0 && s.x2)
+            snprintf(xname, sizeof xname, "k_adv_x2<%s, %d, %d>", R, y2_radix_a(s.P1), y2_radix_b(s.P1));
+        else if (sp == 0 && s.xb)
             snprintf(xname, sizeof xname, "%s<%s, %d>", s.xb == 2 ? "k_adv_xp" : "k_adv_xb", R, s.P1 / 32);
         else if (sp == 0 && s.xw && s.xwmb > 1)
             snprintf(xname, sizeof xname, "k_adv_xwc<%s, %d, %d>", R, s.P1 / 32, s.xwmb);

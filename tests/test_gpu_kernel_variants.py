@@ -82,7 +82,7 @@ CASES = [
 
 
 @pytest.mark.parametrize("res,precision,tol", CASES)
-@pytest.mark.parametrize("family", ["warp", "block", "blockwarp", "pipe", "lines"])
+@pytest.mark.parametrize("family", ["warp", "block", "blockwarp", "pipe", "lines", "twopass"])
 def test_advection_x_kernel_family(oracle, BLD, res, precision, tol, family):
     if family == "warp" and precision == "fp64" and res[0] == 192:
         pytest.skip("the warp-per-row kernel is compiled for radix <= 6 in FP64 (P1 = 288 is radix 9)")
@@ -90,7 +90,9 @@ def test_advection_x_kernel_family(oracle, BLD, res, precision, tol, family):
         pytest.skip("the warp-per-row kernel is compiled for radix <= 12 (P1 = 512, 768 are radix 16, 24)")
     om = _build(oracle, res)
     gm = _forced(BLD, family, res, precision)
-    if family != "block":
+    if family == "twopass":
+        assert gm.kernels()["advection"]["x"].startswith("k_adv_x2<"), gm.kernels()
+    elif family != "block":
         assert gm.info.adv_p1 % 32 == 0
     st = _state(om, seed=sum(res))
     ref = om.compute_rates(st)
@@ -127,7 +129,7 @@ def test_warp_x_kernel_register_caps(oracle, BLD, res, minb):
         assert e < 1e-5, (res, minb, f, e)
 
 
-@pytest.mark.parametrize("family", ["warp", "blockwarp", "pipe"])
+@pytest.mark.parametrize("family", ["warp", "blockwarp", "pipe", "twopass"])
 def test_warp_kernel_les_mixed_trajectory(oracle, BLD, family):
     """The warp advection kernels inside a full LES step sequence (mixed form)."""
     res = (64, 64, 16)
@@ -145,6 +147,26 @@ def test_warp_kernel_les_mixed_trajectory(oracle, BLD, family):
     for f in om.fields:
         e = rel_l2(got[f], om.state[f])
         assert e < 1e-5, (f, e)
+
+
+def test_twopass_x_dns_trajectory(oracle, BLD):
+    """20 SSP-RK33 steps of a DNS with the two-pass x kernel (P1 = 96) in the
+    plain form, against the oracle at the trajectory tolerance (1e-9)."""
+    res = (64, 32, 12)
+    om = _build(oracle, res)
+    gm = _forced(BLD, "twopass", res, "fp64")
+    assert gm.kernels()["advection"]["x"].startswith("k_adv_x2<"), gm.kernels()
+    st = _state(om, seed=12)
+    for f in st:
+        st[f] *= 20.0
+    gm.set_state(st)
+    om.state.update({f: v.copy() for f, v in st.items()})
+    om.evolve(20 * 1e-4, 1e-4)
+    gm.evolve(20 * 1e-4, 1e-4)
+    got = gm.state
+    for f in om.fields:
+        e = rel_l2(got[f], om.state[f])
+        assert e < 1e-9, (f, e)
 
 
 def _forced_y(BLD, family, res, precision, les):
