@@ -22,25 +22,25 @@
 
 #include "bld_tma.cuh"
 
-#define BLD_X2_NR 2
-
-__host__ __device__ constexpr int x2_threads(int B) { return (3 * BLD_X2_NR * B + 31) / 32 * 32; }
+// y rows per block: 2 in double precision, 4 in single (shared memory per block)
+__host__ __device__ constexpr int x2_rows(int csz) { return csz == 16 ? 2 : 4; }
+__host__ __device__ constexpr int x2_threads(int B, int NR) { return (3 * NR * B + 31) / 32 * 32; }
 __host__ __device__ constexpr int x2_al(int b) { return (b + 127) / 128 * 128; }
 // dynamic shared memory: barriers, twiddles, 2 stages x 6 terms x NR rows,
 // pass-1 buffer (3 NR lines of A (B + 1)), physical / spectral lines (3 NR x P),
 // forward inputs (NR + NR / 2 lines of P)
 __host__ __device__ constexpr int x2_smem(int A, int B, int K1, int csz) {
-    return 128 + x2_al(A * B * csz) + x2_al(2 * 6 * BLD_X2_NR * K1 * csz) +
-           x2_al(3 * BLD_X2_NR * (A * (B + 1) + 128 / csz) * csz) +
-           x2_al(3 * BLD_X2_NR * A * B * csz) + x2_al((BLD_X2_NR + BLD_X2_NR / 2) * A * B * csz);
+    return 128 + x2_al(A * B * csz) + x2_al(2 * 6 * x2_rows(csz) * K1 * csz) +
+           x2_al(3 * x2_rows(csz) * (A * (B + 1) + 128 / csz) * csz) + x2_al(3 * x2_rows(csz) * A * B * csz) +
+           x2_al((x2_rows(csz) + x2_rows(csz) / 2) * A * B * csz);
 }
 
-// grid (P2 / NR, nchunks, members), block x2_threads(B)
+// grid (P2 / NR, nchunks, members), block x2_threads(B, NR); NR = x2_rows(sizeof(C))
 template <typename R, int A, int B>
-__global__ void __launch_bounds__(x2_threads(B)) k_adv_x2(XArgs a, int* flag) {
+__global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>)))) k_adv_x2(XArgs a, int* flag) {
     using C = cplx<R>;
-    constexpr int P = A * B, NR = BLD_X2_NR, NLI = 3 * NR, NLF = NR + NR / 2;
-    constexpr int T = x2_threads(B);
+    constexpr int P = A * B, NR = x2_rows(sizeof(C)), NLI = 3 * NR, NLF = NR + NR / 2;
+    constexpr int T = x2_threads(B, NR);
     constexpr int PPT = (NR * P + T - 1) / T;   // product points per thread
     constexpr int X1S = B + 1;                  // pass-1 stride of a task's outputs
     constexpr int E = 128 / (int)sizeof(C);     // elements per 128-byte bank row
@@ -95,7 +95,6 @@ __global__ void __launch_bounds__(x2_threads(B)) k_adv_x2(XArgs a, int* flag) {
     R pu[PPT], pv[PPT], pw[PPT], po1[PPT], po2[PPT];
 #pragma unroll
     for (int i = 0; i < PPT; ++i) pu[i] = pv[i] = pw[i] = po1[i] = po2[i] = R(0);
-    bool ok_all = true;
 
     for (int j = jb; j < z1; ++j) {
         const int s = (j - jb) & 1;
@@ -106,7 +105,6 @@ __global__ void __launch_bounds__(x2_threads(B)) k_adv_x2(XArgs a, int* flag) {
             issue(j + 1, s ^ 1);
         }
         const bool arrived = mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1);
-        ok_all &= arrived;
         const C* cur = stage + (size_t)s * 6 * NR * K1;
         // ---- inverse pass 1: lines L = 3 r + p (pairs (u, v), (vort3, w), (vort1, vort2))
         for (int task = threadIdx.x; task < NLI * B; task += T) {
@@ -137,7 +135,16 @@ __global__ void __launch_bounds__(x2_threads(B)) k_adv_x2(XArgs a, int* flag) {
 #pragma unroll
             for (int q = 0; q < A; ++q) X1[L * X1L + q * X1S + jt] = x[q];
         }
-        __syncthreads();
+        // a block whose wait expired stops here (uniformly), after the copies it
+        // issued have landed
+        if (__syncthreads_or(!arrived)) {
+            if (threadIdx.x == 0) {
+                atomicOr(flag + m, BLD_FLAG_TIMEOUT);
+                mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1);
+                if (j + 1 < z1) mbar_wait_bounded(&bar[s ^ 1], ((j + 1 - jb) >> 1) & 1);
+            }
+            return;
+        }
         // ---- inverse pass 2 -> physical lines Ph[L][x]
         for (int task = threadIdx.x; task < NLI * A; task += T) {
             const int L = task / A, j2 = task - L * A;
@@ -229,13 +236,6 @@ __global__ void __launch_bounds__(x2_threads(B)) k_adv_x2(XArgs a, int* flag) {
                 mrow_w(Mout, a, 2, j - 1, y0 + r + 1)[f] = vb;
             }
         }
-        // a block whose wait expired stops after the copies it issued have landed
-        if (__syncthreads_or(!ok_all)) {
-            if (threadIdx.x == 0) {
-                atomicOr(flag + m, BLD_FLAG_TIMEOUT);
-                if (j + 1 < z1) mbar_wait_bounded(&bar[s ^ 1], ((j + 1 - jb) >> 1) & 1);
-            }
-            return;
-        }
+        __syncthreads();
     }
 }

@@ -122,7 +122,8 @@ struct YCfg {
     int thr = 256;
     int wfft = 0;  // per-term kernels: radix of the warp transform (P2 = 32 wfft), 0 = block stages
     int tp = 0;    // 1: two-pass kernels (k_inv_y2 / k_fwd_y2), BLD_Y2_NL lines, P2 = A * B;
-                   // 2: inverse pass with TMA-staged tiles (k_inv_y3), BLD_Y3_NL lines
+                   // 2: inverse pass with TMA-staged tiles (k_inv_y3), BLD_Y3_NL lines;
+                   // 3: forward two-pass kernel on 8 lines, 3 blocks per SM, 4 outputs in flight
     int zc = 1;    // tp 2: layer chunks (blocks along z)
 };
 
@@ -145,7 +146,7 @@ struct Space {
     int xwmb = 1;                                   // warp-per-row kernel: register cap (min blocks of 128 threads)
     int zmult = 2;                                  // x kernels: z-chunk count multiplier in halves (autotuned)
     int xb = 0;                                     // block of warps per row (advection): 1 three warps, 2 five (pipelined)
-    int x2 = 0;                                     // 1: two-pass shared-memory x kernel (advection, BLD_X2_NR rows)
+    int x2 = 0;                                     // 1: two-pass shared-memory x kernel (advection, x2_rows rows)
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
@@ -262,7 +263,7 @@ int pick_y(int P2, bool fp32, int sets) {
 // fill the GPU a few times over, at least 8 layers per chunk
 void x_chunks(const bld_handle* h, Space& s) {
     const int n3 = h->g.n3;
-    const int rows = s.x2 ? BLD_X2_NR : (s.xb ? 1 : (s.xw ? s.xw : s.YT));
+    const int rows = s.x2 ? x2_rows((int)csize(h->fp32)) : (s.xb ? 1 : (s.xw ? s.xw : s.YT));
     const long long blocks_per_chunk = (long long)((s.P2 + rows - 1) / rows) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
     want = std::min(want, std::max(1, n3 / 8));
@@ -356,33 +357,36 @@ bool y2_ok(int P2, bool fp32) { return y2_radix_a(P2) > 0 && (fp32 || P2 <= 288)
 size_t smem_y2(int P2, int lines, bool fp32) { return (size_t)P2 * (1 + lines) * csize(fp32); }
 
 template <typename R, int P>
-int launch_y2_p(bld_handle* h, bool inverse, const void* args, dim3 grid, size_t sm) {
+int launch_y2_p(bld_handle* h, bool inverse, const void* args, dim3 grid, size_t sm, int tp) {
     constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
     constexpr int MINB = y2_min_blocks<R>(B * BLD_Y2_NL);
-    if (inverse)
-        k_inv_y2<R, A, B, MINB><<<grid, B * BLD_Y2_NL, sm, h->stream>>>(*static_cast<const InvYArgs*>(args));
+    constexpr int MINBI = y2_min_blocks_inv<R>(B * BLD_Y2_NL);
+    if (!inverse && tp == 3)
+        k_fwd_y2<R, A, B, 3, 8, 4><<<grid, B * 8, sm, h->stream>>>(*static_cast<const FwdYArgs*>(args));
+    else if (inverse)
+        k_inv_y2<R, A, B, MINBI><<<grid, B * BLD_Y2_NL, sm, h->stream>>>(*static_cast<const InvYArgs*>(args));
     else
         k_fwd_y2<R, A, B, MINB><<<grid, B * BLD_Y2_NL, sm, h->stream>>>(*static_cast<const FwdYArgs*>(args));
     return BLD_OK;
 }
 
 template <typename R>
-int launch_y2(bld_handle* h, int P2, bool inverse, const void* args, dim3 grid, size_t sm) {
+int launch_y2(bld_handle* h, int P2, bool inverse, const void* args, dim3 grid, size_t sm, int tp = 1) {
     switch (P2) {
-        case 64: return launch_y2_p<R, 64>(h, inverse, args, grid, sm);
-        case 96: return launch_y2_p<R, 96>(h, inverse, args, grid, sm);
-        case 128: return launch_y2_p<R, 128>(h, inverse, args, grid, sm);
-        case 144: return launch_y2_p<R, 144>(h, inverse, args, grid, sm);
-        case 192: return launch_y2_p<R, 192>(h, inverse, args, grid, sm);
-        case 256: return launch_y2_p<R, 256>(h, inverse, args, grid, sm);
-        case 288: return launch_y2_p<R, 288>(h, inverse, args, grid, sm);
+        case 64: return launch_y2_p<R, 64>(h, inverse, args, grid, sm, tp);
+        case 96: return launch_y2_p<R, 96>(h, inverse, args, grid, sm, tp);
+        case 128: return launch_y2_p<R, 128>(h, inverse, args, grid, sm, tp);
+        case 144: return launch_y2_p<R, 144>(h, inverse, args, grid, sm, tp);
+        case 192: return launch_y2_p<R, 192>(h, inverse, args, grid, sm, tp);
+        case 256: return launch_y2_p<R, 256>(h, inverse, args, grid, sm, tp);
+        case 288: return launch_y2_p<R, 288>(h, inverse, args, grid, sm, tp);
         default: break;
     }
     if constexpr (sizeof(R) == 4) {
         switch (P2) {
-            case 384: return launch_y2_p<R, 384>(h, inverse, args, grid, sm);
-            case 512: return launch_y2_p<R, 512>(h, inverse, args, grid, sm);
-            case 768: return launch_y2_p<R, 768>(h, inverse, args, grid, sm);
+            case 384: return launch_y2_p<R, 384>(h, inverse, args, grid, sm, tp);
+            case 512: return launch_y2_p<R, 512>(h, inverse, args, grid, sm, tp);
+            case 768: return launch_y2_p<R, 768>(h, inverse, args, grid, sm, tp);
             default: break;
         }
     }
@@ -521,9 +525,10 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
     a.NL = c.NL;
     const size_t cs = csize(sizeof(R) == 4);
     if (c.tp) {
-        a.NL = BLD_Y2_NL;
-        dim3 grid(a.fields * nm, (h->g.K1 + BLD_Y2_NL - 1) / BLD_Y2_NL, h->g.n3);
-        BLD_TRY(launch_y2<R>(h, s.P2, false, &a, grid, smem_y2(s.P2, s.fsets * BLD_Y2_NL, sizeof(R) == 4)));
+        const int nl = c.tp == 3 ? 8 : BLD_Y2_NL;
+        a.NL = nl;
+        dim3 grid(a.fields * nm, (h->g.K1 + nl - 1) / nl, h->g.n3);
+        BLD_TRY(launch_y2<R>(h, s.P2, false, &a, grid, smem_y2(s.P2, s.fsets * nl, sizeof(R) == 4), c.tp));
         CUDA_TRY(cudaGetLastError());
         return BLD_OK;
     }
@@ -559,16 +564,17 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
 // two-pass advection x kernel: compiled for P1 with a two-pass factorisation
 // (single precision up to 768, double up to 288), whole row pairs per block
 bool x2_ok(const bld_handle* h, const Space& s) {
-    return y2_ok(s.P1, h->fp32) && s.P2 % BLD_X2_NR == 0 &&
+    return y2_ok(s.P1, h->fp32) && s.P2 % x2_rows((int)csize(h->fp32)) == 0 &&
            x2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, (int)csize(h->fp32)) <= 227 * 1024;
 }
 
 template <typename R, int P>
 int launch_x2_p(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
-    dim3 grid(s.P2 / BLD_X2_NR, s.nchunks, nm);
+    constexpr int NR = x2_rows((int)sizeof(cplx<R>));
+    dim3 grid(s.P2 / NR, s.nchunks, nm);
     const size_t sm = x2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>));
-    k_adv_x2<R, A, B><<<grid, x2_threads(B), sm, h->stream>>>(a, h->flag);
+    k_adv_x2<R, A, B><<<grid, x2_threads(B, NR), sm, h->stream>>>(a, h->flag);
     return BLD_OK;
 }
 
@@ -805,8 +811,9 @@ int set_smem_limits_R() {
     BLD_SET((k_inv_y_all<R>));
     BLD_SET((k_fwd_y_all<R>));
 #define BLD_SET_Y2(P)                                                                                  \
-    BLD_SET((k_inv_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks<R>(y2_radix_b(P) * BLD_Y2_NL)>)); \
-    BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks<R>(y2_radix_b(P) * BLD_Y2_NL)>));
+    BLD_SET((k_inv_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks_inv<R>(y2_radix_b(P) * BLD_Y2_NL)>)); \
+    BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks<R>(y2_radix_b(P) * BLD_Y2_NL)>)); \
+    BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), 3, 8, 4>));
     BLD_SET_Y2(64)
     BLD_SET_Y2(96)
     BLD_SET_Y2(128)
@@ -1142,6 +1149,11 @@ bool yforce_tma() {
     const char* e = getenv("BLD_Y_KERNEL");
     return e && !strcmp(e, "tma");
 }
+// BLD_Y_KERNEL=twopass8: the two-pass kernels with the eight-line forward pass
+bool yforce_twopass8() {
+    const char* e = getenv("BLD_Y_KERNEL");
+    return e && !strcmp(e, "twopass8");
+}
 
 // y-pass candidates: per-term blocks (two-buffer FFT) with several line counts
 // and block sizes, and all-terms blocks (in-place FFT); lines * element size of
@@ -1173,12 +1185,23 @@ std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_pe
         c.thr = y2_radix_b(s.P2) * BLD_Y2_NL;
         c.tp = 1;
         out.push_back(c);
+        if (!inverse) {   // eight lines, more blocks per SM
+            c.NL = 8;
+            c.thr = y2_radix_b(s.P2) * 8;
+            c.tp = 3;
+            out.push_back(c);
+        }
     }
-    if (tp_ok && (yforce_twopass() || (yforce_tma() && !inverse))) {
+    if (tp_ok && (yforce_twopass() || yforce_twopass8() || (yforce_tma() && !inverse))) {
         YCfg c{};
         c.NL = BLD_Y2_NL;
         c.thr = y2_radix_b(s.P2) * BLD_Y2_NL;
         c.tp = 1;
+        if (yforce_twopass8() && !inverse) {
+            c.NL = 8;
+            c.thr = y2_radix_b(s.P2) * 8;
+            c.tp = 3;
+        }
         return {c};
     }
     const size_t cs = csize(h->fp32);
@@ -1238,7 +1261,9 @@ int autotune(bld_handle* h) {
     const bool only_bw3 = xk && !strcmp(xk, "blockwarp"), only_pipe = xk && !strcmp(xk, "pipe");
     const bool only_bw = only_bw3 || only_pipe;   // a block-of-warps kernel (three warps, or five pipelined)
     const bool only_lines = xk && !strcmp(xk, "lines");   // block kernels with warp line transforms
-    const bool only_x2 = xk && !strcmp(xk, "twopass");     // the two-pass shared-memory x kernel
+    // the two-pass shared-memory x kernel (where it applies; elsewhere the other families)
+    const bool only_x2 = xk && !strcmp(xk, "twopass") && h->adv.on && x2_ok(h, h->adv);
+    const bool x2_asked = xk && !strcmp(xk, "twopass");
     const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1, h->fp32) > 0;
     if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
     const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
@@ -1361,7 +1386,7 @@ int autotune(bld_handle* h) {
             if ((xbk == 1 && only_pipe) || (xbk == 2 && only_bw3)) continue;
             BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2, 0}));
         }
-        if (sp == 0 && x2_ok(h, s) && (only_x2 || !xk)) BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1}));
+        if (sp == 0 && x2_ok(h, s) && (only_x2 || !xk || x2_asked)) BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1}));
         if (bx >= 1e30f) return fail(BLD_ERR_INVALID_CONFIG, "no x kernel could be timed");
         set_pick(bp);
         x_chunks(h, s);
@@ -2461,7 +2486,8 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         else if (s.inv.tp) snprintf(iname, sizeof iname, "k_inv_y2<%s, %d, %d>", R, y2_radix_a(s.P2), y2_radix_b(s.P2));
         else if (s.inv.all) snprintf(iname, sizeof iname, "k_inv_y_all<%s>", R);
         else snprintf(iname, sizeof iname, "k_inv_y<%s, %d>", R, s.inv.wfft);
-        if (s.fwd.tp) snprintf(fname, sizeof fname, "k_fwd_y2<%s, %d, %d>", R, y2_radix_a(s.P2), y2_radix_b(s.P2));
+        if (s.fwd.tp) snprintf(fname, sizeof fname, "k_fwd_y2<%s, %d, %d%s>", R, y2_radix_a(s.P2), y2_radix_b(s.P2),
+                               s.fwd.tp == 3 ? ", 8 lines" : "");
         else if (s.fwd.all) snprintf(fname, sizeof fname, "k_fwd_y_all<%s>", R);
         else snprintf(fname, sizeof fname, "k_fwd_y<%s, %d>", R, s.fwd.wfft);
         snprintf(tmp, sizeof tmp,

@@ -35,6 +35,11 @@ template <typename R>
 __host__ __device__ constexpr int y2_min_blocks(int threads) {
     return threads <= 256 ? (sizeof(R) == 8 ? 2 : 3) : 2;
 }
+// the inverse pass holds fewer values: single precision fits three blocks of 288
+template <typename R>
+__host__ __device__ constexpr int y2_min_blocks_inv(int threads) {
+    return sizeof(R) == 4 && threads <= 288 ? 3 : y2_min_blocks<R>(threads);
+}
 
 // spectral term `OP` of the inverse pass at mode (jj, k1) of layer z; the
 // pointers address layer z of u, v, w (Su1/Sv1: layer z + 1); same arithmetic as
@@ -141,11 +146,13 @@ __global__ void __launch_bounds__(B * BLD_Y2_NL, MINB) k_inv_y2(InvYArgs a) {
 }
 
 // grid (fields * members, ceil(K1 / NL), n3), block B * NL threads;
-// smem tw[P] + P * nlines complex (nlines = NL, or 2 NL with a D2 contribution)
-template <typename R, int A, int B, int MINB>
-__global__ void __launch_bounds__(B * BLD_Y2_NL, MINB) k_fwd_y2(FwdYArgs a) {
+// smem tw[P] + P * nlines complex (nlines = NL, or 2 NL with a D2 contribution).
+// NL = 16 lines per block, or 8 with more blocks per SM and OB = 4 outputs of
+// the epilogue in flight per thread
+template <typename R, int A, int B, int MINB, int NL = BLD_Y2_NL, int OB = 1>
+__global__ void __launch_bounds__(B * NL, MINB) k_fwd_y2(FwdYArgs a) {
     using C = cplx<R>;
-    constexpr int P = A * B, NL = BLD_Y2_NL;
+    constexpr int P = A * B;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int fi = blockIdx.x % a.fields, m = a.m0 + blockIdx.x / a.fields;
     BLD_SKIP_INACTIVE(a, m);
@@ -215,9 +222,9 @@ __global__ void __launch_bounds__(B * BLD_Y2_NL, MINB) k_fwd_y2(FwdYArgs a) {
         }
     }
     __syncthreads();
-    constexpr int nls = 4;   // log2(NL)
-    static_assert((1 << nls) == NL, "NL is a power of two");
-    fwd_y_epilogue<R, 0, 1>(a, buf, nlines, m, f, z, nz, k10, NL, nls, hasB);
+    constexpr int nls = NL == 16 ? 4 : 3;   // log2(NL)
+    static_assert((1 << nls) == NL, "NL is 8 or 16");
+    fwd_y_epilogue<R, 0, OB>(a, buf, nlines, m, f, z, nz, k10, NL, nls, hasB);
 }
 
 // ----------------------------------------------------------------------------

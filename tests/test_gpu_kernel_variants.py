@@ -91,7 +91,9 @@ def test_advection_x_kernel_family(oracle, BLD, res, precision, tol, family):
     om = _build(oracle, res)
     gm = _forced(BLD, family, res, precision)
     if family == "twopass":
-        assert gm.kernels()["advection"]["x"].startswith("k_adv_x2<"), gm.kernels()
+        # two (double) or four (single precision) y rows per block
+        if gm.info.adv_p2 % (2 if precision == "fp64" else 4) == 0:
+            assert gm.kernels()["advection"]["x"].startswith("k_adv_x2<"), gm.kernels()
     elif family != "block":
         assert gm.info.adv_p1 % 32 == 0
     st = _state(om, seed=sum(res))
@@ -210,12 +212,12 @@ Y2_SIZES_FP32 = {384, 512, 768}
 
 
 @pytest.mark.parametrize("res,precision,les,tol", Y_CASES)
-@pytest.mark.parametrize("family", ["warp", "block", "twopass", "tma"])
+@pytest.mark.parametrize("family", ["warp", "block", "twopass", "twopass8", "tma"])
 def test_y_kernel_family(oracle, BLD, res, precision, les, tol, family):
     om = _build(oracle, res, les=les)
     gm = _forced_y(BLD, family, res, precision, les)
-    if family in ("twopass", "tma"):   # the forced family is the one that runs where it is compiled
-        inv = "k_inv_y2<" if family == "twopass" else "k_inv_y3<"
+    if family in ("twopass", "twopass8", "tma"):   # the forced family is the one that runs where it is compiled
+        inv = "k_inv_y3<" if family == "tma" else "k_inv_y2<"
         for space in gm.kernels().values():
             if not isinstance(space, dict):
                 continue
@@ -224,6 +226,7 @@ def test_y_kernel_family(oracle, BLD, res, precision, les, tol, family):
                 continue
             if p2 in Y2_SIZES or (precision == "mixed" and p2 in Y2_SIZES_FP32):
                 assert space["inv_y"].startswith(inv) and space["fwd_y"].startswith("k_fwd_y2<"), space
+                assert (family == "twopass8") == space["fwd_y"].endswith(", 8 lines>"), space
     st = _state(om, seed=sum(res) + 1)
     ref = om.compute_rates(st)
     got = gm.compute_rates(st)
@@ -232,14 +235,15 @@ def test_y_kernel_family(oracle, BLD, res, precision, les, tol, family):
         assert e < tol, (res, precision, family, f, e)
 
 
+@pytest.mark.parametrize("family", ["twopass", "twopass8"])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
-def test_twopass_y_trajectory(oracle, BLD, precision, tol):
+def test_twopass_y_trajectory(oracle, BLD, precision, tol, family):
     """20 SSP-RK33 steps of an LES with both spaces on the two-pass y kernels
     (advection P2 = 96, SGS P2 = 64): the forward pass forms the fused stage
     values and the chained Euler stages, checked against the oracle."""
     res = (32, 64, 8)
     om = _build(oracle, res, les=True)
-    gm = _forced_y(BLD, "twopass", res, precision, True)
+    gm = _forced_y(BLD, family, res, precision, True)
     for space in gm.kernels().values():
         if isinstance(space, dict):
             assert space["fwd_y"].startswith("k_fwd_y2<"), space
