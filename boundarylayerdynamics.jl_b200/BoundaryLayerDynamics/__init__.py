@@ -322,6 +322,7 @@ class Model:
         info = _capi.BldInfo()
         _capi.check(self._lib.bld_get_info(h, C.byref(info)))
         self.info = info
+        self._has_sgs = bool(cfg.sgs)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -442,6 +443,8 @@ class Model:
         nt = _approxdiv(t2 - t1, dt) if t2 > t1 else 0
         self.prepare()
         for o in output:
+            if hasattr(o, "set_dt"):
+                o.set_dt(dt)
             o.start(self, t1)
         events = set()
         for o in output:
@@ -500,6 +503,35 @@ class Model:
         buf = C.create_string_buffer(4096)
         _capi.check(self._lib.bld_describe(self._h, buf, len(buf)))
         return json.loads(buf.value.decode())
+
+    def init_random_field(self, field, base, scale, distribution="uniform", seed=0, member=0):
+        """Sets ``field`` to base(x3) + scale(x3) r on the device, r uniform on [-1, 1)
+        or standard normal from the counter-based generator of ``bld_init_random_field``
+        (``workloads.seeded_field`` computes the same values on the host)."""
+        nz = self.nz(field)
+        b = np.ascontiguousarray(np.broadcast_to(np.asarray(base, float), (nz,)))
+        sc = np.ascontiguousarray(np.broadcast_to(np.asarray(scale, float), (nz,)))
+        dist = {"uniform": 0, "normal": 1}[distribution]
+        _capi.check(self._lib.bld_init_random_field(self._h, int(member), FIELDS.index(field), b.ctypes.data,
+                                                    sc.ctypes.data, dist, int(seed) & (2**64 - 1)))
+
+    def progress(self, member=0, tstep=None):
+        """The statistics ProgressMonitor reports (src/logging.jl:215-276), computed on
+        the device from the member's state, under the reference's labels:
+        "Mean Velocity", "Mean KE", "Turbulent KE", "Advective Timescale" (or
+        "Adv. Courant Number" with ``tstep``), and with a Smagorinsky wall model
+        "Wall Stress τ₁₃" / "Wall Stress τ₂₃" as (lower, upper)."""
+        p = _capi.BldProgress()
+        _capi.check(self._lib.bld_progress_stats(self._h, int(member), C.byref(p)))
+        out = {"Mean Velocity": tuple(p.mean_velocity), "Mean KE": p.mean_ke, "Turbulent KE": p.turbulent_ke}
+        if tstep is None:
+            out["Advective Timescale"] = p.advective_timescale
+        else:
+            out["Adv. Courant Number"] = tstep / p.advective_timescale
+        if self._has_sgs:
+            out["Wall Stress τ₁₃"] = (p.wall_stress[0][0], p.wall_stress[0][1])
+            out["Wall Stress τ₂₃"] = (p.wall_stress[1][0], p.wall_stress[1][1])
+        return out
 
     def diverged_members(self):
         """Members whose rates turned non-finite since the last query (clears the record)."""
@@ -589,4 +621,4 @@ def openchannelflow(Re, dims, roughness_length=None, **kw):
     return Model(dims, domain, incompressible_flow(1 / Re, **kw))
 
 
-from .output import MeanProfiles, Snapshots  # noqa: E402  (output modules for evolve)
+from .output import MeanProfiles, ProgressMonitor, Snapshots  # noqa: E402  (output modules for evolve)

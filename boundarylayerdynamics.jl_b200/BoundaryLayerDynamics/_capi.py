@@ -66,6 +66,14 @@ class BldPhaseTimes(C.Structure):
     ]
 
 
+class BldProgress(C.Structure):
+    _fields_ = [
+        ("mean_velocity", C.c_double * 3), ("mean_ke", C.c_double), ("turbulent_ke", C.c_double),
+        ("advective_timescale", C.c_double), ("wall_stress", (C.c_double * 2) * 2),
+        ("grid_p1", C.c_int32), ("grid_p2", C.c_int32),
+    ]
+
+
 # exported symbols and their signatures (every declaration of include/bld.h)
 SIGNATURES = {
     "bld_abi_version": (C.c_int32, []),
@@ -102,6 +110,9 @@ SIGNATURES = {
     "bld_prepare_member": (C.c_int32, [C.c_void_p, C.c_int32]),
     "bld_get_diverged": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "bld_describe": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "bld_progress_stats": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(BldProgress)]),
+    "bld_init_random_field": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                          C.c_uint64]),
     "bld_project_noalloc": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32] + [C.c_void_p] * 5
                             + [C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
     "bld_ldlt_solve_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),

@@ -1,4 +1,5 @@
-"""Output modules for ``evolve`` (src/logging.jl): Snapshots and MeanProfiles.
+"""Output modules for ``evolve`` (src/logging.jl): Snapshots, MeanProfiles and
+ProgressMonitor.
 
 Both work on the device-resident state.  ``Snapshots`` reads the physical fields
 back only at its output times (centered transforms run on the device) and
@@ -181,3 +182,62 @@ def initialize_from_snapshot(model, path, member=0):
         if not (np.allclose(x1, ex1) and np.allclose(x2, ex2) and np.allclose(x3, ex3)):
             raise ValueError(f"{fn}: coordinates do not match the model")
         model.set_field(field, np.asarray(data, dtype=np.float64), member=member, centered=centered)
+
+
+class ProgressMonitor:
+    """``ProgressMonitor(frequency=10, description="Progress:", tstep=None)``
+    (src/logging.jl:129-308): prints the progress and the flow statistics at
+    intervals of wall time.  The statistics come from the device-resident state
+    (``Model.progress``: mean velocity, mean and turbulent kinetic energy, the
+    advective time scale or Courant number, wall stresses); the state is checked
+    every ``check_every`` steps (the reference checks after every step, which
+    would break the multi-step device launches), and always at the end."""
+
+    def __init__(self, frequency=10, description="Progress:", tstep=None, checks=20, stream=None):
+        import sys
+        self.frequency = float(frequency)
+        self.description = description
+        self.tstep = tstep
+        self.checks = int(checks)   # times the run is split for the wall-time checks
+        self.stream = stream or sys.stdout
+        self.reports = []      # (simulation time, statistics) of every report
+        self._dt = None
+
+    def set_dt(self, dt):
+        self._dt = float(dt)
+
+    def output_times(self, t1, t2):
+        self._t1, self._t2 = t1, t2
+        if not self._dt or self.checks < 2:
+            return []
+        n = int(round((t2 - t1) / self._dt))
+        every = max(1, n // self.checks)
+        return [t1 + k * self._dt for k in range(every, n, every)]
+
+    def start(self, model, t):
+        import time
+        self._start = time.time()
+        self._last = None
+
+    def at(self, model, t, steps=0, member=0):
+        import time
+        now = time.time()
+        progress = (t - self._t1) / (self._t2 - self._t1) if self._t2 > self._t1 else 1.0
+        if self._last is not None and now - self._last < self.frequency and progress < 1:
+            return
+        self._last = now
+        stats = {"Simulation Time": t}
+        stats.update(model.progress(member=member, tstep=self.tstep))
+        self.reports.append((t, stats))
+        rate = progress / max(now - self._start, 1e-9)
+        eta = (1 - progress) / rate if rate > 0 else float("inf")
+        print(f"{self.description} {100 * progress:3.0f}%  ETA: {eta:.0f} s", file=self.stream)
+        width = max(len(k) for k in stats) + 2
+        for k, v in stats.items():
+            vals = ", ".join(f"{x:.3g}" for x in (v if isinstance(v, tuple) else (v,)))
+            print(f"{k:>{width}} ╎ {vals}", file=self.stream)
+
+    def finish(self, model, t):
+        if not self.reports or self.reports[-1][0] != t:
+            self._last = None
+            self.at(model, t)

@@ -98,6 +98,72 @@ def initial_fields(spec, seed=None):
     return u, v, w
 
 
+# ----------------------------------------------------------- seeded fields on the device
+_GAMMA = np.uint64(0x9E3779B97F4A7C15)
+
+
+def splitmix64(x):
+    """SplitMix64's output function (Steele, Lea and Flood, OOPSLA 2014) of uint64 x,
+    elementwise, with 64-bit wraparound: the generator of bld_init_random_field."""
+    x = np.asarray(x, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        x = x + _GAMMA
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def seeded_field(shape, base, scale, distribution, seed, field):
+    """The values bld_init_random_field puts on the default grid: base[z] + scale[z] r
+    with r uniform on [-1, 1) or standard normal, counter i = (z P2 + y) P1 + x."""
+    nz, P2, P1 = shape
+    with np.errstate(over="ignore"):
+        key = splitmix64(np.uint64(seed)) ^ splitmix64(np.uint64(field + 1))
+        i = np.arange(nz * P2 * P1, dtype=np.uint64)
+        u = (splitmix64(key + np.uint64(2) * i) >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+        if distribution == "uniform":
+            r = 2.0 * u - 1.0
+        else:
+            u2 = (splitmix64(key + np.uint64(2) * i + np.uint64(1)) >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+            r = np.sqrt(-2.0 * np.log(1.0 - u)) * np.cos(2.0 * np.pi * u2)
+    r = r.reshape(nz, P2, P1)
+    return np.asarray(base, float)[:, None, None] + np.asarray(scale, float)[:, None, None] * r
+
+
+def seeded_profiles(spec):
+    """(base, scale, distribution) per field of the workload's initial condition in
+    the form the device generator takes: LES u = p (1 + 0.1 r), v = 0.1 p r,
+    w = 0.1 p_I r with p = (u*/kappa) ln(z/z0) and r uniform on [-1, 1); DNS
+    u = U_c (1 - (z - 1)^2) + sigma n, v = sigma n, w = sigma n with
+    sigma = 0.05 U_c and n standard normal."""
+    _, _, x3c, x3i = default_grid(spec)
+    if spec["kind"] == "les":
+        z0 = spec["lower"][1]
+        pc, pi = np.log(x3c / z0) / KAPPA, np.log(x3i / z0) / KAPPA
+        return {"vel1": (pc, 0.1 * pc, "uniform"), "vel2": (0 * pc, 0.1 * pc, "uniform"),
+                "vel3": (0 * pi, 0.1 * pi, "uniform")}
+    sig = 0.05 * DNS_UC
+    return {"vel1": (DNS_UC * (1 - (x3c - 1) ** 2), sig + 0 * x3c, "normal"),
+            "vel2": (0 * x3c, sig + 0 * x3c, "normal"), "vel3": (0 * x3i, sig + 0 * x3i, "normal")}
+
+
+def seeded_initial_fields(spec, seed):
+    """Host copies of the fields initialize_on_device builds (u, v, w on the default grid)."""
+    x1, x2, x3c, x3i = default_grid(spec)
+    P1, P2 = len(x1), len(x2)
+    out = []
+    for k, (f, (b, sc, dist)) in enumerate(seeded_profiles(spec).items()):
+        nz = len(x3c) if f != "vel3" else len(x3i)
+        out.append(seeded_field((nz, P2, P1), b, sc, dist, seed, k))
+    return tuple(out)
+
+
+def initialize_on_device(spec, model, seed, member=0):
+    """initialize! with the workload's seeded initial condition generated on the device."""
+    for f, (b, sc, dist) in seeded_profiles(spec).items():
+        model.init_random_field(f, b, sc, dist, seed, member)
+
+
 def ensemble_members(seed=3):
     """The 64-member uneven ensemble: 24 x 64^2x32, 24 x 96^2x48, 16 x 128^2x64 with
     z0 ~ logU[1e-5, 1e-3] and Cs ~ U[0.08, 0.16] per member."""

@@ -192,6 +192,10 @@ struct bld_handle {
     int Pd1 = 0, Pd2 = 0;
     void* pd_buf = nullptr;     // double [nz][Pd2][Pd1]
     void* pd_mixed = nullptr;   // double2 [nz][Pd2][K1]
+    // progress statistics (allocated by the first bld_progress_stats call)
+    double* prog_small = nullptr;  // per-layer sums and maxima
+    void* prog_buf = nullptr;      // double [n3][P2][P1] at the largest physical size
+    void* prog_mixed = nullptr;    // double2 [n3][P2][K1]
     // host-side copies used by launches
     double w_lo = 0, w_hi = 0;
     int dyn_lo = 0, dyn_hi = 0;
@@ -1827,7 +1831,8 @@ void free_handle(bld_handle* h) {
     for (auto& kv : h->ens_graphs) cudaGraphExecDestroy(kv.second);
     void* ptrs[] = {h->u, h->t, h->du, h->dp, h->io, h->io2, h->pscr, h->gamma, h->d1, h->d2, h->DD1, h->DD2,
                     h->alpha_c, h->alpha_i, h->alpha_ext, h->mean_w, h->lc2, h->li2, h->wall, h->src,
-                    h->mean_val, h->flag, h->active, h->adv.min, h->adv.mout, h->sgs.min, h->sgs.mout, h->pd_buf, h->pd_mixed};
+                    h->mean_val, h->flag, h->active, h->adv.min, h->adv.mout, h->sgs.min, h->sgs.mout, h->pd_buf, h->pd_mixed,
+                    h->prog_small, h->prog_buf, h->prog_mixed};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& kv : h->tw) {
@@ -2528,14 +2533,13 @@ int32_t bld_prepare_member(bld_handle* h, int32_t m) {
     return check_flag(h);
 }
 
-int32_t bld_set_field_physical(bld_handle* h, int32_t m, int32_t field, const double* values) {
-    if (!member_ok(h, m) || field < 0 || field > 2 || !values) return fail(BLD_ERR_ARGUMENT, "invalid argument");
-    if (!h->pd_buf) return fail(BLD_ERR_INVALID_CONFIG, "default physical size is not an even 2^a*3^b");
-    CUDA_TRY(cudaSetDevice(h->device));
+// set_field! of `field` of member m from the physical values already in
+// h->pd_buf (default size): r2c rows, then the forward y pass assigning the
+// truncated modes (src/physical_space.jl:253-256).  Stream-ordered.
+static int set_field_from_pd(bld_handle* h, int m, int field) {
     const Geo& g = h->g;
     const int nz = field == 2 ? g.n3 - 1 : g.n3;
     const int P1 = h->Pd1, P2 = h->Pd2;
-    CUDA_TRY(cudaMemcpyAsync(h->pd_buf, values, (size_t)nz * P2 * P1 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     XPlainArgs xa{};
     xa.P1 = P1;
     xa.P2 = P2;
@@ -2549,7 +2553,6 @@ int32_t bld_set_field_physical(bld_handle* h, int32_t m, int32_t field, const do
     const long long rows = (long long)nz * P2;
     k_x_r2c<<<(unsigned)((rows + 1) / 2), 256, (size_t)3 * P1 * sizeof(double2), h->stream>>>(xa);
     CUDA_TRY(cudaGetLastError());
-    // forward y pass, assigning the truncated modes (set_field!, src/physical_space.jl:253-256)
     Space s{};
     s.P1 = P1;
     s.P2 = P2;
@@ -2574,18 +2577,53 @@ int32_t bld_set_field_physical(bld_handle* h, int32_t m, int32_t field, const do
     fa.plan = make_plan(P2);
     fa.tw = twp(h, P2, false);
     BLD_TRY(launch_fwd_y<double>(h, s, fa, 1));
-    CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->slope_valid = false;
     return BLD_OK;
 }
 
-int32_t bld_get_field_physical(bld_handle* h, int32_t m, int32_t field, double* values) {
+int32_t bld_set_field_physical(bld_handle* h, int32_t m, int32_t field, const double* values) {
     if (!member_ok(h, m) || field < 0 || field > 2 || !values) return fail(BLD_ERR_ARGUMENT, "invalid argument");
     if (!h->pd_buf) return fail(BLD_ERR_INVALID_CONFIG, "default physical size is not an even 2^a*3^b");
     CUDA_TRY(cudaSetDevice(h->device));
+    const int nz = field == 2 ? h->g.n3 - 1 : h->g.n3;
+    CUDA_TRY(cudaMemcpyAsync(h->pd_buf, values, (size_t)nz * h->Pd2 * h->Pd1 * sizeof(double), cudaMemcpyHostToDevice,
+                             h->stream));
+    BLD_TRY(set_field_from_pd(h, m, field));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
+}
+
+int32_t bld_init_random_field(bld_handle* h, int32_t m, int32_t field, const double* base, const double* scale,
+                              int32_t distribution, uint64_t seed) {
+    if (!member_ok(h, m) || field < 0 || field > 2 || !base || !scale || distribution < 0 || distribution > 1)
+        return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    if (!h->pd_buf) return fail(BLD_ERR_INVALID_CONFIG, "default physical size is not an even 2^a*3^b");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int nz = field == 2 ? h->g.n3 - 1 : h->g.n3;
+    // the per-layer tables travel in the kernel's argument buffer (no allocation):
+    // at most BLD_INIT_MAX_LAYERS layers
+    if (nz > BLD_INIT_MAX_LAYERS) return fail(BLD_ERR_INVALID_CONFIG, "more than %d layers", BLD_INIT_MAX_LAYERS);
+    InitTables t{};
+    for (int z = 0; z < nz; ++z) {
+        t.base[z] = base[z];
+        t.scale[z] = scale[z];
+    }
+    const long long n = (long long)nz * h->Pd2 * h->Pd1;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+    k_init_random<<<blocks, 256, 0, h->stream>>>((double*)h->pd_buf, h->Pd1 * h->Pd2, nz, t, distribution,
+                                                  init_key(seed, field));
+    CUDA_TRY(cudaGetLastError());
+    BLD_TRY(set_field_from_pd(h, m, field));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
+}
+
+// The physical values of `field` of member m on the P1 x P2 grid (inverse y pass
+// and c2r rows with the block-Stockham kernels of the default-size transforms)
+// into out [nz][P2][P1]; `mixed` holds nz P2 K1 complex values.  Stream-ordered.
+static int physical_field_dev(bld_handle* h, int m, int field, int P1, int P2, double2* mixed, double* out) {
     const Geo& g = h->g;
     const int nz = field == 2 ? g.n3 - 1 : g.n3;
-    const int P1 = h->Pd1, P2 = h->Pd2;
     Space s{};
     s.P1 = P1;
     s.P2 = P2;
@@ -2599,7 +2637,7 @@ int32_t bld_get_field_physical(bld_handle* h, int32_t m, int32_t field, double* 
     ia.isI[0] = field == 2;
     ia.m0 = m;
     ia.state = h->u;
-    ia.mixed = h->pd_mixed;
+    ia.mixed = mixed;
     ia.mixed_mstride = 0;
     ia.d1 = h->d1;
     ia.d2 = h->d2;
@@ -2613,15 +2651,99 @@ int32_t bld_get_field_physical(bld_handle* h, int32_t m, int32_t field, double* 
     xa.K1 = g.K1;
     xa.k1max = g.k1max;
     xa.nz = nz;
-    xa.pd_out = (double*)h->pd_buf;
-    xa.mixed_in = (const double2*)h->pd_mixed;
+    xa.pd_out = out;
+    xa.mixed_in = mixed;
     xa.plan = make_plan(P1);
     xa.tw = (const double2*)twp(h, P1, false);
     const long long rows = (long long)nz * P2;
     k_x_c2r<<<(unsigned)((rows + 1) / 2), 256, (size_t)3 * P1 * sizeof(double2), h->stream>>>(xa);
     CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
+int32_t bld_get_field_physical(bld_handle* h, int32_t m, int32_t field, double* values) {
+    if (!member_ok(h, m) || field < 0 || field > 2 || !values) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    if (!h->pd_buf) return fail(BLD_ERR_INVALID_CONFIG, "default physical size is not an even 2^a*3^b");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int nz = field == 2 ? h->g.n3 - 1 : h->g.n3;
+    const int P1 = h->Pd1, P2 = h->Pd2;
+    BLD_TRY(physical_field_dev(h, m, field, P1, P2, (double2*)h->pd_mixed, (double*)h->pd_buf));
     CUDA_TRY(cudaMemcpyAsync(values, h->pd_buf, (size_t)nz * P2 * P1 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BLD_OK;
+}
+
+int32_t bld_progress_stats(bld_handle* h, int32_t m, bld_progress* out) {
+    if (!member_ok(h, m) || !out) return fail(BLD_ERR_ARGUMENT, "invalid argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const Geo& g = h->g;
+    const int n3 = g.n3;
+    // the largest physical grid of the model: advection, else SGS, else the default size
+    const Space* big = h->adv.on ? &h->adv : (h->sgs.on ? &h->sgs : nullptr);
+    const int P1 = big ? big->P1 : h->Pd1, P2 = big ? big->P2 : h->Pd2;
+    if (!big && !h->pd_buf) return fail(BLD_ERR_INVALID_CONFIG, "default physical size is not an even 2^a*3^b");
+    const int nsmall = 6 * n3 + n3 + 4;
+    // prog_buf holds w on the largest grid, later u and v on the SGS grid
+    const size_t buf_doubles = (size_t)n3 * std::max((size_t)P2 * P1, h->sgs.on ? 2 * (size_t)h->sgs.P1 * h->sgs.P2 : 0);
+    if (!h->prog_small) {
+        BLD_TRY(dalloc(h, (void**)&h->prog_small, nsmall * sizeof(double)));
+        BLD_TRY(dalloc(h, &h->prog_buf, buf_doubles * sizeof(double)));
+        BLD_TRY(dalloc(h, &h->prog_mixed, (size_t)n3 * P2 * g.K1 * sizeof(double2)));
+    }
+    CUDA_TRY(cudaMemsetAsync(h->prog_small, 0, nsmall * sizeof(double), h->stream));
+    k_progress_modes<<<dim3(n3, 3), 256, 0, h->stream>>>(g, h->u + (size_t)m * g.mstride, h->prog_small);
+    CUDA_TRY(cudaGetLastError());
+    BLD_TRY(physical_field_dev(h, m, 2, P1, P2, (double2*)h->prog_mixed, (double*)h->prog_buf));
+    k_layer_absmax<<<n3 - 1, 256, 0, h->stream>>>((const double*)h->prog_buf, (long long)P1 * P2, h->prog_small + 6 * n3);
+    CUDA_TRY(cudaGetLastError());
+    // wall-model stresses at the rough walls, from u and v on the SGS grid
+    double wall4[4] = {0, 0, 0, 0};
+    const bool wall = h->sgs.on && (h->dyn_lo || h->dyn_hi);
+    if (wall) {
+        const int S1 = h->sgs.P1, S2 = h->sgs.P2;
+        std::vector<double> lc(n3), li(n3);
+        member_sgs_tables(h, h->member_cs[m], h->member_z0[m], lc.data(), li.data(), wall4);
+        double* bu = (double*)h->prog_buf;   // u, then v behind it
+        double2* mx = (double2*)h->prog_mixed;
+        const long long lay = (long long)S1 * S2;
+        BLD_TRY(physical_field_dev(h, m, 0, S1, S2, mx, bu));
+        BLD_TRY(physical_field_dev(h, m, 1, S1, S2, mx, bu + (long long)n3 * lay));
+        if (h->dyn_lo)
+            k_wall_stress_mean<<<1, 256, 0, h->stream>>>(bu, bu + (long long)n3 * lay, lay, wall4[2], h->prog_small + 7 * n3);
+        if (h->dyn_hi)
+            k_wall_stress_mean<<<1, 256, 0, h->stream>>>(bu + (long long)(n3 - 1) * lay, bu + (long long)(2 * n3 - 1) * lay,
+                                                        lay, wall4[3], h->prog_small + 7 * n3 + 2);
+        CUDA_TRY(cudaGetLastError());
+    }
+    std::vector<double> r(nsmall);
+    CUDA_TRY(cudaMemcpyAsync(r.data(), h->prog_small, nsmall * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const double L3 = h->cfg.x3_max - h->cfg.x3_min;
+    *out = bld_progress{};
+    double mke = 0, ke = 0, dtmin = INFINITY;
+    for (int z = 0; z < n3; ++z) {
+        const double wc = h->tab_dx3c[z] / n3 / L3;   // cweight = dx3(zeta_C) / (n3 L3)
+        const double mu = r[(0 * n3 + z) * 2], mv = r[(1 * n3 + z) * 2];
+        out->mean_velocity[0] += mu * wc;
+        out->mean_velocity[1] += mv * wc;
+        mke += mu * mu + mv * mv;
+        ke += r[(0 * n3 + z) * 2 + 1] + r[(1 * n3 + z) * 2 + 1];
+    }
+    for (int z = 0; z < n3 - 1; ++z) {
+        const double dxi = h->tab_dx3i[z + 1] / n3;   // interior I node zeta = (z + 1) / n3
+        out->mean_velocity[2] += r[(2 * n3 + z) * 2] * dxi / L3;
+        const double mw = r[6 * n3 + z];
+        dtmin = std::min(dtmin, mw > 0 ? dxi / mw : INFINITY);
+    }
+    out->mean_ke = mke;
+    out->turbulent_ke = ke - mke;
+    out->advective_timescale = dtmin;
+    out->wall_stress[0][0] = r[7 * n3 + 0];
+    out->wall_stress[1][0] = r[7 * n3 + 1];
+    out->wall_stress[0][1] = r[7 * n3 + 2];
+    out->wall_stress[1][1] = r[7 * n3 + 3];
+    out->grid_p1 = P1;
+    out->grid_p2 = P2;
     return BLD_OK;
 }
 

@@ -2143,3 +2143,122 @@ __global__ void __launch_bounds__(128) k_profile_sample(Geo g, const double2* __
 }
 
 #include "bld_ypass2.cuh"
+
+// ------------------------------------------------------------ progress statistics
+// Horizontal statistics of one member's spectral state per (field, layer): the
+// mean Re q(0,0) and the mean square over the physical plane by Parseval,
+// sum |q|^2 with the modes k1 > 0 counted twice (their conjugates are not
+// stored); the physical grids that sample a field band-limited to |k| <= kmax
+// hold at least 2 kmax + 1 points, so both are exact (ProgressMonitor,
+// src/logging.jl:246-266).  grid (n3, 3), block 256; out[(f n3 + z) 2 + {0,1}].
+__global__ void __launch_bounds__(256) k_progress_modes(Geo g, const double2* __restrict__ S, double* out) {
+    const int z = blockIdx.x, f = blockIdx.y;
+    if (f == 2 && z >= g.n3 - 1) return;
+    const double2* L = S + fld_off(g, f) + (long long)z * g.F;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < g.F; i += blockDim.x) {
+        const double2 q = L[i];
+        const int k1 = i % g.K1;
+        s += (k1 == 0 ? 1.0 : 2.0) * (q.x * q.x + q.y * q.y);
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[(f * g.n3 + z) * 2 + 0] = L[0].x;
+        out[(f * g.n3 + z) * 2 + 1] = red[0];
+    }
+}
+
+// max |v| over each of `nz` physical layers of n points; grid nz, block 256
+__global__ void __launch_bounds__(256) k_layer_absmax(const double* __restrict__ v, long long n, double* out) {
+    const double* L = v + (long long)blockIdx.x * n;
+    double mx = 0.0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, fabs(L[i]));
+    __shared__ double red[256];
+    red[threadIdx.x] = mx;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
+// Horizontal means of the wall-model stresses factor u_i sqrt(u_1^2 + u_2^2)
+// over one physical layer of n points of u_1 (pu) and u_2 (pv)
+// (stress_bc, src/processes/static_smagorinsky.jl:195-200; hmean,
+// src/logging.jl:411-413).  One block of 256; out[0] tau13, out[1] tau23.
+__global__ void __launch_bounds__(256) k_wall_stress_mean(const double* __restrict__ pu, const double* __restrict__ pv,
+                                                          long long n, double factor, double* out) {
+    double s1 = 0.0, s2 = 0.0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        const double u = pu[i], v = pv[i];
+        const double sp = sqrt(u * u + v * v);
+        s1 += factor * u * sp;
+        s2 += factor * v * sp;
+    }
+    __shared__ double r1[256], r2[256];
+    r1[threadIdx.x] = s1;
+    r2[threadIdx.x] = s2;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            r1[threadIdx.x] += r1[threadIdx.x + w];
+            r2[threadIdx.x] += r2[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = r1[0] / (double)n;
+        out[1] = r2[0] / (double)n;
+    }
+}
+
+// ----------------------------------------------------------- seeded initial fields
+// Counter-based random numbers: the SplitMix64 output function (Steele, Lea and
+// Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014) of a
+// key plus a counter, so that any point's variate is computed independently
+// and the host (numpy) produces the same bits.
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+// the stream key of one field: splitmix64(seed) xor splitmix64(field + 1)
+__host__ __device__ __forceinline__ uint64_t init_key(uint64_t seed, int field) {
+    return splitmix64(seed) ^ splitmix64((uint64_t)field + 1);
+}
+
+#define BLD_INIT_MAX_LAYERS 512
+struct InitTables {
+    double base[BLD_INIT_MAX_LAYERS];
+    double scale[BLD_INIT_MAX_LAYERS];
+};
+
+// physical values base[z] + scale[z] r at the nz x plane points of the default
+// grid (index i = z plane + y P1 + x); r uniform on [-1, 1) (distribution 0:
+// 2 u - 1 with u = (splitmix64(key + 2 i) >> 11) 2^-53) or standard normal
+// (distribution 1: Box-Muller, sqrt(-2 log(1 - u)) cos(2 pi u') with u' from
+// key + 2 i + 1).  Grid-stride loop.
+__global__ void __launch_bounds__(256) k_init_random(double* __restrict__ pd, int plane, int nz, InitTables t,
+                                                     int distribution, uint64_t key) {
+    const long long n = (long long)nz * plane;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int z = (int)(i / plane);
+        const double u = (double)(splitmix64(key + 2ull * (uint64_t)i) >> 11) * 0x1.0p-53;
+        double r;
+        if (distribution == 0) {
+            r = 2.0 * u - 1.0;
+        } else {
+            const double u2 = (double)(splitmix64(key + 2ull * (uint64_t)i + 1ull) >> 11) * 0x1.0p-53;
+            r = sqrt(-2.0 * log(1.0 - u)) * cospi(2.0 * u2);
+        }
+        pd[i] = __dadd_rn(t.base[z], __dmul_rn(t.scale[z], r));   // rounded like the host's base + scale * r
+    }
+}

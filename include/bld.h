@@ -236,6 +236,20 @@ int32_t bld_get_field_physical(bld_handle* h, int32_t member, int32_t field, dou
 int32_t bld_get_field_centered(bld_handle* h, int32_t member, int32_t field, double* values);
 int32_t bld_set_field_centered(bld_handle* h, int32_t member, int32_t field, const double* values);
 
+/* Seeded initial condition generated on the device: initialize!(model; vel =
+   f) (src/State.jl:11-31, set_field! src/physical_space.jl:253-275) for the
+   fields f(x1, x2, x3) = base(x3) + scale(x3) r(x1, x2, x3) of the benchmark
+   workloads (a mean profile with uniform or Gaussian perturbations), without
+   building the physical field on the host.  `base` and `scale` are host arrays
+   of the field's nz layers (nz <= 512); r is uniform on [-1, 1) (distribution
+   0) or standard normal (1, Box-Muller), drawn from the SplitMix64 output
+   function of key + counter with key = splitmix64(seed) ^ splitmix64(field +
+   1) and counter 2 i (and 2 i + 1 for the second Box-Muller draw), i = (z P2 +
+   y) P1 + x on the default grid, so a host can reproduce every value.  The
+   physical values go through the forward transforms as in bld_set_field_physical. */
+int32_t bld_init_random_field(bld_handle* h, int32_t member, int32_t field, const double* base, const double* scale,
+                              int32_t distribution, uint64_t seed);
+
 /* Mean profiles accumulated on the device (MeanProfiles, src/logging.jl:333-491).
    The horizontal mean of a frequency-space field is the real part of its (0,0)
    mode.  bld_profiles_start(h, 1) zeroes the time integrals and records the
@@ -251,6 +265,30 @@ int32_t bld_set_field_centered(bld_handle* h, int32_t member, int32_t field, con
 int32_t bld_profiles_start(bld_handle* h, int32_t on);
 int32_t bld_profiles_read(bld_handle* h, int32_t member, double* out);
 int32_t bld_profiles_sample(bld_handle* h, int32_t member, double* out);
+
+/* The statistics ProgressMonitor prints (src/logging.jl:215-276), from one
+   member's device-resident state:
+   - mean_velocity: sum over layers of Re q(0,0) weighted by dx3 / L3 (vel1,
+     vel2 on the C nodes, vel3 on the interior I nodes);
+   - mean_ke / turbulent_ke: sum over the C layers of <u>^2 + <v>^2 and of
+     <u^2 + v^2> - <u>^2 - <v>^2 (horizontal means; by Parseval from the modes,
+     as exact as on the physical grids);
+   - advective_timescale: min over the I layers of dx3 / max |w|, with max |w|
+     over the largest physical grid of the model (grid_p1 x grid_p2; +inf
+     where w vanishes); the Courant number is dt / advective_timescale;
+   - wall_stress[i][side]: horizontal mean of the wall-model stress tau_i3 =
+     factor u_i sqrt(u_1^2 + u_2^2) at the first C layer next to a rough wall
+     (lower, upper), on the Smagorinsky grid (src/processes/static_smagorinsky.jl:
+     195-200); 0 elsewhere.
+   The first call allocates the handle's scratch for the physical fields. */
+typedef struct {
+    double mean_velocity[3];
+    double mean_ke, turbulent_ke;
+    double advective_timescale;
+    double wall_stress[2][2];
+    int32_t grid_p1, grid_p2;
+} bld_progress;
+int32_t bld_progress_stats(bld_handle* h, int32_t member, bld_progress* out);
 
 /* Standalone batched symmetric tridiagonal solve (the kernel of
    ldiv!(::DistributedBatchLDLt, b), src/processes/pressure.jl:106-201):

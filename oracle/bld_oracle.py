@@ -40,7 +40,7 @@ __all__ = [
     "CustomBoundary", "MomentumAdvection", "MolecularDiffusion", "Pressure", "ConstantSource",
     "ConstantMean", "StaticSmagorinskyModel", "Model", "incompressible_flow", "pdsize",
     "Transform2D", "ODEProblem", "solve", "Euler", "AB2", "SSPRK22", "SSPRK33",
-    "set_fft_workers", "DivergenceError",
+    "set_fft_workers", "DivergenceError", "progress_stats",
 ]
 
 
@@ -425,6 +425,62 @@ class MeanProfiles:
     def averages(self):                                                 # :461-467
         dt = self.timespan[1] - self.timespan[0]
         return {f: v / dt for f, v in self.means.items()}
+
+
+def progress_stats(model, state=None, tstep=None):
+    """The statistics ProgressMonitor prints (src/logging.jl:215-266), from the
+    state of ``model``: "Mean Velocity" (log_state! for the NamedTuple state,
+    :240-247), "Mean KE" / "Turbulent KE" and the advective time scale (or Courant
+    number) from the physical fields of the largest physical-domain size
+    (log_state! for the Dict of physical fields, :249-276, ``largest`` :206-211),
+    and the mean wall-model stresses of the SGS model (log_sample!, :230-237;
+    stress_bc, src/processes/static_smagorinsky.jl:195-200; hmean,
+    src/logging.jl:411-413)."""
+    state = model.state if state is None else state
+    g, dom = model.grid, model.domain
+    n = g.n3global
+    L3 = dom.size3()
+    dzeta = Fraction(1, n)
+    dx3c = np.array([float(dzeta) * dom.Dvmap(z) for z in g.vrange("C")])       # :164-165
+    dx3i = np.array([float(dzeta) * dom.Dvmap(z) for z in g.vrange("I")])
+    out = {"Mean Velocity": tuple(float(np.sum(np.real(state[f][:, 0, 0]) * w / L3))
+                                  for f, w in (("vel1", dx3c), ("vel2", dx3c), ("vel3", dx3i)))}
+    dims = []
+    for p in model.processes:
+        if isinstance(p, (_DiscretizedAdvection, _DiscretizedSmagorinsky)):
+            dims.append(tuple(p.dims))
+    big = max(dims) if dims else pdsize(g)
+    tf = model.transform(big)
+    u, v, w = (tf.get_field(state[f]) for f in ("vel1", "vel2", "vel3"))
+    ub, vb = u.mean(axis=(1, 2)), v.mean(axis=(1, 2))
+    mke = ub ** 2 + vb ** 2
+    ke = (u ** 2).mean(axis=(1, 2)) + (v ** 2).mean(axis=(1, 2))
+    out["Mean KE"] = float(np.sum(mke))
+    out["Turbulent KE"] = float(np.sum(ke - mke))
+    wmax = np.abs(w).max(axis=(1, 2))
+    with np.errstate(divide="ignore"):
+        dtmin = float(np.min(dx3i / wmax)) if len(wmax) else math.inf
+    if tstep is None:
+        out["Advective Timescale"] = dtmin
+    else:
+        out["Adv. Courant Number"] = tstep / dtmin
+    for p in model.processes:
+        if isinstance(p, _DiscretizedSmagorinsky):
+            ts = model.transform(tuple(p.dims))
+            us, vs = ts.get_field(state["vel1"]), ts.get_field(state["vel2"])
+            taus = []
+            for i in (0, 1):
+                vals = []
+                for side, layer in ((0, 0), (1, -1)):
+                    if p.wall_dynamic[side]:
+                        uu, vv = us[layer], vs[layer]
+                        vel = uu if i == 0 else vv
+                        vals.append(float(np.mean(p.factors_stress[side] * vel * np.sqrt(uu ** 2 + vv ** 2))))
+                    else:
+                        vals.append(0.0)                                # ConstantValue(0) at a free-slip wall
+                taus.append(tuple(vals))
+            out["Wall Stress τ₁₃"], out["Wall Stress τ₂₃"] = taus
+    return out
 
 
 def h1range(P, centered=False):                                         # src/physical_space.jl:64-65

@@ -136,3 +136,31 @@ def test_mean_profiles_oracle_trapezoid(oracle):
     avg = mp.averages()
     assert np.allclose(avg["vel1"], [1, 2, 3, 4]) and np.allclose(avg["vel3"], [0, 5, 6, 7, 0])
     assert mp.intervals == 5
+
+
+def test_progress_monitor_checks_and_reports():
+    """ProgressMonitor's host logic with a fake model: the check times fall on
+    whole steps, reports follow the wall-time interval and the last one comes
+    at the end time (src/logging.jl:175-191)."""
+    import io
+    import BoundaryLayerDynamics.output as out
+
+    class Fake:
+        def progress(self, member=0, tstep=None):
+            return {"Mean Velocity": (1.0, 0.0, 0.0), "Mean KE": 0.5, "Turbulent KE": 0.1,
+                    "Adv. Courant Number": 0.2}
+
+    buf = io.StringIO()
+    pm = out.ProgressMonitor(frequency=1e9, tstep=0.1, checks=5, stream=buf)
+    pm.set_dt(0.1)
+    times = pm.output_times(0.0, 2.0)
+    assert times == pytest.approx([0.4, 0.8, 1.2, 1.6])
+    model = Fake()
+    pm.start(model, 0.0)
+    for t in times:
+        pm.at(model, t)
+    pm.finish(model, 2.0)
+    # the first check reports, the others fall inside the (huge) wall-time interval,
+    # the end always reports
+    assert [t for t, _ in pm.reports] == pytest.approx([0.4, 2.0])
+    assert "Turbulent KE" in buf.getvalue()
