@@ -33,10 +33,8 @@ METRIC = "grid-pt updates/s (plain FP64 vs mixed) @192^2x96"
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the x-pass
 # kernel the autotuner picks at 192^2x96, from one ncu capture of a step
 # (profiles/step_kernels_dns192_fp64.md, profiles/step_kernels_dns192_mixed.md)
-TRAFFIC = {("dns192", "k_adv_xb<double, 9>"): (258.7 + 94.14) * 1e6,
-           ("dns192", "k_adv_xp<double, 9>"): (255.0 + 97.5) * 1e6,
-           ("dns192", "k_adv_xwc<float, 9, 3>"): (133.4 + 33.06) * 1e6,
-           ("dns192", "k_adv_xw<float, 9>"): (130.8 + 36.81) * 1e6}
+TRAFFIC = {("dns192", "k_adv_x2<double, 16, 18>"): (254.1 + 95.65) * 1e6,
+           ("dns192", "k_adv_x2<float, 16, 18>"): (127.4 + 36.42) * 1e6}
 TRAFFIC_SOURCE = "ncu capture of one step in profiles/ (a fixed figure, not measured in this run)"
 UNIT = "grid-pt updates/s"
 # the workload both arms report under "config" (identical dicts); how the engine
@@ -60,7 +58,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the ensemble, serving, tridiagonal and LES lines (run at N=1 only)")
     ap.add_argument("--only", default="", help="comma list of extras to run (ensemble,serving,tridiag,les64,les512)")
-    ap.add_argument("--serve-budget-gb", type=float, default=48.0, help="HBM budget of the served stream")
+    ap.add_argument("--serve-budget-gb", type=float, default=16.0, help="HBM budget of the served stream")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="target length of the served stream")
     ap.add_argument("--profile", action="store_true",
                     help="profiler mode: set up the workload, then run --profile-steps steps between "
@@ -442,17 +440,21 @@ def run_ensemble(steps, warmup, local):
 def run_serving(budget_gb, seconds, local):
     """Served stream: Poisson arrivals at 80% of the measured batched capacity,
     sizes {64^2x32, 128^2x64, 192^2x96, 256^2x128} with p {0.4, 0.3, 0.2, 0.1},
-    500 SSPRK33 steps each, seeded z0 and forcing; admission by HBM budget."""
+    500 SSPRK33 steps each, seeded z0 and forcing; pools are created and released
+    against the HBM budget as requests come and go (admission by free HBM), and
+    every request's initial field is generated on the device at admission."""
     from BoundaryLayerDynamics import serving as S
-    srv = S.Server.create(int(budget_gb * 2**30), precision="mixed", device=local, tick=10)
-    rate, per_req = S.calibrate_rate(srv, steps=500, load=0.8)
-    n = int(min(64, max(16, round(rate * seconds))))      # initial fields are made before the stream starts
-    reqs = S.make_requests(n, rate, seed=2024, steps=500)
+    srv = S.ElasticServer.create(int(budget_gb * 2**30), precision="mixed", device=local, tick=10)
+    rate, per_req = S.calibrate_rate_elastic(srv, steps=500, load=0.8)
+    n = int(min(64, max(16, round(rate * seconds))))
+    reqs = S.make_requests(n, rate, seed=2024, steps=500, materialize=False)
     st = srv.run(reqs)
     st.update({
         "workload": "served LES stream: sizes 64^2x32/128^2x64/192^2x96/256^2x128 (p .4/.3/.2/.1), "
                     "500 SSPRK33 steps each, z0 ~ logU[1e-5,1e-3], forcing ~ U[0.5,1.5]",
         "dtype": "f32 transforms/products, f64 state+pressure",
+        "admission": "pools created on demand and released when idle against the HBM budget; "
+                     "initial fields generated on the device at admission",
         "arrival_rate_per_s": rate, "load": 0.8,
         "service_s_per_request_at_full_pool": {f"{s[0]}^2x{s[1]}": v for s, v in per_req.items()},
         "unit_latency": "s", "unit": UNIT, "tick_steps": 10,

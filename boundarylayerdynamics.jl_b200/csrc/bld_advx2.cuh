@@ -22,24 +22,26 @@
 
 #include "bld_tma.cuh"
 
-// y rows per block: 2 in double precision, 4 in single (shared memory per block)
-__host__ __device__ constexpr int x2_rows(int csz) { return csz == 16 ? 2 : 4; }
+// y rows per block: 2 in double precision, 4 in single up to P1 = 384 (shared
+// memory per block)
+__host__ __device__ constexpr int x2_rows(int csz, int P) { return csz == 16 || P > 384 ? 2 : 4; }
 __host__ __device__ constexpr int x2_threads(int B, int NR) { return (3 * NR * B + 31) / 32 * 32; }
 __host__ __device__ constexpr int x2_al(int b) { return (b + 127) / 128 * 128; }
 // dynamic shared memory: barriers, twiddles, 2 stages x 6 terms x NR rows,
 // pass-1 buffer (3 NR lines of A (B + 1)), physical / spectral lines (3 NR x P),
 // forward inputs (NR + NR / 2 lines of P)
 __host__ __device__ constexpr int x2_smem(int A, int B, int K1, int csz) {
-    return 128 + x2_al(A * B * csz) + x2_al(2 * 6 * x2_rows(csz) * K1 * csz) +
-           x2_al(3 * x2_rows(csz) * (A * (B + 1) + 128 / csz) * csz) + x2_al(3 * x2_rows(csz) * A * B * csz) +
-           x2_al((x2_rows(csz) + x2_rows(csz) / 2) * A * B * csz);
+    return 128 + x2_al(A * B * csz) + x2_al(2 * 6 * x2_rows(csz, A * B) * K1 * csz) +
+           x2_al(3 * x2_rows(csz, A * B) * (A * (B + 1) + 128 / csz) * csz) +
+           x2_al(3 * x2_rows(csz, A * B) * A * B * csz) +
+           x2_al((x2_rows(csz, A * B) + x2_rows(csz, A * B) / 2) * A * B * csz);
 }
 
-// grid (P2 / NR, nchunks, members), block x2_threads(B, NR); NR = x2_rows(sizeof(C))
+// grid (P2 / NR, nchunks, members), block x2_threads(B, NR); NR = x2_rows(sizeof(C), P)
 template <typename R, int A, int B>
-__global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>)))) k_adv_x2(XArgs a, int* flag) {
+__global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B))) k_adv_x2(XArgs a, int* flag) {
     using C = cplx<R>;
-    constexpr int P = A * B, NR = x2_rows(sizeof(C)), NLI = 3 * NR, NLF = NR + NR / 2;
+    constexpr int P = A * B, NR = x2_rows(sizeof(C), P), NLI = 3 * NR, NLF = NR + NR / 2;
     constexpr int T = x2_threads(B, NR);
     constexpr int PPT = (NR * P + T - 1) / T;   // product points per thread
     constexpr int X1S = B + 1;                  // pass-1 stride of a task's outputs

@@ -12,7 +12,9 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <functional>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "bld.h"
@@ -147,6 +149,7 @@ struct Space {
     int zmult = 2;                                  // x kernels: z-chunk count multiplier in halves (autotuned)
     int xb = 0;                                     // block of warps per row (advection): 1 three warps, 2 five (pipelined)
     int x2 = 0;                                     // 1: two-pass shared-memory x kernel (advection, x2_rows rows)
+    int sx2 = 0;                                    // 1: SGS block x kernel with two-pass line transforms
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
@@ -267,7 +270,7 @@ int pick_y(int P2, bool fp32, int sets) {
 // fill the GPU a few times over, at least 8 layers per chunk
 void x_chunks(const bld_handle* h, Space& s) {
     const int n3 = h->g.n3;
-    const int rows = s.x2 ? x2_rows((int)csize(h->fp32)) : (s.xb ? 1 : (s.xw ? s.xw : s.YT));
+    const int rows = s.x2 ? x2_rows((int)csize(h->fp32), s.P1) : (s.xb ? 1 : (s.xw ? s.xw : s.YT));
     const long long blocks_per_chunk = (long long)((s.P2 + rows - 1) / rows) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
     want = std::min(want, std::max(1, n3 / 8));
@@ -329,6 +332,11 @@ size_t smem_adv(const Space& s, bool fp32) {
     return (size_t)(s.P1 + 2 * 3 * s.YT * (s.P1 + (s.xr ? 32 : 0))) * csize(fp32);
 }
 size_t smem_sgs(const Space& s, bool fp32) {
+    if (s.sx2) {
+        const int A = y2_radix_a(s.P1), B = y2_radix_b(s.P1);
+        const int lp = fp32 ? twopass_line<float2>(A, B) : twopass_line<double2>(A, B);
+        return (size_t)(s.P1 + 2 * 5 * s.YT * lp) * csize(fp32);
+    }
     return (size_t)(s.P1 + 2 * 5 * s.YT * (s.P1 + (s.xr ? 32 : 0))) * csize(fp32);
 }
 
@@ -568,14 +576,14 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
 // two-pass advection x kernel: compiled for P1 with a two-pass factorisation
 // (single precision up to 768, double up to 288), whole row pairs per block
 bool x2_ok(const bld_handle* h, const Space& s) {
-    return y2_ok(s.P1, h->fp32) && s.P2 % x2_rows((int)csize(h->fp32)) == 0 &&
+    return y2_ok(s.P1, h->fp32) && s.P2 % x2_rows((int)csize(h->fp32), s.P1) == 0 &&
            x2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, (int)csize(h->fp32)) <= 227 * 1024;
 }
 
 template <typename R, int P>
 int launch_x2_p(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
-    constexpr int NR = x2_rows((int)sizeof(cplx<R>));
+    constexpr int NR = x2_rows((int)sizeof(cplx<R>), P);
     dim3 grid(s.P2 / NR, s.nchunks, nm);
     const size_t sm = x2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>));
     k_adv_x2<R, A, B><<<grid, x2_threads(B, NR), sm, h->stream>>>(a, h->flag);
@@ -757,11 +765,44 @@ int launch_adv_xb(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     return BLD_OK;
 }
 
+template <typename R, int P>
+int launch_sgs_x2_p(bld_handle* h, const Space& s, const XArgs& a, dim3 grid, int thr, size_t sm) {
+    if (s.PPT == 1)
+        k_sgs_x<R, 1, 0, P><<<grid, thr, sm, h->stream>>>(a);
+    else
+        k_sgs_x<R, 2, 0, P><<<grid, thr, sm, h->stream>>>(a);
+    return BLD_OK;
+}
+
+// SGS x kernel with two-pass line transforms: compiled for the two-pass sizes and
+// one or two points per thread of the products
+bool sx2_ok(const bld_handle* h, const Space& s) { return y2_ok(s.P1, h->fp32); }
+
 template <typename R>
 int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     dim3 grid(s.P2 / s.YT, s.nchunks, nm);
     const int thr = s.YT * s.P1 / s.PPT;
     const size_t sm = smem_sgs(s, sizeof(R) == 4);
+    if (s.sx2) {
+        switch (s.P1) {
+            case 64: BLD_TRY((launch_sgs_x2_p<R, 64>(h, s, a, grid, thr, sm))); break;
+            case 96: BLD_TRY((launch_sgs_x2_p<R, 96>(h, s, a, grid, thr, sm))); break;
+            case 128: BLD_TRY((launch_sgs_x2_p<R, 128>(h, s, a, grid, thr, sm))); break;
+            case 144: BLD_TRY((launch_sgs_x2_p<R, 144>(h, s, a, grid, thr, sm))); break;
+            case 192: BLD_TRY((launch_sgs_x2_p<R, 192>(h, s, a, grid, thr, sm))); break;
+            case 256: BLD_TRY((launch_sgs_x2_p<R, 256>(h, s, a, grid, thr, sm))); break;
+            case 288: BLD_TRY((launch_sgs_x2_p<R, 288>(h, s, a, grid, thr, sm))); break;
+            default:
+                if constexpr (sizeof(R) == 4) {
+                    if (s.P1 == 384) { BLD_TRY((launch_sgs_x2_p<R, 384>(h, s, a, grid, thr, sm))); break; }
+                    if (s.P1 == 512) { BLD_TRY((launch_sgs_x2_p<R, 512>(h, s, a, grid, thr, sm))); break; }
+                    if (s.P1 == 768) { BLD_TRY((launch_sgs_x2_p<R, 768>(h, s, a, grid, thr, sm))); break; }
+                }
+                return fail(BLD_ERR_INVALID_CONFIG, "no two-pass SGS x kernel for P1=%d", s.P1);
+        }
+        CUDA_TRY(cudaGetLastError());
+        return BLD_OK;
+    }
     if (s.xr) {
         switch (s.xr) {
             BLD_XR_CASES(k_sgs_x)
@@ -859,6 +900,20 @@ int set_smem_limits_R() {
         BLD_SET_X2(768)
     }
 #undef BLD_SET_X2
+#define BLD_SET_SX2(P) BLD_SET((k_sgs_x<R, 1, 0, P>)); BLD_SET((k_sgs_x<R, 2, 0, P>));
+    BLD_SET_SX2(64)
+    BLD_SET_SX2(96)
+    BLD_SET_SX2(128)
+    BLD_SET_SX2(144)
+    BLD_SET_SX2(192)
+    BLD_SET_SX2(256)
+    BLD_SET_SX2(288)
+    if constexpr (sizeof(R) == 4) {
+        BLD_SET_SX2(384)
+        BLD_SET_SX2(512)
+        BLD_SET_SX2(768)
+    }
+#undef BLD_SET_SX2
     BLD_SET((k_adv_x<R, 1, 0>));
     BLD_SET((k_adv_x<R, 2, 0>));
     BLD_SET((k_adv_x<R, 3, 0>));
@@ -1258,7 +1313,82 @@ bool stage_fusable(const bld_handle* h);
 // tiling by timing every candidate on the handle's own buffers.  All candidates
 // perform the same arithmetic, so the choice changes speed, not results.
 
+// Autotuner choices of earlier handles of the same geometry, precision, process
+// set and member count on the same device (process-wide), so that handles
+// created again and again (the sub-pools of a server) are not re-timed.
+struct TuneKey {
+    int device, n1, n2, n3, members, fp32, adv_p1, adv_p2, sgs_p1, sgs_p2, pressure, env;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(device, n1, n2, n3, members, fp32, adv_p1, adv_p2, sgs_p1, sgs_p2, pressure, env) <
+               std::tie(o.device, o.n1, o.n2, o.n3, o.members, o.fp32, o.adv_p1, o.adv_p2, o.sgs_p1, o.sgs_p2,
+                        o.pressure, o.env);
+    }
+};
+struct TuneVal {
+    Space adv, sgs;
+    int proj_variant;
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, TuneVal> g_tune_cache;
+
+TuneKey tune_key(const bld_handle* h) {
+    // any kernel-family switch in the environment makes its own entry
+    int env = 0;
+    for (const char* v : {"BLD_X_KERNEL", "BLD_Y_KERNEL", "BLD_XW_MINB", "BLD_PROJ_VARIANT", "BLD_X_LINES",
+                          "BLD_SGS_X_KERNEL"}) {
+        const char* e = getenv(v);
+        env = env * 31 + (e ? (int)(std::hash<std::string>{}(e) % 1000003) + 1 : 0);
+    }
+    return TuneKey{h->device, h->cfg.n1, h->cfg.n2, h->g.n3, h->B, h->fp32 ? 1 : 0, h->adv.P1, h->adv.P2, h->sgs.P1,
+                   h->sgs.P2, h->cfg.pressure, env};
+}
+
+// the tuned fields of a space (its buffers stay the handle's own)
+void copy_tuning(Space& dst, const Space& src) {
+    dst.YT = src.YT;
+    dst.PPT = src.PPT;
+    dst.xw = src.xw;
+    dst.xwmb = src.xwmb;
+    dst.zmult = src.zmult;
+    dst.xb = src.xb;
+    dst.xr = src.xr;
+    dst.x2 = src.x2;
+    dst.sx2 = src.sx2;
+    dst.inv = src.inv;
+    dst.fwd = src.fwd;
+}
+
+int autotune_impl(bld_handle* h);
+
 int autotune(bld_handle* h) {
+    const char* env = getenv("BLD_NO_AUTOTUNE");
+    const bool cached = !(env && env[0] && env[0] != '0');
+    const TuneKey key = tune_key(h);
+    if (cached) {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            copy_tuning(h->adv, it->second.adv);
+            copy_tuning(h->sgs, it->second.sgs);
+            if (h->adv.on) x_chunks(h, h->adv);
+            if (h->sgs.on) x_chunks(h, h->sgs);
+            h->proj_variant = it->second.proj_variant;
+            return BLD_OK;
+        }
+    }
+    BLD_TRY(autotune_impl(h));
+    if (cached) {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        TuneVal v;
+        copy_tuning(v.adv, h->adv);
+        copy_tuning(v.sgs, h->sgs);
+        v.proj_variant = h->proj_variant;
+        g_tune_cache[key] = v;
+    }
+    return BLD_OK;
+}
+
+int autotune_impl(bld_handle* h) {
     // BLD_X_KERNEL=warp|block restricts the advection x kernel to one family
     const char* xk = getenv("BLD_X_KERNEL");
     const bool only_warp = xk && !strcmp(xk, "warp"), only_block = xk && !strcmp(xk, "block");
@@ -1268,6 +1398,9 @@ int autotune(bld_handle* h) {
     // the two-pass shared-memory x kernel (where it applies; elsewhere the other families)
     const bool only_x2 = xk && !strcmp(xk, "twopass") && h->adv.on && x2_ok(h, h->adv);
     const bool x2_asked = xk && !strcmp(xk, "twopass");
+    // BLD_SGS_X_KERNEL=twopass keeps the SGS x pass on two-pass line transforms
+    const char* sk = getenv("BLD_SGS_X_KERNEL");
+    const bool only_sx2 = sk && !strcmp(sk, "twopass") && h->sgs.on && sx2_ok(h, h->sgs);
     const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1, h->fp32) > 0;
     if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
     const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
@@ -1335,14 +1468,45 @@ int autotune(bld_handle* h) {
             }
             s.xr = 0;
         }
+        // SGS: the block kernel with two-pass line transforms
+        int bsx2 = 0;
+        if (sp == 1 && sx2_ok(h, s) && !only_block && !only_lines) {
+            float best2 = 1e30f;
+            int yt2 = 1, ppt2 = 1;
+            for (int yt = 1; yt <= 2; ++yt)
+                for (int ppt = 1; ppt <= 2; ++ppt) {
+                    const int thr = yt * s.P1 / ppt;
+                    if (s.P2 % yt || thr > 256 || thr < 32 || thr % 32) continue;
+                    s.sx2 = 1;
+                    s.xr = 0;
+                    s.YT = yt;
+                    s.PPT = ppt;
+                    if (smem_sgs(s, h->fp32) > 200 * 1024) continue;
+                    x_chunks(h, s);
+                    BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
+                    if (t < best2) {
+                        best2 = t;
+                        yt2 = yt;
+                        ppt2 = ppt;
+                    }
+                }
+            s.sx2 = 0;
+            if (best2 < 1e30f && (best2 < best || only_sx2)) {
+                best = best2;
+                bsx2 = 1;
+                bxr = 0;
+                byt = yt2;
+                bppt = ppt2;
+            }
+        }
         // finalists: the best block kernel above, the warp-per-row kernel with
         // 1, 2, 4 warps per block and the block-of-warps kernels, each timed at
         // its best z-chunk count (and, for the warp-per-row kernel, register
         // cap: more resident warps want more chunks)
         struct XPick {
-            int YT, PPT, xr, xw, xwmb, xb, zmult, x2;
+            int YT, PPT, xr, xw, xwmb, xb, zmult, x2, sx2;
         };
-        auto get_pick = [&]() { return XPick{s.YT, s.PPT, s.xr, s.xw, s.xwmb, s.xb, s.zmult, s.x2}; };
+        auto get_pick = [&]() { return XPick{s.YT, s.PPT, s.xr, s.xw, s.xwmb, s.xb, s.zmult, s.x2, s.sx2}; };
         auto set_pick = [&](const XPick& p) {
             s.YT = p.YT;
             s.PPT = p.PPT;
@@ -1352,6 +1516,7 @@ int autotune(bld_handle* h) {
             s.xb = p.xb;
             s.zmult = p.zmult;
             s.x2 = p.x2;
+            s.sx2 = p.sx2;
             x_chunks(h, s);
         };
         const char* mbe = getenv("BLD_XW_MINB");   // force one register cap (1, 3, 4)
@@ -1382,15 +1547,15 @@ int autotune(bld_handle* h) {
             return BLD_OK;
         };
         const bool block_ok = best < 1e30f;   // a block kernel was timed above
-        if (block_ok && (sp == 1 || !only_x2)) BLD_TRY(tune_chunks(XPick{byt, bppt, bxr, 0, 1, 0, 2, 0}));
+        if (block_ok && (sp == 1 || !only_x2)) BLD_TRY(tune_chunks(XPick{byt, bppt, bxr, 0, 1, 0, 2, 0, bsx2}));
         const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw && !only_lines && !only_x2;
-        for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) BLD_TRY(tune_chunks(XPick{1, 1, 0, wpb, 1, 0, 2, 0}));
+        for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) BLD_TRY(tune_chunks(XPick{1, 1, 0, wpb, 1, 0, 2, 0, 0}));
         for (int xbk = 1; xbk <= 2; ++xbk) {
             if (!(sp == 0 && adv_bw_ok && !only_block && !only_warp && !only_lines && !only_x2)) break;
             if ((xbk == 1 && only_pipe) || (xbk == 2 && only_bw3)) continue;
-            BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2, 0}));
+            BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2, 0, 0}));
         }
-        if (sp == 0 && x2_ok(h, s) && (only_x2 || !xk || x2_asked)) BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1}));
+        if (sp == 0 && x2_ok(h, s) && (only_x2 || !xk || x2_asked)) BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1, 0}));
         if (bx >= 1e30f) return fail(BLD_ERR_INVALID_CONFIG, "no x kernel could be timed");
         set_pick(bp);
         x_chunks(h, s);
@@ -2484,6 +2649,8 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
             snprintf(xname, sizeof xname, "k_adv_xwc<%s, %d, %d>", R, s.P1 / 32, s.xwmb);
         else if (sp == 0 && s.xw)
             snprintf(xname, sizeof xname, "k_adv_xw<%s, %d>", R, s.P1 / 32);
+        else if (sp == 1 && s.sx2)
+            snprintf(xname, sizeof xname, "%s<%s, %d, 0, %d>", xk, R, s.PPT, s.P1);
         else
             snprintf(xname, sizeof xname, "%s<%s, %d, %d>", xk, R, s.PPT, s.xr);
         char iname[64], fname[64];

@@ -24,6 +24,14 @@
 #define BLD_MAXT 10
 #define BLD_MAXC 4
 
+// the two-pass factorisations compiled (P = A B with A <= B; the transforms of
+// bld_ypass2.cuh, the advection x kernel of bld_advx2.cuh and k_sgs_x<.., TP>)
+__host__ __device__ constexpr int y2_radix_a(int P) {
+    return P == 64 ? 8 : P == 96 ? 8 : P == 128 ? 8 : P == 144 ? 12 : P == 192 ? 12 : P == 256 ? 16 : P == 288 ? 16
+         : P == 384 ? 16 : P == 512 ? 16 : P == 768 ? 24 : 0;
+}
+__host__ __device__ constexpr int y2_radix_b(int P) { return y2_radix_a(P) ? P / y2_radix_a(P) : 0; }
+
 struct Geo {
     int K1, K2, k1max, k2max, n3, F;  // F = K1*K2 modes per layer
     long long mstride;                // complex values per member state (3*n3-1)*F
@@ -597,13 +605,58 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
 // Streaming in z with a two-layer lag: step j loads C layer j and I layer j and
 // completes C layer j-1, I layer j-1 and the d3 tau33 of I layer j-2.
 // RAD > 0: the x transforms run one line per warp in registers (P1 = 32 RAD).
-template <typename R, int PPT, int RAD>
+// In-place transforms of `nlines` lines of P = A B points in shared memory
+// (point p of line L at buf[L LP + p], natural order in and out) by the two
+// passes of the y kernels: pass 1 (B tasks per line, radix-A DFTs of points
+// j + B t) into the scratch X1 at q (B + 1) + j of its line, pass 2 (A tasks
+// per line, W_P^(DIR j t) then radix-B DFTs) back into buf at j + A q.  `tw2`
+// holds W_P^(-j t) as [t][j] (P entries).  X1 needs nlines * twopass_line(A, B)
+// values.  All threads of the block call it after a barrier that publishes buf;
+// it ends with a barrier.
+template <typename C>
+__host__ __device__ constexpr int twopass_line(int A, int B) {
+    return A * (B + 1) + ((B - A * (B + 1)) % (int)(128 / sizeof(C)) + (int)(128 / sizeof(C))) % (int)(128 / sizeof(C));
+}
+template <typename R, int A, int B, int DIR>
+__device__ __forceinline__ void twopass_inplace(cplx<R>* buf, int nlines, int LP, cplx<R>* X1,
+                                                const cplx<R>* __restrict__ tw2) {
+    using C = cplx<R>;
+    constexpr int X1S = B + 1, X1L = twopass_line<C>(A, B);
+    for (int task = threadIdx.x; task < nlines * B; task += blockDim.x) {
+        const int L = task / B, jt = task - L * B;
+        C x[A];
+#pragma unroll
+        for (int t = 0; t < A; ++t) x[t] = buf[L * LP + jt + B * t];
+        dft<R, A, DIR>(x);
+#pragma unroll
+        for (int q = 0; q < A; ++q) X1[L * X1L + q * X1S + jt] = x[q];
+    }
+    __syncthreads();
+    for (int task = threadIdx.x; task < nlines * A; task += blockDim.x) {
+        const int L = task / A, j2 = task - L * A;
+        C x[B];
+#pragma unroll
+        for (int t = 0; t < B; ++t) x[t] = X1[L * X1L + j2 * X1S + t];
+#pragma unroll
+        for (int t = 1; t < B; ++t) x[t] = c_tw<DIR>(x[t], tw2[t * A + j2]);
+        dft<R, B, DIR>(x);
+#pragma unroll
+        for (int q = 0; q < B; ++q) buf[L * LP + j2 + A * q] = x[q];
+    }
+    __syncthreads();
+}
+
+// TP > 0: the x transforms of a compile-time P1 = TP by twopass_inplace (the
+// other buffer is the scratch; lines at stride twopass_line), RAD must be 0
+template <typename R, int PPT, int RAD, int TP = 0>
 __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P1 = a.P1, YT = a.YT, n3 = a.g.n3, k1max = a.g.k1max;
     const int NLin = 5 * YT, NLout = 4 * YT;
-    const int LP = RAD ? P1 + 32 : P1;   // RAD > 0: swizzled positions on a padded line stride
+    constexpr int TA = TP ? y2_radix_a(TP) : 1, TB = TP ? y2_radix_b(TP) : 1;
+    // RAD > 0: swizzled positions on a padded line stride; TP > 0: the two-pass scratch stride
+    const int LP = TP ? twopass_line<C>(TA, TB) : (RAD ? P1 + 32 : P1);
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* bufA = tw + P1;
     C* bufB = bufA + NLin * LP;
@@ -614,7 +667,11 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
     const int z1 = min(n3, z0 + a.zchunk);
     const int nthr = blockDim.x;
     const C* twg = reinterpret_cast<const C*>(a.tw);
-    lane_table<RAD>(tw, twg, P1);
+    if constexpr (TP > 0) {
+        for (int i = threadIdx.x; i < TP; i += blockDim.x) tw[i] = twg[(i / TA) * (i % TA)];
+    } else {
+        lane_table<RAD>(tw, twg, P1);
+    }
     const C* Min = reinterpret_cast<const C*>(a.min) + (long long)m * a.min_mstride;
     C* Mout = reinterpret_cast<C*>(a.mout) + (long long)m * a.mout_mstride;
     const double* lcm = a.lc + (long long)m * n3;
@@ -671,7 +728,9 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
                 }
             }
             __syncthreads();
-            if constexpr (RAD > 0) {
+            if constexpr (TP > 0) {
+                twopass_inplace<R, TA, TB, +1>(bufA, NLin, LP, bufB, tw);
+            } else if constexpr (RAD > 0) {
                 warp_lines_inplace<R, RAD, +1>(bufA, NLin, P1, tw, twg);
                 __syncthreads();
             } else {
@@ -797,7 +856,9 @@ __global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
         if (doC || do5) {
             __syncthreads();
             C* r2 = outb;
-            if constexpr (RAD > 0) {
+            if constexpr (TP > 0) {
+                twopass_inplace<R, TA, TB, -1>(outb, NLout, LP, phys, tw);
+            } else if constexpr (RAD > 0) {
                 warp_lines_inplace<R, RAD, -1>(outb, NLout, P1, tw, twg);
                 __syncthreads();
             } else {

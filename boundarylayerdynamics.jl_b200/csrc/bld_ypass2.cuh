@@ -22,12 +22,6 @@
 // and adds the linear terms.
 #pragma once
 
-// the two-pass factorisations compiled (P2 -> A, B with A <= B)
-__host__ __device__ constexpr int y2_radix_a(int P) {
-    return P == 64 ? 8 : P == 96 ? 8 : P == 128 ? 8 : P == 144 ? 12 : P == 192 ? 12 : P == 256 ? 16 : P == 288 ? 16
-         : P == 384 ? 16 : P == 512 ? 16 : P == 768 ? 24 : 0;
-}
-__host__ __device__ constexpr int y2_radix_b(int P) { return y2_radix_a(P) ? P / y2_radix_a(P) : 0; }
 #define BLD_Y2_NL 16
 // resident blocks per SM the register allocation is held to (launch bounds):
 // up to ~110 registers per thread for blocks of up to 288 threads

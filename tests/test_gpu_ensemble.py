@@ -183,3 +183,40 @@ def test_served_request_same_alone_and_in_mix(oracle, BLD, precision, tol):
         om.initialize(vel1=u, vel2=v, vel3=w)
         om.evolve(20 * DT, DT)
         _close(target.result, om.state, TRAJ_TOL)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-6)])
+def test_elastic_server_request_same_alone_and_in_mix(oracle, BLD, precision, tol):
+    """Pools created and released against the HBM budget (ElasticServer), requests
+    initialised on the device: a request gives the same result alone and among
+    concurrent requests, and (FP64) the oracle's trajectory from the same seeded
+    field.  The budget holds two pools, so pools are released and re-made."""
+    from BoundaryLayerDynamics import serving as S
+    from BoundaryLayerDynamics import workloads
+    sizes = ((16, 8), (24, 12))
+
+    def server():
+        def factory(size, n):
+            return workloads.build(S.spec_for(size), BLD, precision=precision, members=n)
+        return S.ElasticServer(factory, {(16, 8): 3, (24, 12): 2}, {(16, 8): 10, (24, 12): 10}, budget=20, dt=DT,
+                               tick=5, keep_results=True)
+
+    def requests():
+        return S.make_requests(12, rate=2000.0, seed=11, sizes=sizes, probs=(0.5, 0.5), steps=20, materialize=False)
+
+    mix = requests()
+    srv = server()
+    st = srv.run(mix)
+    assert st["completed"] == 12 and st["peak_resident_bytes"] <= 20
+    target = mix[7]
+    alone = [r for r in requests() if r.rid == target.rid]
+    alone[0].arrival = 0.0
+    assert server().run(alone)["completed"] == 1
+    _close(target.result, alone[0].result, tol)
+    if precision == "fp64":
+        s = S.spec_for(target.size, z0=target.z0, forcing=target.forcing, seed=target.seed)
+        om = workloads.build(s, oracle)
+        u, v, w = workloads.seeded_initial_fields(s, target.seed)
+        om.initialize(vel1=u, vel2=v, vel3=w)
+        om.evolve(20 * DT, DT)
+        _close(target.result, om.state, TRAJ_TOL)

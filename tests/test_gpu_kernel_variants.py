@@ -92,7 +92,7 @@ def test_advection_x_kernel_family(oracle, BLD, res, precision, tol, family):
     gm = _forced(BLD, family, res, precision)
     if family == "twopass":
         # two (double) or four (single precision) y rows per block
-        if gm.info.adv_p2 % (2 if precision == "fp64" else 4) == 0:
+        if gm.info.adv_p2 % (2 if precision == "fp64" or gm.info.adv_p1 > 384 else 4) == 0:
             assert gm.kernels()["advection"]["x"].startswith("k_adv_x2<"), gm.kernels()
     elif family != "block":
         assert gm.info.adv_p1 % 32 == 0
@@ -270,16 +270,59 @@ SGS_CASES = [
 
 
 @pytest.mark.parametrize("res,precision,tol", SGS_CASES)
-@pytest.mark.parametrize("family", ["block", "lines"])
+@pytest.mark.parametrize("family", ["block", "lines", "twopass"])
 def test_sgs_x_kernel_family(oracle, BLD, res, precision, tol, family):
     om = _build(oracle, res, les=True)
-    gm = _forced(BLD, family, res, precision, les=True)
+    if family == "twopass":   # the SGS x pass on two-pass line transforms (BLD_SGS_X_KERNEL)
+        old = os.environ.get("BLD_SGS_X_KERNEL")
+        os.environ["BLD_SGS_X_KERNEL"] = "twopass"
+        try:
+            gm = _build(BLD, res, precision, les=True)
+        finally:
+            if old is None:
+                del os.environ["BLD_SGS_X_KERNEL"]
+            else:
+                os.environ["BLD_SGS_X_KERNEL"] = old
+        p1 = gm.info.sgs_p1
+        if p1 <= 288 or precision == "mixed":
+            assert gm.kernels()["sgs"]["x"].endswith(", 0, %d>" % p1), gm.kernels()
+    else:
+        gm = _forced(BLD, family, res, precision, les=True)
     st = _state(om, seed=sum(res) + 2)
     ref = om.compute_rates(st)
     got = gm.compute_rates(st)
     for f in om.fields:
         e = rel_l2(got[f], ref[f])
         assert e < tol, (res, precision, family, f, e)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
+def test_sgs_twopass_les_trajectory(oracle, BLD, precision, tol):
+    """20 SSP-RK33 steps of an LES (64^2 x 16: SGS P1 = 64) with the SGS x pass
+    on two-pass line transforms, against the oracle."""
+    res = (64, 64, 16)
+    om = _build(oracle, res, les=True)
+    old = os.environ.get("BLD_SGS_X_KERNEL")
+    os.environ["BLD_SGS_X_KERNEL"] = "twopass"
+    try:
+        gm = _build(BLD, res, precision, les=True)
+    finally:
+        if old is None:
+            del os.environ["BLD_SGS_X_KERNEL"]
+        else:
+            os.environ["BLD_SGS_X_KERNEL"] = old
+    assert gm.kernels()["sgs"]["x"].endswith(", 0, 64>"), gm.kernels()
+    st = _state(om, seed=21)
+    for f in st:
+        st[f] *= 5.0
+    gm.set_state(st)
+    om.state.update({f: v.copy() for f, v in st.items()})
+    gm.evolve(20 * 1e-4, 1e-4)
+    om.evolve(20 * 1e-4, 1e-4)
+    got = gm.state
+    for f in om.fields:
+        e = rel_l2(got[f], om.state[f])
+        assert e < tol, (precision, f, e)
 
 
 @pytest.mark.parametrize("variant", ["0", "1", "2", "3"])

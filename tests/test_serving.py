@@ -45,6 +45,11 @@ class FakePool:
         self.loaded.setdefault(member, []).append(f)
         self.steps[member] = 0
 
+    def init_random_field(self, f, base, scale, distribution, seed, member):
+        assert self.idle(), "a pool is loaded only between ticks"
+        self.loaded.setdefault(member, []).append(f)
+        self.steps[member] = 0
+
     def set_member_params(self, m, cs=None, z0=None, forcing=None):
         self.params[m] = (z0, forcing)
 
@@ -224,3 +229,71 @@ def test_server_pools_advance_independently():
     assert big.status == tiny.status == "done"
     assert tiny.result["steps"] == 50 and big.result["steps"] == 50
     assert tiny.latency < 0.01 < big.latency          # 50 x 1e-5 s vs 50 x 1e-2 s of device time
+
+
+# ------------------------------------------------------ admission by free HBM (elastic pools)
+def _elastic(slots, pool_bytes, budget, tick=5, costs=None):
+    clock = FakeClock()
+    made = []
+
+    def factory(size, n):
+        p = FakePool(n, clock, cost=(costs or {}).get(size, 1e-4))
+        made.append((size, p))
+        return p
+    srv = S.ElasticServer(factory, slots, pool_bytes, budget, tick=tick, keep_results=True, clock=clock,
+                          sleep=clock.sleep, poll=1e-5)
+    return srv, clock, made
+
+
+def test_elastic_scheduler_reclaims_idle_pools_for_a_large_request():
+    small, large = (32, 16), (128, 64)
+    sch = S.ElasticScheduler({small: 2, large: 1}, {small: 30, large: 100}, budget=100)
+    created, destroyed = [], []
+    create = lambda pid, size: created.append((pid, size))
+    destroy = lambda pid: destroyed.append(pid)
+    ready = lambda pid: True
+    reqs = [S.Request(i, s, 5, 0.0, 1e-4, 1.0, i) for i, s in enumerate([small, small, small, large, small])]
+    for r in reqs:
+        assert sch.submit(r)
+    got = sch.admit(ready, create, destroy)
+    # two small pools (60 of 100 bytes) take the three small requests; the large one
+    # does not fit and blocks new pools for the small request behind it, which
+    # still finds the free slot of the second small pool
+    assert [(r.rid, pid) for r, pid, _ in got] == [(0, 0), (1, 0), (2, 1), (4, 1)]
+    assert [r.rid for r in sch.queue] == [3] and sch.allocated == 60
+    for r, pid, slot in list(got):
+        sch.release(pid, slot)
+    got = sch.admit(ready, create, destroy)        # both small pools idle: released, large pool made
+    assert destroyed == [0, 1] and [(r.rid, pid) for r, pid, _ in got] == [(3, 2)]
+    assert sch.allocated == 100 and sch.peak_resident == 100
+
+
+def test_elastic_server_serves_a_large_request_between_small_ones():
+    small, large = (32, 16), (256, 128)
+    srv, clock, made = _elastic({small: 4, large: 1}, {small: 40, large: 100}, budget=120, tick=5,
+                                costs={small: 1e-4, large: 1e-3})
+    reqs = [S.Request(i, small, 20, 1e-4 * i, 1e-4, 1.0, i) for i in range(10)]
+    reqs.append(S.Request(10, large, 20, 2e-4, 1e-4, 1.0, 10))
+    reqs += [S.Request(11 + i, small, 20, 3e-4 + 1e-4 * i, 1e-4, 1.0, 11 + i) for i in range(10)]
+    st = srv.run(reqs)
+    assert st["completed"] == len(reqs) and st["rejected"] == 0
+    for r in reqs:
+        assert r.result["steps"] == 20
+    big = reqs[10]
+    assert big.status == "done"
+    assert st["peak_resident_bytes"] <= 120
+    assert st["pools_released"] >= 1                     # small pools gave their memory back
+    assert {s for s, _ in made} == {small, large}
+
+
+def test_elastic_server_exact_steps_many_sizes():
+    sizes = [(32, 16), (48, 24), (64, 32)]
+    slots = {(32, 16): 3, (48, 24): 2, (64, 32): 1}
+    pb = {(32, 16): 30, (48, 24): 50, (64, 32): 70}
+    srv, clock, made = _elastic(slots, pb, budget=150, tick=7)
+    reqs = S.make_requests(60, 2000.0, seed=9, sizes=sizes, probs=[1 / 3] * 3, steps=30, materialize=False)
+    st = srv.run(reqs)
+    assert st["completed"] == 60
+    for r in reqs:
+        assert r.result["steps"] == 30 and r.result["params"] == (r.z0, r.forcing)
+    assert st["peak_resident_bytes"] <= 150
