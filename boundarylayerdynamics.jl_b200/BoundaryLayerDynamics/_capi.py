@@ -103,6 +103,7 @@ SIGNATURES = {
     "bld_get_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bld_step_async": (C.c_int32, [C.c_void_p, C.c_int64, C.c_double, C.c_int32]),
     "bld_stream_idle": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "bld_set_wait_limit": (C.c_int32, [C.c_int32, C.c_int64]),
     "bld_time_phases": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(BldPhaseTimes)]),
     "bld_ensemble_step": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_int32]),
     "bld_set_active": (C.c_int32, [C.c_void_p, C.c_void_p]),

@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B))
         }
     };
     const int jb = max(0, z0 - 1);
+    const long long wait_limit = g_bld_wait_limit;
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B))
             fence_async_shared();
             issue(j + 1, s ^ 1);
         }
-        const bool arrived = mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1);
+        const bool arrived = mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1, wait_limit);
         const C* cur = stage + (size_t)s * 6 * NR * K1;
         // ---- inverse pass 1: lines L = 3 r + p (pairs (u, v), (vort3, w), (vort1, vort2))
         for (int task = threadIdx.x; task < NLI * B; task += T) {

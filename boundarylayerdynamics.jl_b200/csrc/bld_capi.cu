@@ -2597,6 +2597,17 @@ int32_t bld_stream_idle(bld_handle* h, int32_t* idle) {
     return BLD_OK;
 }
 
+int32_t bld_set_wait_limit(int32_t device, int64_t cycles) {
+    int prev = 0;
+    CUDA_TRY(cudaGetDevice(&prev));
+    CUDA_TRY(cudaSetDevice(device));
+    const long long v = cycles < 0 ? BLD_WAIT_CYCLES : (long long)cycles;
+    const cudaError_t e = cudaMemcpyToSymbol(g_bld_wait_limit, &v, sizeof(v));
+    cudaSetDevice(prev);
+    CUDA_TRY(e);
+    return BLD_OK;
+}
+
 int32_t bld_set_active(bld_handle* h, const int32_t* mask) {
     if (!h) return fail(BLD_ERR_ARGUMENT, "null handle");
     CUDA_TRY(cudaSetDevice(h->device));

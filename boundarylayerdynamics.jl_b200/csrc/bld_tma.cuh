@@ -4,7 +4,8 @@
 // cp.async.bulk.tensor instruction each, issued by one thread; completion is
 // tracked by an mbarrier whose transaction count the copies decrement.  Only
 // plain (non-multicast) loads from this GPU's own memory are used.  Every wait
-// is bounded: after BLD_WAIT_CYCLES clock cycles the waiting thread gives up
+// is bounded: after g_bld_wait_limit clock cycles (BLD_WAIT_CYCLES unless the
+// host set another limit with bld_set_wait_limit) the waiting thread gives up
 // and the kernel reports BLD_FLAG_TIMEOUT through its per-member flag.
 #pragma once
 
@@ -14,6 +15,11 @@
 #define BLD_WAIT_CYCLES (1LL << 31)   // about one second at the B200's clocks
 #define BLD_FLAG_NONFINITE 1
 #define BLD_FLAG_TIMEOUT 2
+
+// limit of the kernels' waits for their own TMA copies, in clock cycles; 0 makes
+// every such wait give up at once (a diagnostic setting: the kernels then take
+// their timeout exit with no copy missing)
+__device__ long long g_bld_wait_limit = BLD_WAIT_CYCLES;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -44,12 +50,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
-// waits for the phase `parity` of `bar` to complete; false after BLD_WAIT_CYCLES
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+// waits for the phase `parity` of `bar` to complete; false after `limit` cycles
+// (at once for limit <= 0)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, long long limit = BLD_WAIT_CYCLES) {
+    if (limit <= 0) return false;
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > BLD_WAIT_CYCLES) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 

@@ -354,6 +354,7 @@ __global__ void __launch_bounds__(B * BLD_Y3_NL) k_inv_y3(InvYArgs a, const __gr
     }
     const C* twg = reinterpret_cast<const C*>(a.tw);
     for (int i = threadIdx.x; i < P; i += blockDim.x) tw[i] = twg[i];
+    const long long wait_limit = g_bld_wait_limit;
     const int l = threadIdx.x % NL, j = threadIdx.x / NL;
     const int k1 = k10 + l;
     const bool ok = k1 < K1;
@@ -362,7 +363,7 @@ __global__ void __launch_bounds__(B * BLD_Y3_NL) k_inv_y3(InvYArgs a, const __gr
     for (int z = z0; z < z1; ++z) {
         const int s = (z - z0) & 1;
         const unsigned parity = ((z - z0) >> 1) & 1;
-        const bool arrived = mbar_wait_bounded(&bar[s], parity);
+        const bool arrived = mbar_wait_bounded(&bar[s], parity, wait_limit);
         const double2* ts = tiles + (size_t)s * NT * tile_elems;
         switch (op) {
             case T_DIRECT: inv_y3_pass1<R, A, B, T_DIRECT>(a, ts, tile_elems, z, ok, e1, j, l, X1); break;

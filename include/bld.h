@@ -178,6 +178,14 @@ int32_t bld_step_async(bld_handle* h, int64_t nsteps, double dt, int32_t method)
    finished (then bld_sync returns at once with the divergence check), else 0. */
 int32_t bld_stream_idle(bld_handle* h, int32_t* idle);
 
+/* Limit, in SM clock cycles, of the kernels' bounded waits for their own TMA
+   copies on `device` (default 2^31, about one second); cycles < 0 restores the
+   default.  cycles = 0 is a diagnostic setting: every such wait gives up at once,
+   the kernels take their timeout exit (after their copies have landed) and the
+   next call that checks the flags returns BLD_ERR_TIMEOUT.  Affects only the
+   TMA-staged kernels (k_adv_x2, k_inv_y3); the setting is device-wide. */
+int32_t bld_set_wait_limit(int32_t device, int64_t cycles);
+
 /* Average device time of each launch kind of one right-hand side, measured with
    CUDA events on the handle's stream over `iters` back-to-back launches of that
    kind on the resident state (index 0: advection space, 1: SGS space). */

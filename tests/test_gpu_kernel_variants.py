@@ -356,3 +356,30 @@ def test_projection_variants(oracle, BLD, variant, res):
     om.evolve(3 * 1e-3, 1e-3)
     for f in om.fields:
         assert rel_l2(gm.state[f], om.state[f]) < 1e-10, (variant, res, f)
+
+
+def test_bounded_wait_timeout_exit(oracle, BLD):
+    """The TMA-staged x kernel's bounded wait taken to its timeout exit: with the
+    device's wait limit set to 0 every block gives up at its first wait, lets the
+    copies it issued land, sets the member's timeout flag and returns; the call
+    reports BLD_ERR_TIMEOUT.  With the limit restored the same handle computes the
+    rates exactly again (the context stays usable)."""
+    from BoundaryLayerDynamics import _capi
+    res = (64, 64, 6)
+    gm = _forced(BLD, "twopass", res, "fp64")
+    assert gm.kernels()["advection"]["x"].startswith("k_adv_x2<"), gm.kernels()
+    om = _build(oracle, res)
+    st = _state(om, seed=11)
+    ref = om.compute_rates(st)
+    lib = _capi.load()
+    _capi.check(lib.bld_set_wait_limit(0, 0))
+    try:
+        with pytest.raises(_capi.BldError) as err:
+            gm.compute_rates(st)
+        assert err.value.status == _capi.BLD_ERR_TIMEOUT, err.value
+    finally:
+        _capi.check(lib.bld_set_wait_limit(0, -1))
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < 1e-12, (f, e)
