@@ -373,9 +373,10 @@ def _event_time(stream, fn):
 
 def run_les(name, precisions, steps, warmup, local):
     """Single-member LES at one of the LES sizes: updates/s per precision."""
+    import ctypes
     import torch
     import BoundaryLayerDynamics as BLD
-    from BoundaryLayerDynamics import workloads
+    from BoundaryLayerDynamics import workloads, _capi
     spec = workloads.CONFIGS[name]
     u0, v0, w0 = workloads.initial_fields(spec)
     n = spec["resolution"]
@@ -394,8 +395,13 @@ def run_les(name, precisions, steps, warmup, local):
         sb = state_bytes(m)
         peak, _ = peaks()
         ach = 8 * sb / (ms / steps * 1e-3) / 1e9
+        # device time per launch of each phase (index 0: advection space, 1: SGS space)
+        pt = _capi.BldPhaseTimes()
+        _capi.check(m._lib.bld_time_phases(m._h, 5, _capi.SSPRK33, ctypes.byref(pt)))
+        phases = {"inv_y": list(pt.inv_y_ms), "x": list(pt.x_ms), "fwd_y": list(pt.fwd_y_ms),
+                  "project": pt.project_ms, "launches_per_step": pt.launches_per_step}
         out[prec] = {"value": npts * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
-                     "device_bytes": m.info.device_bytes,
+                     "device_bytes": m.info.device_bytes, "kernels": m.kernels(), "phases_ms": phases,
                      "roofline_step": {"algorithmic_bytes_per_step": 8 * sb, "achieved": ach, "unit": "GB/s",
                                        "frac": ach / peak}}
         del m

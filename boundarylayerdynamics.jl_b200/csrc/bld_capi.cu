@@ -15,12 +15,14 @@
 #include <functional>
 #include <string>
 #include <tuple>
+#include <initializer_list>
 #include <vector>
 
 #include "bld.h"
 #include "bld_kernels.cuh"
 #include "bld_warpx.cuh"
 #include "bld_advx2.cuh"
+#include "bld_project_tile.cuh"
 
 double2 h_wtab64[BLD_WTAB_SIZE];
 float2 h_wtab32[BLD_WTAB_SIZE];
@@ -54,12 +56,15 @@ int fail(int code, const char* fmt, ...) {
     } while (0)
 
 // ---------------------------------------------------------------- FFT sizes and plans
-bool smooth23(int n) {
+bool smooth_of(int n, std::initializer_list<int> primes) {
     if (n < 2) return false;
-    while (n % 2 == 0) n /= 2;
-    while (n % 3 == 0) n /= 3;
+    for (int p : primes)
+        while (n % p == 0) n /= p;
     return n == 1;
 }
+bool smooth23(int n) { return smooth_of(n, {2, 3}); }
+// sizes the block Stockham kernels transform: products of 2, 3, 5 and 7
+bool smooth2357(int n) { return smooth_of(n, {2, 3, 5, 7}); }
 
 int next_even_smooth(int n) {
     int m = std::max(n, 2);
@@ -68,15 +73,17 @@ int next_even_smooth(int n) {
 }
 
 // Fewest Stockham stages whose radices are register codelet sizes, then the
-// smallest largest radix (register pressure), capped at BLD_FP32_MAXR / BLD_FP64_MAXR.
+// smallest largest radix (register pressure), capped at BLD_FP32_MAXR / BLD_FP64_MAXR;
+// nst = 0 if no such plan of at most four stages exists.
 FftPlan make_plan(int n, bool fp32 = false) {
-    static const int rads[] = {32, 24, 18, 16, 12, 9, 8, 6, 4, 3, 2};
+    static const int rads[] = {32, 24, 18, 16, 15, 14, 12, 10, 9, 8, 7, 6, 5, 4, 3, 2};
     const int cap = fp32 ? BLD_FP32_MAXR : BLD_FP64_MAXR;
     FftPlan best{};
     best.n = n;
+    best.nst = 0;
     int best_st = 99, best_max = 99;
     int seq[6];
-    // depth-first search over radix sequences (n <= 2048 needs at most 4 stages)
+    // depth-first search over radix sequences (n <= 1024 of 2, 3, 5, 7 needs at most 4 stages of <= 18)
     auto dfs = [&](auto&& self, int rem, int depth, int mx) -> void {
         if (depth > 4 || depth > best_st) return;
         if (rem == 1) {
@@ -95,12 +102,6 @@ FftPlan make_plan(int n, bool fp32 = false) {
         }
     };
     dfs(dfs, n, 0, 0);
-    if (best_st == 99) {  // cannot happen for 2^a 3^b, kept for safety: radix 2/3 chain
-        int m = n, s = 0;
-        while (m % 2 == 0) { best.radix[s++] = 2; m /= 2; }
-        while (m % 3 == 0) { best.radix[s++] = 3; m /= 3; }
-        best.nst = s;
-    }
     return best;
 }
 
@@ -148,7 +149,7 @@ struct Space {
     int xwmb = 1;                                   // warp-per-row kernel: register cap (min blocks of 128 threads)
     int zmult = 2;                                  // x kernels: z-chunk count multiplier in halves (autotuned)
     int xb = 0;                                     // block of warps per row (advection): 1 three warps, 2 five (pipelined)
-    int x2 = 0;                                     // 1: two-pass shared-memory x kernel (advection, x2_rows rows)
+    int x2 = 0;                                     // 1 + V: two-pass shared-memory x kernel k_adv_x2<.., V> (advection)
     int sx2 = 0;                                    // 1: SGS block x kernel with two-pass line transforms
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
@@ -176,6 +177,7 @@ struct bld_handle {
     // tables
     double *d1 = nullptr, *d2 = nullptr, *DD1 = nullptr, *DD2 = nullptr;
     double *alpha_c = nullptr, *alpha_i = nullptr, *alpha_ext = nullptr, *mean_w = nullptr;
+    double* inv_alpha_c = nullptr;   // 1 / alpha_c (the projections' divergence)
     double *lc2 = nullptr, *li2 = nullptr, *wall = nullptr, *src = nullptr, *mean_val = nullptr;
     int* flag = nullptr;
     int* flag_host = nullptr;
@@ -184,6 +186,7 @@ struct bld_handle {
     std::vector<int> active_host;
     bool mask_on = false;        // the active mask applies to whole-ensemble steps only
     int proj_variant = 1;        // 0: column kernel, 1/2: z-segmented kernel, 3: with a shared tile (autotuned)
+    int proj_tile = 0;           // LN > 0: projections of stored stage values by k_project_tile<.., LN> (autotuned)
     double* prof_acc = nullptr;  // [members][3][n3+1] time integral of the mean profiles
     double* prof_prev = nullptr; // [members][3][n3+1] last sample
     bool prof_on = false;        // step graphs sample the profiles after every step
@@ -441,6 +444,38 @@ int state_tmap(const bld_handle* h, const void* base, int nl, CUtensorMap* out) 
     return BLD_OK;
 }
 
+// k_project_tile applies: the pressure solve with <= 256 layers, an even number
+// of modes per layer (gamma rows are 16-byte multiples for the TMA map) and
+// LN columns x all layers within a block's shared memory
+bool project_tile_ok(const bld_handle* h, int ln) {
+    return h->cfg.pressure && h->g.n3 <= 256 && h->g.F % 2 == 0 && (ln == 8 || ln == 16) &&
+           project_tile_smem(h->g.n3, ln) <= 200 * 1024 && encode_tiled() != nullptr;
+}
+
+// tensor maps of k_project_tile: the members' states from `u` as float64
+// (2 F, 3 n3 - 1, members) with the box (2 LN, n3, 1), and gamma as (F, n3) with
+// the box (LN, n3)
+int project_tmaps(const bld_handle* h, const void* u, int ln, CUtensorMap* umap, CUtensorMap* gmap) {
+    const Geo& g = h->g;
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return fail(BLD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const cuuint64_t udims[3] = {(cuuint64_t)(2 * g.F), (cuuint64_t)(3 * g.n3 - 1), (cuuint64_t)h->B};
+    const cuuint64_t ustr[2] = {(cuuint64_t)g.F * 16, (cuuint64_t)g.mstride * 16};
+    const cuuint32_t ubox[3] = {(cuuint32_t)(2 * ln), (cuuint32_t)g.n3, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(umap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(u), udims, ustr, ubox, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(BLD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    const cuuint64_t gdims[2] = {(cuuint64_t)g.F, (cuuint64_t)g.n3};
+    const cuuint64_t gstr[1] = {(cuuint64_t)g.F * 8};
+    const cuuint32_t gbox[2] = {(cuuint32_t)ln, (cuuint32_t)g.n3};
+    r = fn(gmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, h->gamma, gdims, gstr, gbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(BLD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return BLD_OK;
+}
+
 // k_inv_y3 applies: a two-pass factorisation, whole K2 columns in one TMA box
 // (K2 <= 256) and the staged tiles within the shared memory of a block
 bool y3_ok(const bld_handle* h, int P2) {
@@ -574,19 +609,29 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
 }
 
 // two-pass advection x kernel: compiled for P1 with a two-pass factorisation
-// (single precision up to 768, double up to 288), whole row pairs per block
-bool x2_ok(const bld_handle* h, const Space& s) {
-    return y2_ok(s.P1, h->fp32) && s.P2 % x2_rows((int)csize(h->fp32), s.P1) == 0 &&
-           x2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, (int)csize(h->fp32)) <= 227 * 1024;
+// (single precision up to 768, double up to 288), whole row pairs per block;
+// variants V = 1 (lean) and 2 (wide) in double precision only
+bool x2_ok(const bld_handle* h, const Space& s, int V = 0) {
+    return y2_ok(s.P1, h->fp32) && s.P2 % x2_rows((int)csize(h->fp32), s.P1) == 0 && (V == 0 || !h->fp32) &&
+           x2_smem_v(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, (int)csize(h->fp32), V) <= 227 * 1024;
+}
+
+template <typename R, int P, int V>
+void launch_x2_pv(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
+    constexpr int NR = x2_rows((int)sizeof(cplx<R>), P);
+    dim3 grid(s.P2 / NR, s.nchunks, nm);
+    const size_t sm = x2_smem_v(A, B, h->g.K1, (int)sizeof(cplx<R>), V);
+    k_adv_x2<R, A, B, V><<<grid, x2_threads(B, NR, V), sm, h->stream>>>(a, h->flag);
 }
 
 template <typename R, int P>
 int launch_x2_p(bld_handle* h, const Space& s, const XArgs& a, int nm) {
-    constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
-    constexpr int NR = x2_rows((int)sizeof(cplx<R>), P);
-    dim3 grid(s.P2 / NR, s.nchunks, nm);
-    const size_t sm = x2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>));
-    k_adv_x2<R, A, B><<<grid, x2_threads(B, NR), sm, h->stream>>>(a, h->flag);
+    if constexpr (sizeof(R) == 8) {
+        if (s.x2 == 2) return launch_x2_pv<R, P, 1>(h, s, a, nm), BLD_OK;
+        if (s.x2 == 3) return launch_x2_pv<R, P, 2>(h, s, a, nm), BLD_OK;
+    }
+    launch_x2_pv<R, P, 0>(h, s, a, nm);
     return BLD_OK;
 }
 
@@ -886,7 +931,12 @@ int set_smem_limits_R() {
         BLD_SET_Y3(768)
     }
 #undef BLD_SET_Y3
-#define BLD_SET_X2(P) BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P)>));
+#define BLD_SET_X2(P)                                                   \
+    BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P), 0>));            \
+    if constexpr (sizeof(R) == 8) {                                     \
+        BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P), 1>));        \
+        BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P), 2>));        \
+    }
     BLD_SET_X2(64)
     BLD_SET_X2(96)
     BLD_SET_X2(128)
@@ -982,7 +1032,7 @@ int init_codelet_twiddles() {
     CUDA_TRY(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lock(mu);
     if (done[dev]) return BLD_OK;
-    const int sizes[] = {6, 8, 9, 12, 16, 18, 24, 32};
+    const int sizes[] = {5, 6, 7, 8, 9, 10, 12, 14, 15, 16, 18, 24, 32};
     for (int N : sizes)
         for (int m = 0; m < N; ++m) {
             const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)N;
@@ -1003,6 +1053,11 @@ int set_smem_limits() {
     BLD_TRY(set_smem_limits_R<float>());
     CUDA_TRY(cudaFuncSetAttribute(k_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CUDA_TRY(cudaFuncSetAttribute(k_project_seg<8, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    // dynamic shared memory of k_project_tile: at most 200 KB (project_tile_ok)
+    CUDA_TRY(cudaFuncSetAttribute(k_project_tile<8, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_tile<8, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_tile<16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_tile<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CUDA_TRY(cudaFuncSetAttribute(k_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     done = 1;
     return BLD_OK;
@@ -1144,7 +1199,7 @@ int enqueue_fwd_y_R(bld_handle* h, int sp, bool first, bool last, const double2*
         fa.st_cu = sf->cu;
         fa.st_ct = sf->ct;
         fa.st_cd = sf->cd;
-        fa.st_div = sf->div;
+        fa.st_inv = 1.0 / sf->div;
     }
     return launch_fwd_y<R>(h, s, fa, nm);
 }
@@ -1326,7 +1381,7 @@ struct TuneKey {
 };
 struct TuneVal {
     Space adv, sgs;
-    int proj_variant;
+    int proj_variant, proj_tile;
 };
 std::mutex g_tune_mutex;
 std::map<TuneKey, TuneVal> g_tune_cache;
@@ -1335,7 +1390,7 @@ TuneKey tune_key(const bld_handle* h) {
     // any kernel-family switch in the environment makes its own entry
     int env = 0;
     for (const char* v : {"BLD_X_KERNEL", "BLD_Y_KERNEL", "BLD_XW_MINB", "BLD_PROJ_VARIANT", "BLD_X_LINES",
-                          "BLD_SGS_X_KERNEL"}) {
+                          "BLD_SGS_X_KERNEL", "BLD_X2_VARIANT", "BLD_PROJ_TILE"}) {
         const char* e = getenv(v);
         env = env * 31 + (e ? (int)(std::hash<std::string>{}(e) % 1000003) + 1 : 0);
     }
@@ -1373,6 +1428,7 @@ int autotune(bld_handle* h) {
             if (h->adv.on) x_chunks(h, h->adv);
             if (h->sgs.on) x_chunks(h, h->sgs);
             h->proj_variant = it->second.proj_variant;
+            h->proj_tile = it->second.proj_tile;
             return BLD_OK;
         }
     }
@@ -1383,6 +1439,7 @@ int autotune(bld_handle* h) {
         copy_tuning(v.adv, h->adv);
         copy_tuning(v.sgs, h->sgs);
         v.proj_variant = h->proj_variant;
+        v.proj_tile = h->proj_tile;
         g_tune_cache[key] = v;
     }
     return BLD_OK;
@@ -1555,7 +1612,12 @@ int autotune_impl(bld_handle* h) {
             if ((xbk == 1 && only_pipe) || (xbk == 2 && only_bw3)) continue;
             BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2, 0, 0}));
         }
-        if (sp == 0 && x2_ok(h, s) && (only_x2 || !xk || x2_asked)) BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1, 0}));
+        // the two-pass kernel's variants (BLD_X2_VARIANT = 0, 1, 2 forces one)
+        const char* x2v = getenv("BLD_X2_VARIANT");
+        const int x2_only = x2v && x2v[0] ? atoi(x2v) : -1;
+        for (int v = 0; v <= 2; ++v)
+            if (sp == 0 && x2_ok(h, s, v) && (only_x2 || !xk || x2_asked) && (x2_only < 0 || x2_only == v))
+                BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1 + v, 0}));
         if (bx >= 1e30f) return fail(BLD_ERR_INVALID_CONFIG, "no x kernel could be timed");
         set_pick(bp);
         x_chunks(h, s);
@@ -1605,8 +1667,30 @@ int autotune_impl(bld_handle* h) {
             }
         }
         h->proj_variant = bv;
+        // projections of stored stage values (the step's in-place projections):
+        // the chosen kernel against k_project_tile with 8 or 16 columns per block
+        // (BLD_PROJ_TILE = 0, 8, 16 keeps one)
+        const char* pt = getenv("BLD_PROJ_TILE");
+        const int only_t = (pt && pt[0]) ? atoi(pt) : -1;
+        float bt = 1e30f;
+        int btile = 0;
+        for (int ln : {0, 8, 16}) {
+            if (ln && !project_tile_ok(h, ln)) continue;
+            if (only_t >= 0 && ln != only_t) continue;
+            h->proj_tile = ln;
+            BLD_TRY(time_launches(h, [&] {
+                for (int k = 0; k < 3; ++k)
+                    BLD_TRY(enqueue_project(h, S_NONE, 1e-4, h->io, nullptr, nullptr, nullptr, h->io, 0, B));
+                return (int)BLD_OK;
+            }, 3, &t));
+            if (t < bt) {
+                bt = t;
+                btile = ln;
+            }
+        }
+        h->proj_tile = btile;
         const char* v = getenv("BLD_VERBOSE");
-        if (v && v[0] && v[0] != '0') fprintf(stderr, "bld autotune projection: variant %d\n", bv);
+        if (v && v[0] && v[0] != '0') fprintf(stderr, "bld autotune projection: variant %d, tile %d\n", bv, btile);
     }
     CUDA_TRY(cudaMemsetAsync(h->flag, 0, h->B * sizeof(int), h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1675,6 +1759,7 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
     a.pscr = h->pscr;
     a.gamma = h->gamma;
     a.alpha_c = h->alpha_c;
+    a.inv_alpha_c = h->inv_alpha_c;
     a.alpha_i = h->alpha_i;
     a.d1 = h->d1;
     a.d2 = h->d2;
@@ -1686,6 +1771,20 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
     const bool any_mean = h->cfg.mean[0] || h->cfg.mean[1];
     if (!a.pressure && !any_mean && kind == S_NONE && out == u) return BLD_OK;
     const int n3 = h->g.n3;
+    if (kind == S_NONE && h->proj_tile && project_tile_ok(h, h->proj_tile)) {
+        const int ln = h->proj_tile, lmax = n3 <= 128 ? 8 : 16;
+        CUtensorMap umap, gmap;
+        BLD_TRY(project_tmaps(h, u, ln, &umap, &gmap));
+        dim3 grid((unsigned)((h->g.F + ln - 1) / ln), nm);
+        dim3 block(ln, std::max(1, std::min(16, (n3 + lmax - 1) / lmax)));
+        const size_t sm = project_tile_smem(n3, ln);
+        if (lmax == 8 && ln == 8) k_project_tile<8, 8><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
+        else if (lmax == 8) k_project_tile<8, 16><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
+        else if (ln == 8) k_project_tile<16, 8><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
+        else k_project_tile<16, 16><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
+        CUDA_TRY(cudaGetLastError());
+        return BLD_OK;
+    }
     if (a.pressure && n3 <= 256 && h->proj_variant > 0) {
         // z-segmented solve: <= 16 segments of <= 8 (n3 <= 128) or <= 16 layers;
         // 16 modes side by side (256-byte rows), <= 256 threads; variant 1 lets the
@@ -1912,8 +2011,10 @@ int setup_space(bld_handle* h, Space& s, int dealias, int e1, int e2, bool is_ad
     s.ref_P1 = r1;
     s.ref_P2 = r2;
     for (int P : {s.P1, s.P2})
-        if (!(P % 2 == 0 && smooth23(P)))
-            return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size %d is not an even 2^a*3^b (kernels support radix 2/3 only)", P);
+        if (!(P % 2 == 0 && smooth2357(P)) || make_plan(P, h->fp32).nst == 0)
+            return fail(BLD_ERR_INVALID_CONFIG,
+                        "physical-domain size %d is not an even product of 2, 3, 5 and 7 with at most four "
+                        "codelet stages", P);
     if (s.P1 < 2 * k1 + 2 || s.P2 < 2 * k2 + 2)
         return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size (%d, %d) smaller than the resolved modes", s.P1, s.P2);
     if (s.P1 > 1024 || s.P2 > 1024) return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size above 1024");
@@ -1995,7 +2096,7 @@ void free_handle(bld_handle* h) {
     if (h->prof_prev) cudaFree(h->prof_prev);
     for (auto& kv : h->ens_graphs) cudaGraphExecDestroy(kv.second);
     void* ptrs[] = {h->u, h->t, h->du, h->dp, h->io, h->io2, h->pscr, h->gamma, h->d1, h->d2, h->DD1, h->DD2,
-                    h->alpha_c, h->alpha_i, h->alpha_ext, h->mean_w, h->lc2, h->li2, h->wall, h->src,
+                    h->alpha_c, h->inv_alpha_c, h->alpha_i, h->alpha_ext, h->mean_w, h->lc2, h->li2, h->wall, h->src,
                     h->mean_val, h->flag, h->active, h->adv.min, h->adv.mout, h->sgs.min, h->sgs.mout, h->pd_buf, h->pd_mixed,
                     h->prog_small, h->prog_buf, h->prog_mixed};
     for (void* p : ptrs)
@@ -2106,8 +2207,9 @@ int32_t bld_create(const bld_config* cfg, bld_handle** out) {
         DD2[j] = (double)(-k2 * k2) * (c2 * c2);
     }
     // ---- vertical factors alpha = N3 / (dx3/dzeta) (src/derivatives.jl:10-19)
-    std::vector<double> ac(n3), ai(n3 - 1), aext(n3 + 1), mw(n3);
+    std::vector<double> ac(n3), ai(n3 - 1), aext(n3 + 1), mw(n3), iac(n3);
     for (int i = 0; i < n3; ++i) ac[i] = (double)n3 / cfg->dx3_c[i];
+    for (int i = 0; i < n3; ++i) iac[i] = 1.0 / ac[i];
     for (int i = 0; i <= n3; ++i) aext[i] = (double)n3 / cfg->dx3_i[i];
     for (int i = 0; i < n3 - 1; ++i) ai[i] = aext[i + 1];
     const double L3 = cfg->x3_max - cfg->x3_min;
@@ -2117,6 +2219,7 @@ int32_t bld_create(const bld_config* cfg, bld_handle** out) {
     H_TRY(upload(h, &h->DD1, DD1));
     H_TRY(upload(h, &h->DD2, DD2));
     H_TRY(upload(h, &h->alpha_c, ac));
+    H_TRY(upload(h, &h->inv_alpha_c, iac));
     H_TRY(upload(h, &h->alpha_i, ai));
     H_TRY(upload(h, &h->alpha_ext, aext));
     H_TRY(upload(h, &h->mean_w, mw));
@@ -2653,7 +2756,8 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         const char* xk = sp == 0 ? "k_adv_x" : "k_sgs_x";
         char xname[96];
         if (sp == 0 && s.x2)
-            snprintf(xname, sizeof xname, "k_adv_x2<%s, %d, %d>", R, y2_radix_a(s.P1), y2_radix_b(s.P1));
+            snprintf(xname, sizeof xname, "k_adv_x2<%s, %d, %d%s>", R, y2_radix_a(s.P1), y2_radix_b(s.P1),
+                     s.x2 == 2 ? ", lean" : (s.x2 == 3 ? ", wide" : ""));
         else if (sp == 0 && s.xb)
             snprintf(xname, sizeof xname, "%s<%s, %d>", s.xb == 2 ? "k_adv_xp" : "k_adv_xb", R, s.P1 / 32);
         else if (sp == 0 && s.xw && s.xwmb > 1)
@@ -2683,10 +2787,16 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
     char tmp[160];
     const bool seg = h->cfg.pressure && h->g.n3 <= 256 && h->proj_variant > 0;
     if (seg)
-        snprintf(tmp, sizeof tmp, "%s\"projection\": \"k_project_seg<%d, %d, %s>\"}", out.size() > 1 ? ", " : "",
+        snprintf(tmp, sizeof tmp, "%s\"projection\": \"k_project_seg<%d, %d, %s>\"", out.size() > 1 ? ", " : "",
                  h->g.n3 <= 128 ? 8 : 16, h->proj_variant == 2 ? 2 : 1, h->proj_variant == 3 ? "true" : "false");
     else
-        snprintf(tmp, sizeof tmp, "%s\"projection\": \"k_project\"}", out.size() > 1 ? ", " : "");
+        snprintf(tmp, sizeof tmp, "%s\"projection\": \"k_project\"", out.size() > 1 ? ", " : "");
+    out += tmp;
+    if (h->proj_tile)
+        snprintf(tmp, sizeof tmp, ", \"projection_stored\": \"k_project_tile<%d, %d>\"}", h->g.n3 <= 128 ? 8 : 16,
+                 h->proj_tile);
+    else
+        snprintf(tmp, sizeof tmp, "}");
     out += tmp;
     if (out.size() + 1 > len) return fail(BLD_ERR_ARGUMENT, "buffer too small (%zu bytes needed)", out.size() + 1);
     memcpy(buf, out.c_str(), out.size() + 1);

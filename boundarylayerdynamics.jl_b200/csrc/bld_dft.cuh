@@ -1,10 +1,12 @@
-// Register DFT codelets of size N in {2,3,4,6,8,9,12,16,18,24,32}.
+// Register DFT codelets of size N in {2,3,4,5,6,7,8,9,10,12,14,15,16,18,24,32}.
 //
 // dft<R, N, DIR>(x) transforms x[0..N) in place (registers, compile-time
 // indices after unrolling): X[k] = sum_n x[n] exp(DIR * 2 pi i n k / N).
 // Composite sizes split N = Rr * M (Rr = 4, 2 or 3; decimation in time): M-point
 // DFTs of the Rr interleaved subsequences, twiddles W_N^(r k'), then Rr-point
-// DFTs.  The twiddles W_N^m of every codelet size live in one small table
+// DFTs.  The odd primes 5 and 7 pair x[k] with x[N - k]: with s_k = x[k] +
+// x[N - k] and d_k = x[k] - x[N - k], X[m] = x[0] + sum_k cos(2 pi k m / N) s_k
+// + i DIR sum_k sin(2 pi k m / N) d_k and X[N - m] the same with -i.  The twiddles W_N^m of every codelet size live in one small table
 // (constant memory on the device, a host array in host builds) filled from
 // long-double cos/sin on the host.
 #pragma once
@@ -13,7 +15,7 @@
 
 #include "bld_fft.cuh"
 
-#define BLD_WTAB_SIZE 125
+#define BLD_WTAB_SIZE 176
 
 // largest codelets compiled for double and single precision (register budget)
 #ifndef BLD_FP64_MAXR
@@ -26,11 +28,11 @@
 // offsets of W_N (m = 0..N-1) in the twiddle table
 __host__ __device__ constexpr int woff(int N) {
     return N == 6 ? 0 : N == 8 ? 6 : N == 9 ? 14 : N == 12 ? 23 : N == 16 ? 35 : N == 18 ? 51 : N == 24 ? 69
-         : N == 32 ? 93 : -1;
+         : N == 32 ? 93 : N == 5 ? 125 : N == 7 ? 130 : N == 10 ? 137 : N == 14 ? 147 : N == 15 ? 161 : -1;
 }
 __host__ __device__ constexpr bool codelet_size(int N) {
-    return N == 2 || N == 3 || N == 4 || N == 6 || N == 8 || N == 9 || N == 12 || N == 16 || N == 18 || N == 24 ||
-           N == 32;
+    return N == 2 || N == 3 || N == 4 || N == 5 || N == 6 || N == 7 || N == 8 || N == 9 || N == 10 || N == 12 ||
+           N == 14 || N == 15 || N == 16 || N == 18 || N == 24 || N == 32;
 }
 
 #ifdef __CUDACC__
@@ -128,6 +130,44 @@ __host__ __device__ __forceinline__ void dft(cplx<R> (&x)[N]) {
             x[1] = c_add(a1, a3);
             x[3] = c_sub(a1, a3);
         }
+    } else if constexpr (N == 5 || N == 7) {
+        constexpr int H = (N - 1) / 2;
+        C sp[H], dm[H];
+#pragma unroll
+        for (int k = 1; k <= H; ++k) {
+            sp[k - 1] = c_add(x[k], x[N - k]);
+            dm[k - 1] = c_sub(x[k], x[N - k]);
+        }
+        const C x0 = x[0];
+        C sum = x0;
+#pragma unroll
+        for (int k = 0; k < H; ++k) sum = c_add(sum, sp[k]);
+#pragma unroll
+        for (int m = 1; m <= H; ++m) {
+            C a = x0, b;
+            b.x = R(0);
+            b.y = R(0);
+#pragma unroll
+            for (int k = 1; k <= H; ++k) {
+                // W_N^(m k) = (cos, -sin) of 2 pi (m k mod N) / N
+                const C w = wtab<R>(woff(N) + (m * k) % N);
+                a.x += w.x * sp[k - 1].x;
+                a.y += w.x * sp[k - 1].y;
+                b.x -= w.y * dm[k - 1].x;
+                b.y -= w.y * dm[k - 1].y;
+            }
+            C ib;   // i b
+            ib.x = -b.y;
+            ib.y = b.x;
+            if (DIR > 0) {
+                x[m] = c_add(a, ib);
+                x[N - m] = c_sub(a, ib);
+            } else {
+                x[m] = c_sub(a, ib);
+                x[N - m] = c_add(a, ib);
+            }
+        }
+        x[0] = sum;
     } else {
         constexpr int Rr = (N % 4 == 0) ? 4 : (N % 2 == 0) ? 2 : 3;
         constexpr int M = N / Rr;
@@ -207,6 +247,11 @@ __device__ __forceinline__ cplx<R>* fft_big(cplx<R>* a, cplx<R>* b, int nlines, 
             case 4: stockham_stage<R, DIR, 4>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
             case 6: stockham_stage<R, DIR, 6>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
             case 8: stockham_stage<R, DIR, 8>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 5: stockham_stage<R, DIR, 5>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 7: stockham_stage<R, DIR, 7>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 10: stockham_stage<R, DIR, 10>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 14: stockham_stage<R, DIR, 14>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 15: stockham_stage<R, DIR, 15>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
             case 9:
                 if constexpr (MAXR >= 9) stockham_stage<R, DIR, 9>(src, dst, n, Ns, nlines, ls, ps, pos_fastest, tw);
                 break;
@@ -321,6 +366,11 @@ __device__ __forceinline__ void fft_inplace(cplx<R>* buf, int nlines, int ls, in
             case 4: inplace_load<R, 4>(x, buf, n, nlines, ls, ps, pos_fastest); break;
             case 6: inplace_load<R, 6>(x, buf, n, nlines, ls, ps, pos_fastest); break;
             case 8: inplace_load<R, 8>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 5: inplace_load<R, 5>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 7: inplace_load<R, 7>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 10: inplace_load<R, 10>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 14: inplace_load<R, 14>(x, buf, n, nlines, ls, ps, pos_fastest); break;
+            case 15: inplace_load<R, 15>(x, buf, n, nlines, ls, ps, pos_fastest); break;
             case 9: if constexpr (MAXR >= 9) inplace_load<R, 9>(x, buf, n, nlines, ls, ps, pos_fastest); break;
             case 12: if constexpr (MAXR >= 12) inplace_load<R, 12>(x, buf, n, nlines, ls, ps, pos_fastest); break;
             case 16: if constexpr (MAXR >= 16) inplace_load<R, 16>(x, buf, n, nlines, ls, ps, pos_fastest); break;
@@ -335,6 +385,11 @@ __device__ __forceinline__ void fft_inplace(cplx<R>* buf, int nlines, int ls, in
             case 4: inplace_store<R, DIR, 4>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
             case 6: inplace_store<R, DIR, 6>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
             case 8: inplace_store<R, DIR, 8>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 5: inplace_store<R, DIR, 5>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 7: inplace_store<R, DIR, 7>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 10: inplace_store<R, DIR, 10>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 14: inplace_store<R, DIR, 14>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
+            case 15: inplace_store<R, DIR, 15>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
             case 9: if constexpr (MAXR >= 9) inplace_store<R, DIR, 9>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
             case 12: if constexpr (MAXR >= 12) inplace_store<R, DIR, 12>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;
             case 16: if constexpr (MAXR >= 16) inplace_store<R, DIR, 16>(x, buf, n, Ns, nlines, ls, ps, pos_fastest, tw); break;

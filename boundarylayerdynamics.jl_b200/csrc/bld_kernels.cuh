@@ -923,14 +923,16 @@ struct FwdYArgs {
     double2* du;               // member stride g.mstride
     long long du_mstride;
     // fused stage update (k_fwd_y, modes 0 and 1): instead of the rate d, write
-    // sout = (st_cu su + st_ct state + st_cd d) / st_div, the explicit
+    // sout = (st_cu su + st_ct state + st_cd d) * st_inv, the explicit
     // SSP-RK stage value that the projection would otherwise form from d
-    // (src/ODEMethods.jl:101,143,157,164); su (NULL: no su term, st_ct = st_div = 1)
+    // (src/ODEMethods.jl:101,143,157,164; the reference divides by 2, 3 or 4,
+    // here the host passes the reciprocal: exact for 2 and 4, within one
+    // rounding of the quotient for 3); su (NULL: no su term, st_ct = st_inv = 1)
     // and sout have the member stride of du
     int fuse;
     const double2* su;
     double2* sout;
-    double st_cu, st_ct, st_cd, st_div;
+    double st_cu, st_ct, st_cd, st_inv;
     const double2* state;
     Linear lin;
     const double* d1;
@@ -1168,8 +1170,8 @@ __device__ __forceinline__ void fwd_y_epilogue(const FwdYArgs& a, const cplx<R>*
                     }
                     if constexpr (FZ == 1) {
                         const double2 uz = U[q];
-                        so[idx] = make_double2((a.st_cu * uz.x + a.st_ct * tz.x + a.st_cd * v.x) / a.st_div,
-                                               (a.st_cu * uz.y + a.st_ct * tz.y + a.st_cd * v.y) / a.st_div);
+                        so[idx] = make_double2((a.st_cu * uz.x + a.st_ct * tz.x + a.st_cd * v.x) * a.st_inv,
+                                               (a.st_cu * uz.y + a.st_ct * tz.y + a.st_cd * v.y) * a.st_inv);
                     } else {   // Euler stage: state + dt rate (src/ODEMethods.jl:101)
                         so[idx] = make_double2(tz.x + a.st_cd * v.x, tz.y + a.st_cd * v.y);
                     }
@@ -1531,6 +1533,7 @@ struct ProjArgs {
     const double* gamma;     // [n3][F]
     const double* alpha_c;   // [n3]
     const double* alpha_i;   // [n3-1]  (off-diagonal beta)
+    const double* inv_alpha_c;   // [n3] 1 / alpha_c, rounded as the division (segmented and tile kernels)
     const double* d1;
     const double* d2;
     double w_lo, w_hi;
@@ -1806,7 +1809,7 @@ __device__ __forceinline__ void project_seg_body(const ProjArgs& a, double2* til
                     a.out[o2 + z * F + c] = vz;
                     if (z < n - 1) a.out[o3 + z * F + c] = wz;
                 }
-                const double h = 1.0 / a.alpha_c[z];
+                const double h = a.inv_alpha_c[z];
                 double2 val;
                 val.x = (-e1 * uz.y) * h + (-e2 * vz.y) * h;
                 val.y = (e1 * uz.x) * h + (e2 * vz.x) * h;

@@ -383,3 +383,79 @@ def test_bounded_wait_timeout_exit(oracle, BLD):
     for f in om.fields:
         e = rel_l2(got[f], ref[f])
         assert e < 1e-12, (f, e)
+
+
+@pytest.mark.parametrize("variant,name", [("0", ""), ("1", ", lean"), ("2", ", wide")])
+@pytest.mark.parametrize("res", [(192, 8, 5), (64, 12, 6), (128, 10, 5), (85, 10, 5)])
+def test_twopass_x_variants_fp64(oracle, BLD, res, variant, name):
+    """The double-precision variants of the two-pass x kernel (two staging
+    buffers; one buffer with in-place second passes; 1.5x the threads), forced,
+    against the oracle at 1e-12."""
+    saved = {k: os.environ.get(k) for k in ("BLD_X_KERNEL", "BLD_X2_VARIANT")}
+    os.environ["BLD_X_KERNEL"] = "twopass"
+    os.environ["BLD_X2_VARIANT"] = variant
+    try:
+        gm = _build(BLD, res, "fp64")
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    xk = gm.kernels()["advection"]["x"]
+    assert xk.startswith("k_adv_x2<double") and xk.endswith(name + ">"), xk
+    om = _build(oracle, res)
+    st = _state(om, seed=sum(res) + int(variant))
+    ref = om.compute_rates(st)
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < 1e-12, (res, variant, f, e)
+
+
+@pytest.mark.parametrize("tile", ["8", "16"])
+@pytest.mark.parametrize("res,flux", [((16, 12, 7), False), ((24, 20, 40), True), ((16, 16, 200), False),
+                                      ((64, 64, 96), True), ((17, 12, 9), False)])
+def test_projection_tile(oracle, BLD, tile, res, flux):
+    """k_project_tile (each block's columns brought into shared memory by TMA
+    tensor copies, 8 or 16 columns per block) forced for the projections of
+    stored stage values: apply_projections and 10 chained SSP-RK33 steps against
+    the oracle, with and without ConstantMean.  An odd number of modes per layer
+    (17 x 12: F = 9 x 11) keeps the z-segmented kernel."""
+    saved = os.environ.get("BLD_PROJ_TILE")
+    os.environ["BLD_PROJ_TILE"] = tile
+
+    def build(api):
+        dom = api.Domain((4 * math.pi, 2 * math.pi, 2.0), api.SmoothWall(), api.SmoothWall())
+        procs = (api.incompressible_flow(1 / 180, constant_flux=(1.0, 0.3)) if flux
+                 else api.incompressible_flow(1 / 180, constant_forcing=1))
+        return api.Model(res, dom, procs)
+    try:
+        gm = build(BLD)
+    finally:
+        if saved is None:
+            del os.environ["BLD_PROJ_TILE"]
+        else:
+            os.environ["BLD_PROJ_TILE"] = saved
+    om = build(oracle)
+    F = om.state["vel1"].shape[1] * om.state["vel1"].shape[2]
+    stored = gm.kernels().get("projection_stored", "")
+    if F % 2 == 0:
+        assert stored == "k_project_tile<%d, %s>" % (8 if res[2] <= 128 else 16, tile), gm.kernels()
+    else:
+        assert stored == "", gm.kernels()
+    rng = np.random.default_rng(int(tile) + sum(res))
+    st = {f: rng.standard_normal(om.state[f].shape) + 1j * rng.standard_normal(om.state[f].shape)
+          for f in om.fields}
+    ref = om.apply_projections({f: v.copy() for f, v in st.items()})
+    got = gm.apply_projections({f: v.copy() for f, v in st.items()})
+    for f in om.fields:
+        assert rel_l2(got[f], ref[f]) < 1e-12, (tile, res, f)
+    st = _state(om, seed=int(tile) + 7)
+    gm.set_state(st)
+    om.state.update({f: v.copy() for f, v in st.items()})
+    gm.evolve(10 * 1e-4, 1e-4)
+    om.evolve(10 * 1e-4, 1e-4)
+    for f in om.fields:
+        e = rel_l2(gm.state[f], om.state[f])
+        assert e < 1e-10, (tile, res, f, e)
