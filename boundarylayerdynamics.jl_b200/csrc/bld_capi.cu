@@ -150,7 +150,8 @@ struct Space {
     int zmult = 2;                                  // x kernels: z-chunk count multiplier in halves (autotuned)
     int xb = 0;                                     // block of warps per row (advection): 1 three warps, 2 five (pipelined)
     int x2 = 0;                                     // 1 + V: two-pass shared-memory x kernel k_adv_x2<.., V> (advection)
-    int sx2 = 0;                                    // 1: SGS block x kernel with two-pass line transforms
+    int sx2 = 0;                                    // 1: SGS block x kernel with two-pass line transforms; 2: the same
+                                                    // with registers capped for two blocks of 256 threads per SM
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
@@ -810,8 +811,21 @@ int launch_adv_xb(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     return BLD_OK;
 }
 
+// the register-capped two-pass SGS x kernels: single precision, P1 >= 256
+// (where the uncapped kernel needs ~170 registers, one block per SM)
+__host__ __device__ constexpr bool sx2_capped_size(int P) { return P >= 256; }
+
 template <typename R, int P>
 int launch_sgs_x2_p(bld_handle* h, const Space& s, const XArgs& a, dim3 grid, int thr, size_t sm) {
+    if constexpr (sizeof(R) == 4 && sx2_capped_size(P)) {
+        if (s.sx2 == 2) {
+            if (s.PPT == 1)
+                k_sgs_x<R, 1, 0, P, 2><<<grid, thr, sm, h->stream>>>(a);
+            else
+                k_sgs_x<R, 2, 0, P, 2><<<grid, thr, sm, h->stream>>>(a);
+            return BLD_OK;
+        }
+    }
     if (s.PPT == 1)
         k_sgs_x<R, 1, 0, P><<<grid, thr, sm, h->stream>>>(a);
     else
@@ -820,8 +834,10 @@ int launch_sgs_x2_p(bld_handle* h, const Space& s, const XArgs& a, dim3 grid, in
 }
 
 // SGS x kernel with two-pass line transforms: compiled for the two-pass sizes and
-// one or two points per thread of the products
-bool sx2_ok(const bld_handle* h, const Space& s) { return y2_ok(s.P1, h->fp32); }
+// one or two points per thread of the products; v = 2: the register-capped form
+bool sx2_ok(const bld_handle* h, const Space& s, int v = 1) {
+    return y2_ok(s.P1, h->fp32) && (v == 1 || (h->fp32 && sx2_capped_size(s.P1)));
+}
 
 template <typename R>
 int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
@@ -962,6 +978,13 @@ int set_smem_limits_R() {
         BLD_SET_SX2(384)
         BLD_SET_SX2(512)
         BLD_SET_SX2(768)
+#define BLD_SET_SX2C(P) BLD_SET((k_sgs_x<R, 1, 0, P, 2>)); BLD_SET((k_sgs_x<R, 2, 0, P, 2>));
+        BLD_SET_SX2C(256)
+        BLD_SET_SX2C(288)
+        BLD_SET_SX2C(384)
+        BLD_SET_SX2C(512)
+        BLD_SET_SX2C(768)
+#undef BLD_SET_SX2C
     }
 #undef BLD_SET_SX2
     BLD_SET((k_adv_x<R, 1, 0>));
@@ -1457,7 +1480,9 @@ int autotune_impl(bld_handle* h) {
     const bool x2_asked = xk && !strcmp(xk, "twopass");
     // BLD_SGS_X_KERNEL=twopass keeps the SGS x pass on two-pass line transforms
     const char* sk = getenv("BLD_SGS_X_KERNEL");
-    const bool only_sx2 = sk && !strcmp(sk, "twopass") && h->sgs.on && sx2_ok(h, h->sgs);
+    // (twopass_capped: only the register-capped two-pass kernels, where compiled)
+    const bool sx2_capped_only = sk && !strcmp(sk, "twopass_capped") && h->sgs.on && sx2_ok(h, h->sgs, 2);
+    const bool only_sx2 = sk && (!strcmp(sk, "twopass") || sx2_capped_only) && h->sgs.on && sx2_ok(h, h->sgs);
     const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1, h->fp32) > 0;
     if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
     const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
@@ -1529,28 +1554,31 @@ int autotune_impl(bld_handle* h) {
         int bsx2 = 0;
         if (sp == 1 && sx2_ok(h, s) && !only_block && !only_lines) {
             float best2 = 1e30f;
-            int yt2 = 1, ppt2 = 1;
-            for (int yt = 1; yt <= 2; ++yt)
-                for (int ppt = 1; ppt <= 2; ++ppt) {
-                    const int thr = yt * s.P1 / ppt;
-                    if (s.P2 % yt || thr > 256 || thr < 32 || thr % 32) continue;
-                    s.sx2 = 1;
-                    s.xr = 0;
-                    s.YT = yt;
-                    s.PPT = ppt;
-                    if (smem_sgs(s, h->fp32) > 200 * 1024) continue;
-                    x_chunks(h, s);
-                    BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
-                    if (t < best2) {
-                        best2 = t;
-                        yt2 = yt;
-                        ppt2 = ppt;
+            int yt2 = 1, ppt2 = 1, v2 = 1;
+            for (int v = 1; v <= 2; ++v)
+                for (int yt = 1; yt <= 2; ++yt)
+                    for (int ppt = 1; ppt <= 2; ++ppt) {
+                        const int thr = yt * s.P1 / ppt;
+                        if (!sx2_ok(h, s, v) || s.P2 % yt || thr > 256 || thr < 32 || thr % 32) continue;
+                        if (sx2_capped_only && v != 2) continue;
+                        s.sx2 = v;
+                        s.xr = 0;
+                        s.YT = yt;
+                        s.PPT = ppt;
+                        if (smem_sgs(s, h->fp32) > 200 * 1024) continue;
+                        x_chunks(h, s);
+                        BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
+                        if (t < best2) {
+                            best2 = t;
+                            yt2 = yt;
+                            ppt2 = ppt;
+                            v2 = v;
+                        }
                     }
-                }
             s.sx2 = 0;
             if (best2 < 1e30f && (best2 < best || only_sx2)) {
                 best = best2;
-                bsx2 = 1;
+                bsx2 = v2;
                 bxr = 0;
                 byt = yt2;
                 bppt = ppt2;
@@ -2765,7 +2793,7 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         else if (sp == 0 && s.xw)
             snprintf(xname, sizeof xname, "k_adv_xw<%s, %d>", R, s.P1 / 32);
         else if (sp == 1 && s.sx2)
-            snprintf(xname, sizeof xname, "%s<%s, %d, 0, %d>", xk, R, s.PPT, s.P1);
+            snprintf(xname, sizeof xname, "%s<%s, %d, 0, %d%s>", xk, R, s.PPT, s.P1, s.sx2 == 2 ? ", 2" : "");
         else
             snprintf(xname, sizeof xname, "%s<%s, %d, %d>", xk, R, s.PPT, s.xr);
         char iname[64], fname[64];

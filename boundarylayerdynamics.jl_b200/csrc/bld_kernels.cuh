@@ -648,8 +648,8 @@ __device__ __forceinline__ void twopass_inplace(cplx<R>* buf, int nlines, int LP
 
 // TP > 0: the x transforms of a compile-time P1 = TP by twopass_inplace (the
 // other buffer is the scratch; lines at stride twopass_line), RAD must be 0
-template <typename R, int PPT, int RAD, int TP = 0>
-__global__ void __launch_bounds__(256) k_sgs_x(XArgs a) {
+template <typename R, int PPT, int RAD, int TP = 0, int MINB = 0>
+__global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P1 = a.P1, YT = a.YT, n3 = a.g.n3, k1max = a.g.k1max;

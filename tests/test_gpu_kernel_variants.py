@@ -285,7 +285,8 @@ def test_sgs_x_kernel_family(oracle, BLD, res, precision, tol, family):
                 os.environ["BLD_SGS_X_KERNEL"] = old
         p1 = gm.info.sgs_p1
         if p1 <= 288 or precision == "mixed":
-            assert gm.kernels()["sgs"]["x"].endswith(", 0, %d>" % p1), gm.kernels()
+            xk = gm.kernels()["sgs"]["x"]
+            assert xk.endswith(", 0, %d>" % p1) or xk.endswith(", 0, %d, 2>" % p1), gm.kernels()
     else:
         gm = _forced(BLD, family, res, precision, les=True)
     st = _state(om, seed=sum(res) + 2)
@@ -459,3 +460,26 @@ def test_projection_tile(oracle, BLD, tile, res, flux):
     for f in om.fields:
         e = rel_l2(gm.state[f], om.state[f])
         assert e < 1e-10, (tile, res, f, e)
+
+
+@pytest.mark.parametrize("res", [(256, 6, 4), (512, 4, 4)])
+def test_sgs_twopass_capped(oracle, BLD, res):
+    """The single-precision two-pass SGS x kernel compiled for two blocks of 256
+    threads per SM (registers capped at 128), forced, against the oracle (1e-5)."""
+    om = _build(oracle, res, les=True)
+    old = os.environ.get("BLD_SGS_X_KERNEL")
+    os.environ["BLD_SGS_X_KERNEL"] = "twopass_capped"
+    try:
+        gm = _build(BLD, res, "mixed", les=True)
+    finally:
+        if old is None:
+            del os.environ["BLD_SGS_X_KERNEL"]
+        else:
+            os.environ["BLD_SGS_X_KERNEL"] = old
+    assert gm.kernels()["sgs"]["x"].endswith(", 0, %d, 2>" % gm.info.sgs_p1), gm.kernels()
+    st = _state(om, seed=sum(res) + 5)
+    ref = om.compute_rates(st)
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < 1e-5, (res, f, e)
