@@ -150,8 +150,9 @@ struct Space {
     int zmult = 2;                                  // x kernels: z-chunk count multiplier in halves (autotuned)
     int xb = 0;                                     // block of warps per row (advection): 1 three warps, 2 five (pipelined)
     int x2 = 0;                                     // 1 + V: two-pass shared-memory x kernel k_adv_x2<.., V> (advection)
-    int sx2 = 0;                                    // 1: SGS block x kernel with two-pass line transforms; 2: the same
-                                                    // with registers capped for two blocks of 256 threads per SM
+    int sx2 = 0;                                    // SGS block x kernel with two-pass line transforms: 1 plain,
+                                                    // 2 registers capped for two blocks of 256 threads per SM,
+                                                    // 3 / 4 as 1 / 2 with the input rows staged by bulk copies
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
@@ -335,10 +336,18 @@ size_t smem_y_term(int P2, int lines, int wfft, bool fp32) {
 size_t smem_adv(const Space& s, bool fp32) {
     return (size_t)(s.P1 + 2 * 3 * s.YT * (s.P1 + (s.xr ? 32 : 0))) * csize(fp32);
 }
-size_t smem_sgs(const Space& s, bool fp32) {
+// the two-pass SGS kernel stages its input rows by bulk copies when a block's
+// YT rows of K1 values fill whole 16-byte units
+bool sgs_stage_fits(const Space& s, bool fp32, int K1) { return !fp32 || K1 % 2 == 0 || s.YT % 2 == 0; }
+bool sgs_staged(const Space& s, bool fp32, int K1) { return s.sx2 >= 3 && sgs_stage_fits(s, fp32, K1); }
+
+size_t smem_sgs(const Space& s, bool fp32, int K1) {
     if (s.sx2) {
         const int A = y2_radix_a(s.P1), B = y2_radix_b(s.P1);
         const int lp = fp32 ? twopass_line<float2>(A, B) : twopass_line<double2>(A, B);
+        if (sgs_staged(s, fp32, K1))
+            return (size_t)sgs_stage_offset(s.P1, 5 * s.YT, lp, (int)csize(fp32)) + 128 +
+                   (size_t)2 * 9 * s.YT * K1 * csize(fp32);
         return (size_t)(s.P1 + 2 * 5 * s.YT * lp) * csize(fp32);
     }
     return (size_t)(s.P1 + 2 * 5 * s.YT * (s.P1 + (s.xr ? 32 : 0))) * csize(fp32);
@@ -818,7 +827,7 @@ __host__ __device__ constexpr bool sx2_capped_size(int P) { return P >= 256; }
 template <typename R, int P>
 int launch_sgs_x2_p(bld_handle* h, const Space& s, const XArgs& a, dim3 grid, int thr, size_t sm) {
     if constexpr (sizeof(R) == 4 && sx2_capped_size(P)) {
-        if (s.sx2 == 2) {
+        if (s.sx2 == 2 || s.sx2 == 4) {
             if (s.PPT == 1)
                 k_sgs_x<R, 1, 0, P, 2><<<grid, thr, sm, h->stream>>>(a);
             else
@@ -836,14 +845,14 @@ int launch_sgs_x2_p(bld_handle* h, const Space& s, const XArgs& a, dim3 grid, in
 // SGS x kernel with two-pass line transforms: compiled for the two-pass sizes and
 // one or two points per thread of the products; v = 2: the register-capped form
 bool sx2_ok(const bld_handle* h, const Space& s, int v = 1) {
-    return y2_ok(s.P1, h->fp32) && (v == 1 || (h->fp32 && sx2_capped_size(s.P1)));
+    return y2_ok(s.P1, h->fp32) && (v % 2 == 1 || (h->fp32 && sx2_capped_size(s.P1)));
 }
 
 template <typename R>
 int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     dim3 grid(s.P2 / s.YT, s.nchunks, nm);
     const int thr = s.YT * s.P1 / s.PPT;
-    const size_t sm = smem_sgs(s, sizeof(R) == 4);
+    const size_t sm = smem_sgs(s, sizeof(R) == 4, h->g.K1);
     if (s.sx2) {
         switch (s.P1) {
             case 64: BLD_TRY((launch_sgs_x2_p<R, 64>(h, s, a, grid, thr, sm))); break;
@@ -1152,6 +1161,8 @@ int enqueue_x_R(bld_handle* h, int sp, int m0, int nm) {
     xa.dyn_hi = h->dyn_hi;
     xa.w_lo = h->w_lo;
     xa.w_hi = h->w_hi;
+    xa.staged = sgs_staged(s, sizeof(R) == 4, h->g.K1) ? 1 : 0;
+    xa.flag = h->flag;
     xa.active = h->mask_on ? h->active : nullptr;
     if (sp == 0) {
         if (s.x2) return launch_adv_x2<R>(h, s, xa, nm);
@@ -1481,8 +1492,11 @@ int autotune_impl(bld_handle* h) {
     // BLD_SGS_X_KERNEL=twopass keeps the SGS x pass on two-pass line transforms
     const char* sk = getenv("BLD_SGS_X_KERNEL");
     // (twopass_capped: only the register-capped two-pass kernels, where compiled)
+    // (twopass_staged: only those with the input rows staged by bulk copies)
     const bool sx2_capped_only = sk && !strcmp(sk, "twopass_capped") && h->sgs.on && sx2_ok(h, h->sgs, 2);
-    const bool only_sx2 = sk && (!strcmp(sk, "twopass") || sx2_capped_only) && h->sgs.on && sx2_ok(h, h->sgs);
+    const bool sx2_staged_only = sk && !strcmp(sk, "twopass_staged") && h->sgs.on && sx2_ok(h, h->sgs);
+    const bool only_sx2 = sk && (!strcmp(sk, "twopass") || sx2_capped_only || sx2_staged_only) && h->sgs.on &&
+                          sx2_ok(h, h->sgs);
     const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1, h->fp32) > 0;
     if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
     const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
@@ -1555,17 +1569,19 @@ int autotune_impl(bld_handle* h) {
         if (sp == 1 && sx2_ok(h, s) && !only_block && !only_lines) {
             float best2 = 1e30f;
             int yt2 = 1, ppt2 = 1, v2 = 1;
-            for (int v = 1; v <= 2; ++v)
-                for (int yt = 1; yt <= 2; ++yt)
+            for (int v = 1; v <= 4; ++v)
+                for (int yt = 1; yt <= 4; yt *= 2)
                     for (int ppt = 1; ppt <= 2; ++ppt) {
                         const int thr = yt * s.P1 / ppt;
                         if (!sx2_ok(h, s, v) || s.P2 % yt || thr > 256 || thr < 32 || thr % 32) continue;
-                        if (sx2_capped_only && v != 2) continue;
+                        if ((sx2_capped_only && v % 2 == 1) || (sx2_staged_only && v < 3)) continue;
+                        s.YT = yt;
+                        if (v >= 3 && !sgs_stage_fits(s, h->fp32, h->g.K1)) continue;
                         s.sx2 = v;
                         s.xr = 0;
                         s.YT = yt;
                         s.PPT = ppt;
-                        if (smem_sgs(s, h->fp32) > 200 * 1024) continue;
+                        if (smem_sgs(s, h->fp32, h->g.K1) > 200 * 1024) continue;
                         x_chunks(h, s);
                         BLD_TRY(time_launches(h, [&] { return enqueue_x(h, sp, 0, B); }, 3, &t));
                         if (t < best2) {
@@ -1662,9 +1678,9 @@ int autotune_impl(bld_handle* h) {
         s.fwd = bf;
         const char* v = getenv("BLD_VERBOSE");
         if (v && v[0] && v[0] != '0')
-            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d wfft=%d | x YT=%d PPT=%d xr=%d warps=%d bw=%d chunks=%d | fwd all=%d NL=%d thr=%d wfft=%d\n",
-                    sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.inv.wfft, s.YT, s.PPT, s.xr, s.xw, (int)s.xb,
-                    s.nchunks, s.fwd.all, s.fwd.NL, s.fwd.thr, s.fwd.wfft);
+            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d wfft=%d tp=%d | x YT=%d PPT=%d xr=%d warps=%d bw=%d x2=%d sx2=%d chunks=%d | fwd all=%d NL=%d thr=%d wfft=%d tp=%d\n",
+                    sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.inv.wfft, s.inv.tp, s.YT, s.PPT, s.xr, s.xw, (int)s.xb,
+                    s.x2, s.sx2, s.nchunks, s.fwd.all, s.fwd.NL, s.fwd.thr, s.fwd.wfft, s.fwd.tp);
     }
     if (h->cfg.pressure && h->g.n3 <= 256) {
         float best = 1e30f, t = 0;
@@ -2067,7 +2083,7 @@ int setup_space(bld_handle* h, Space& s, int dealias, int e1, int e2, bool is_ad
     BLD_TRY(dalloc(h, &s.min, (size_t)s.min_ms * h->B * cs));
     BLD_TRY(dalloc(h, &s.mout, (size_t)s.mout_ms * h->B * cs));
     CUDA_TRY(cudaMemset(s.mout, 0, (size_t)s.mout_ms * h->B * cs));
-    const size_t sm = is_adv ? smem_adv(s, h->fp32) : smem_sgs(s, h->fp32);
+    const size_t sm = is_adv ? smem_adv(s, h->fp32) : smem_sgs(s, h->fp32, h->g.K1);
     if (sm > 200 * 1024 || (size_t)(s.P2 + 2 * s.P2 * s.fsets * s.fwd.NL) * csize(h->fp32) > 200 * 1024)
         return fail(BLD_ERR_INVALID_CONFIG, "physical-domain size (%d, %d) needs too much shared memory", s.P1, s.P2);
     s.on = true;
@@ -2793,7 +2809,7 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         else if (sp == 0 && s.xw)
             snprintf(xname, sizeof xname, "k_adv_xw<%s, %d>", R, s.P1 / 32);
         else if (sp == 1 && s.sx2)
-            snprintf(xname, sizeof xname, "%s<%s, %d, 0, %d%s>", xk, R, s.PPT, s.P1, s.sx2 == 2 ? ", 2" : "");
+            snprintf(xname, sizeof xname, "%s<%s, %d, 0, %d%s>", xk, R, s.PPT, s.P1, s.sx2 % 2 == 0 ? ", 2" : "");
         else
             snprintf(xname, sizeof xname, "%s<%s, %d, %d>", xk, R, s.PPT, s.xr);
         char iname[64], fname[64];

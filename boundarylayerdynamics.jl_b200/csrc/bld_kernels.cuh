@@ -20,6 +20,7 @@
 #include "bld_fft.cuh"
 #include "bld_dft.cuh"
 #include "bld_warpfft.cuh"
+#include "bld_tma.cuh"
 
 #define BLD_MAXT 10
 #define BLD_MAXC 4
@@ -390,6 +391,11 @@ struct XArgs {
     const double* wall;      // [members][4]: strain factor lo, hi; stress factor lo, hi
     int dyn_lo, dyn_hi;      // rough wall (dynamic wall-model values) below / above
     double w_lo, w_hi;       // Dirichlet values of vel3
+    // two-pass SGS kernel: the input rows of layer j + 1 are copied into shared
+    // memory by 1-d TMA bulk copies while layer j is processed (needs YT K1
+    // elements to fill whole 16-byte units); a timed-out wait sets flag[m]
+    int staged;
+    int* flag;
 };
 
 template <typename C>
@@ -646,6 +652,13 @@ __device__ __forceinline__ void twopass_inplace(cplx<R>* buf, int nlines, int LP
     __syncthreads();
 }
 
+// byte offset of the staging area of the two-pass SGS x kernel: after the
+// twiddles and the two line buffers, rounded up to 128 bytes; the area holds
+// the two barriers (128 bytes) and 2 x 9 staged rows of YT K1 values
+__host__ __device__ constexpr int sgs_stage_offset(int P1, int NLin, int LP, int csz) {
+    return ((P1 + 2 * NLin * LP) * csz + 127) & ~127;
+}
+
 // TP > 0: the x transforms of a compile-time P1 = TP by twopass_inplace (the
 // other buffer is the scratch; lines at stride twopass_line), RAD must be 0
 template <typename R, int PPT, int RAD, int TP = 0, int MINB = 0>
@@ -666,6 +679,34 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
     const int z0 = blockIdx.y * a.zchunk;
     const int z1 = min(n3, z0 + a.zchunk);
     const int nthr = blockDim.x;
+    // staging (two-pass form): barriers and 2 x 9 terms x YT rows after the line
+    // buffers, on 128-byte boundaries (sgs_stage_offset)
+    const bool staged = TP > 0 && a.staged;
+    const int K1 = a.g.K1;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + sgs_stage_offset(P1, NLin, LP, (int)sizeof(C)));
+    C* stage = reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(bar) + 128);
+    const unsigned row_bytes = (unsigned)(YT * K1 * (int)sizeof(C));
+    const long long wait_limit = g_bld_wait_limit;
+    const int jb = max(0, z0 - 2);
+    // input terms of C layer j: u, v, u1, u2, v1, v2, and below the top layer w, w1, w2
+    auto issue = [&](int j, int sl) {
+        const bool hi = (j <= n3 - 2);
+        mbar_arrive_expect_tx(&bar[sl], (hi ? 9u : 6u) * row_bytes);
+        for (int t = 0; t < 9; ++t)
+            if (hi || (t != 2 && t != 7 && t != 8))
+                bulk_load(stage + (size_t)(sl * 9 + t) * YT * K1, mrow(reinterpret_cast<const C*>(a.min) +
+                                                                          (long long)m * a.min_mstride, a, t, j, y0),
+                          row_bytes, &bar[sl]);
+    };
+    if (staged) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar[0], 1);
+            mbar_init(&bar[1], 1);
+            fence_async_shared();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && jb <= n3 - 1) issue(jb, 0);
+    }
     const C* twg = reinterpret_cast<const C*>(a.tw);
     if constexpr (TP > 0) {
         for (int i = threadIdx.x; i < TP; i += blockDim.x) tw[i] = twg[(i / TA) * (i % TA)];
@@ -691,10 +732,21 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
     }
 
     const int jend = min(n3, z1 + 1);
-    for (int j = max(0, z0 - 2); j <= jend; ++j) {
+    for (int j = jb; j <= jend; ++j) {
         const bool hasC = (j <= n3 - 1), hasI = (j <= n3 - 2);
         C* cur = bufA;
         C* phys = bufA;
+        const int sl = (j - jb) & 1;
+        bool arrived = true;
+        if (staged && hasC) {
+            // slot sl ^ 1 was last read by layer j - 1's packing, several barriers ago
+            if (threadIdx.x == 0 && j + 1 <= min(jend, n3 - 1)) {
+                fence_async_shared();
+                issue(j + 1, sl ^ 1);
+            }
+            arrived = mbar_wait_bounded(&bar[sl], ((j - jb) >> 1) & 1, wait_limit);
+        }
+        const C* srow = stage + (size_t)sl * 9 * YT * K1;
         if (hasC) {
             const int nk = k1max + 1;
             for (int i = threadIdx.x; i < NLin * (P1 - 2 * k1max - 1); i += nthr) {
@@ -714,8 +766,13 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
                         // only below the top layer; table lookups keep the loads branch-free
                         const int ta = (0x82530 >> (4 * qq)) & 0xF, tb = (0xF7641 >> (4 * qq)) & 0xF;
                         const bool oka = qq < 3 || hasI, okb = qq < 3 || (qq == 3 && hasI);
-                        if (oka) va[q] = mrow(Min, a, ta, j, y)[k];
-                        if (okb) vb[q] = mrow(Min, a, tb, j, y)[k];
+                        if (staged) {
+                            if (oka) va[q] = srow[(ta * YT + yl) * K1 + k];
+                            if (okb) vb[q] = srow[(tb * YT + yl) * K1 + k];
+                        } else {
+                            if (oka) va[q] = mrow(Min, a, ta, j, y)[k];
+                            if (okb) vb[q] = mrow(Min, a, tb, j, y)[k];
+                        }
                     }
                 }
 #pragma unroll
@@ -727,7 +784,16 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
                     }
                 }
             }
-            __syncthreads();
+            // a block whose staged wait expired stops here (uniformly), after the
+            // copies it issued have landed
+            if (__syncthreads_or(!arrived)) {
+                if (threadIdx.x == 0) {
+                    atomicOr(a.flag + m, BLD_FLAG_TIMEOUT);
+                    mbar_wait_bounded(&bar[sl], ((j - jb) >> 1) & 1);
+                    if (j + 1 <= min(jend, n3 - 1)) mbar_wait_bounded(&bar[sl ^ 1], ((j + 1 - jb) >> 1) & 1);
+                }
+                return;
+            }
             if constexpr (TP > 0) {
                 twopass_inplace<R, TA, TB, +1>(bufA, NLin, LP, bufB, tw);
             } else if constexpr (RAD > 0) {

@@ -483,3 +483,41 @@ def test_sgs_twopass_capped(oracle, BLD, res):
     for f in om.fields:
         e = rel_l2(got[f], ref[f])
         assert e < 1e-5, (res, f, e)
+
+
+@pytest.mark.parametrize("res,precision,tol,sgs_sizes", [((64, 12, 6), "fp64", 1e-12, None),
+                                                         ((128, 8, 5), "mixed", 1e-5, None),
+                                                         ((512, 4, 4), "mixed", 1e-5, None),
+                                                         ((58, 12, 5), "mixed", 1e-5, (96, 96))])
+def test_sgs_twopass_staged(oracle, BLD, res, precision, tol, sgs_sizes):
+    """The two-pass SGS x kernel with its input rows staged in shared memory by 1-d
+    TMA bulk copies one layer ahead (forced), against the oracle.  The last case
+    runs the Smagorinsky model at an explicit 96 x 96 grid for 58 x 12 modes:
+    K1 = 29 single-precision values per row, so a block takes an even number of
+    rows to fill whole 16-byte units."""
+    def build(api, prec=None):
+        if sgs_sizes is None:
+            return _build(api, res, prec, les=True)
+        dom = api.Domain((2 * math.pi, math.pi, 1.0), api.RoughWall(1e-4), api.FreeSlipBoundary())
+        procs = api.incompressible_flow(1e-5, constant_forcing=1,
+                                        sgs_model=api.StaticSmagorinskyModel(dealiasing=sgs_sizes))
+        kw = {} if prec is None else dict(precision=prec)
+        return api.Model(res, dom, procs, **kw)
+    om = build(oracle)
+    old = os.environ.get("BLD_SGS_X_KERNEL")
+    os.environ["BLD_SGS_X_KERNEL"] = "twopass_staged"
+    try:
+        gm = build(BLD, precision)
+    finally:
+        if old is None:
+            del os.environ["BLD_SGS_X_KERNEL"]
+        else:
+            os.environ["BLD_SGS_X_KERNEL"] = old
+    xk = gm.kernels()["sgs"]["x"]
+    assert xk.startswith("k_sgs_x<") and ", 0, %d" % gm.info.sgs_p1 in xk, gm.kernels()
+    st = _state(om, seed=sum(res) + 9)
+    ref = om.compute_rates(st)
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < tol, (res, precision, f, e)
