@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B),
         __syncthreads();
         // ---- unpack the two real lines of each spectrum and write the modes
         for (int task = threadIdx.x; task < (lf1 - lf0) * K1; task += T) {
-            const int L = lf0 + task / K1, f = task % K1;
+            const int Lr = fdiv(task, a.k1_magic), L = lf0 + Lr, f = task - Lr * K1;
             const C Zk = Ph[L * PHL + f], Zr = Ph[L * PHL + (P - f) % P];
             const C va = mk<R>((Zk.x + Zr.x) * R(0.5), (Zk.y - Zr.y) * R(0.5));
             const C vb = mk<R>((Zk.y + Zr.y) * R(0.5), -(Zk.x - Zr.x) * R(0.5));

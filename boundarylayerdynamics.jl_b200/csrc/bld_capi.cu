@@ -1162,6 +1162,8 @@ int enqueue_x_R(bld_handle* h, int sp, int m0, int nm) {
     xa.w_lo = h->w_lo;
     xa.w_hi = h->w_hi;
     xa.staged = sgs_staged(s, sizeof(R) == 4, h->g.K1) ? 1 : 0;
+    xa.k1_magic = fdiv_magic((unsigned)h->g.K1);
+    xa.p1_magic = fdiv_magic((unsigned)s.P1);
     xa.flag = h->flag;
     xa.active = h->mask_on ? h->active : nullptr;
     if (sp == 0) {

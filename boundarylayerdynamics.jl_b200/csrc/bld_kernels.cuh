@@ -396,7 +396,22 @@ struct XArgs {
     // elements to fill whole 16-byte units); a timed-out wait sets flag[m]
     int staged;
     int* flag;
+    // ceil(2^32 / K1) and ceil(2^32 / P1) (0 for a divisor of 1): fdiv
+    unsigned k1_magic, p1_magic;
 };
+
+// n / d for 0 <= n < 2^16 and 1 <= d < 2^16 by one multiply-high with
+// magic = ceil(2^32 / d) (0 for d = 1): with n = q d + r, n magic / 2^32 exceeds
+// n / d by less than 2^-16 <= 1 / d, so its floor is q.  Replaces runtime integer
+// divisions (tens of instructions each) in the index arithmetic of the x kernels.
+__host__ __device__ __forceinline__ int fdiv(int n, unsigned magic) {
+#ifdef __CUDA_ARCH__
+    return magic ? (int)__umulhi((unsigned)n, magic) : n;
+#else
+    return magic ? (int)(((unsigned long long)(unsigned)n * magic) >> 32) : n;
+#endif
+}
+inline unsigned fdiv_magic(unsigned d) { return d <= 1 ? 0u : (unsigned)(((1ull << 32) + d - 1) / d); }
 
 template <typename C>
 __device__ __forceinline__ const C* mrow(const C* M, const XArgs& a, int t, int z, int y) {
@@ -494,7 +509,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
                 const int i = i0 + q * nthr + threadIdx.x;
                 va[q] = vb[q] = mk<R>(0, 0);
                 if (i < NLin * nk) {
-                    const int line = i / nk, k = i - line * nk;
+                    const int line = fdiv(i, a.k1_magic), k = i - line * nk;
                     const int yl = line / 3, qq = line - yl * 3, y = y0 + yl;
                     // packed line qq: terms (0,1) (5,2) (3,4); w and the I-node
                     // vorticities only below the top layer (branch-free loads)
@@ -508,7 +523,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
             for (int q = 0; q < 4; ++q) {
                 const int i = i0 + q * nthr + threadIdx.x;
                 if (i < NLin * nk) {
-                    const int line = i / nk, k = i - line * nk;
+                    const int line = fdiv(i, a.k1_magic), k = i - line * nk;
                     put_packed<R, RAD>(cur + line * LP, va[q], vb[q], k, P1);
                 }
             }
@@ -532,7 +547,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
 #pragma unroll
         for (int i = 0; i < PPT; ++i) {
             const int p = threadIdx.x + i * nthr;
-            const int yl = p / P1, x = p - yl * P1;
+            const int yl = fdiv(p, a.p1_magic), x = p - yl * P1;
             const int xs = swz<C, RAD>(x);
             const C c0 = phys[(yl * 3 + 0) * LP + xs];
             const C c1 = phys[(yl * 3 + 1) * LP + xs];
@@ -582,7 +597,7 @@ __global__ void __launch_bounds__(256) k_adv_x(XArgs a) {
             }
             const int nk = k1max + 1;
             for (int i = threadIdx.x; i < NLout * nk; i += nthr) {
-                const int line = i / nk, k = i - line * nk;
+                const int line = fdiv(i, a.k1_magic), k = i - line * nk;
                 C A, B;
                 unpack_pair<R, RAD>(r2 + line * LP, k, P1, A, B);
                 if (line < YT) {
@@ -760,7 +775,7 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
                     const int i = i0 + q * nthr + threadIdx.x;
                     va[q] = vb[q] = mk<R>(0, 0);
                     if (i < NLin * nk) {
-                        const int line = i / nk, k = i - line * nk;
+                        const int line = fdiv(i, a.k1_magic), k = i - line * nk;
                         const int yl = line / 5, qq = line - yl * 5, y = y0 + yl;
                         // packed line qq: terms (0,1) (3,4) (5,6) (2,7) (8,-), the last two
                         // only below the top layer; table lookups keep the loads branch-free
@@ -779,7 +794,7 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
                 for (int q = 0; q < 4; ++q) {
                     const int i = i0 + q * nthr + threadIdx.x;
                     if (i < NLin * nk) {
-                        const int line = i / nk, k = i - line * nk;
+                        const int line = fdiv(i, a.k1_magic), k = i - line * nk;
                         put_packed<R, RAD>(cur + line * LP, va[q], vb[q], k, P1);
                     }
                 }
@@ -811,7 +826,7 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
 #pragma unroll
         for (int i = 0; i < PPT; ++i) {
             const int p = threadIdx.x + i * nthr;
-            const int yl = p / P1, x = p - yl * P1;
+            const int yl = fdiv(p, a.p1_magic), x = p - yl * P1;
             R u = 0, v = 0, u1 = 0, u2 = 0, v1 = 0, v2 = 0, w = whi, w1 = 0, w2 = 0;
             const int xs = swz<C, RAD>(x);
             if (hasC) {
@@ -932,7 +947,7 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
             }
             const int nk = k1max + 1;
             for (int i = threadIdx.x; i < NLout * nk; i += nthr) {
-                const int line = i / nk, k = i - line * nk;
+                const int line = fdiv(i, a.k1_magic), k = i - line * nk;
                 const int yl = line / 4, q = line - yl * 4, y = y0 + yl;
                 C A, B;
                 unpack_pair<R, RAD>(r2 + line * LP, k, P1, A, B);

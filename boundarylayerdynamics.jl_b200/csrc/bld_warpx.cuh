@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(96) k_adv_xb(XArgs a) {
     auto issue = [&](int j, C* buf) {
         const int nrows = (j < n3 - 1) ? 6 : 3;
         for (int i = threadIdx.x; i < nrows * K1; i += blockDim.x) {
-            const int r = i / K1, k = i - r * K1;
+            const int r = fdiv(i, a.k1_magic), k = i - r * K1;
             const int t = r < 2 ? r : (r == 2 ? 5 : r - 1);
             cp_async_elem<C>(buf + i, mrow(Min, a, t, j, y) + k);
         }
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(160) k_adv_xp(XArgs a) {
     auto issue = [&](int j, C* buf) {
         const int nrows = (j < n3 - 1) ? 6 : 3;
         for (int i = threadIdx.x; i < nrows * K1; i += blockDim.x) {
-            const int r = i / K1, k = i - r * K1;
+            const int r = fdiv(i, a.k1_magic), k = i - r * K1;
             const int t = r < 2 ? r : (r == 2 ? 5 : r - 1);
             cp_async_elem<C>(buf + i, mrow(Min, a, t, j, y) + k);
         }
