@@ -23,6 +23,7 @@
 #include "bld_warpx.cuh"
 #include "bld_advx2.cuh"
 #include "bld_project_tile.cuh"
+#include "bld_sgsx2.cuh"
 
 double2 h_wtab64[BLD_WTAB_SIZE];
 float2 h_wtab32[BLD_WTAB_SIZE];
@@ -153,6 +154,7 @@ struct Space {
     int sx2 = 0;                                    // SGS block x kernel with two-pass line transforms: 1 plain,
                                                     // 2 registers capped for two blocks of 256 threads per SM,
                                                     // 3 / 4 as 1 / 2 with the input rows staged by bulk copies
+    int sxk = 0;                                    // 1: SGS x kernel k_sgs_x2 (rows staged by bulk copies, two-pass lines)
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
@@ -275,7 +277,8 @@ int pick_y(int P2, bool fp32, int sets) {
 // fill the GPU a few times over, at least 8 layers per chunk
 void x_chunks(const bld_handle* h, Space& s) {
     const int n3 = h->g.n3;
-    const int rows = s.x2 ? x2_rows((int)csize(h->fp32), s.P1) : (s.xb ? 1 : (s.xw ? s.xw : s.YT));
+    const int rows = s.x2 ? x2_rows((int)csize(h->fp32), s.P1)
+                           : (s.sxk ? sx2_rows((int)csize(h->fp32), s.P1) : (s.xb ? 1 : (s.xw ? s.xw : s.YT)));
     const long long blocks_per_chunk = (long long)((s.P2 + rows - 1) / rows) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
     want = std::min(want, std::max(1, n3 / 8));
@@ -848,8 +851,48 @@ bool sx2_ok(const bld_handle* h, const Space& s, int v = 1) {
     return y2_ok(s.P1, h->fp32) && (v % 2 == 1 || (h->fp32 && sx2_capped_size(s.P1)));
 }
 
+// k_sgs_x2: compiled for the two-pass sizes; whole row groups per block
+bool sxk_ok(const bld_handle* h, const Space& s) {
+    const int cs = (int)csize(h->fp32);
+    return y2_ok(s.P1, h->fp32) && s.P2 % sx2_rows(cs, s.P1) == 0 &&
+           sx2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, cs) <= 227 * 1024;
+}
+
+template <typename R, int P>
+int launch_sgs_xk_p(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
+    constexpr int NR = sx2_rows((int)sizeof(cplx<R>), P);
+    dim3 grid(s.P2 / NR, s.nchunks, nm);
+    const size_t sm = sx2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>));
+    k_sgs_x2<R, A, B><<<grid, sx2_threads(B, NR), sm, h->stream>>>(a);
+    return BLD_OK;
+}
+
+template <typename R>
+int launch_sgs_xk(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    switch (s.P1) {
+        case 64: BLD_TRY((launch_sgs_xk_p<R, 64>(h, s, a, nm))); break;
+        case 96: BLD_TRY((launch_sgs_xk_p<R, 96>(h, s, a, nm))); break;
+        case 128: BLD_TRY((launch_sgs_xk_p<R, 128>(h, s, a, nm))); break;
+        case 144: BLD_TRY((launch_sgs_xk_p<R, 144>(h, s, a, nm))); break;
+        case 192: BLD_TRY((launch_sgs_xk_p<R, 192>(h, s, a, nm))); break;
+        case 256: BLD_TRY((launch_sgs_xk_p<R, 256>(h, s, a, nm))); break;
+        case 288: BLD_TRY((launch_sgs_xk_p<R, 288>(h, s, a, nm))); break;
+        default:
+            if constexpr (sizeof(R) == 4) {
+                if (s.P1 == 384) { BLD_TRY((launch_sgs_xk_p<R, 384>(h, s, a, nm))); break; }
+                if (s.P1 == 512) { BLD_TRY((launch_sgs_xk_p<R, 512>(h, s, a, nm))); break; }
+                if (s.P1 == 768) { BLD_TRY((launch_sgs_xk_p<R, 768>(h, s, a, nm))); break; }
+            }
+            return fail(BLD_ERR_INVALID_CONFIG, "no k_sgs_x2 kernel for P1=%d", s.P1);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
+}
+
 template <typename R>
 int launch_sgs_x(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    if (s.sxk) return launch_sgs_xk<R>(h, s, a, nm);
     dim3 grid(s.P2 / s.YT, s.nchunks, nm);
     const int thr = s.YT * s.P1 / s.PPT;
     const size_t sm = smem_sgs(s, sizeof(R) == 4, h->g.K1);
@@ -975,7 +1018,8 @@ int set_smem_limits_R() {
         BLD_SET_X2(768)
     }
 #undef BLD_SET_X2
-#define BLD_SET_SX2(P) BLD_SET((k_sgs_x<R, 1, 0, P>)); BLD_SET((k_sgs_x<R, 2, 0, P>));
+#define BLD_SET_SX2(P) BLD_SET((k_sgs_x<R, 1, 0, P>)); BLD_SET((k_sgs_x<R, 2, 0, P>));   \
+    if constexpr (P <= 288) BLD_SET((k_sgs_x2<R, y2_radix_a(P), y2_radix_b(P)>));
     BLD_SET_SX2(64)
     BLD_SET_SX2(96)
     BLD_SET_SX2(128)
@@ -987,6 +1031,9 @@ int set_smem_limits_R() {
         BLD_SET_SX2(384)
         BLD_SET_SX2(512)
         BLD_SET_SX2(768)
+        BLD_SET((k_sgs_x2<R, y2_radix_a(384), y2_radix_b(384)>));
+        BLD_SET((k_sgs_x2<R, y2_radix_a(512), y2_radix_b(512)>));
+        BLD_SET((k_sgs_x2<R, y2_radix_a(768), y2_radix_b(768)>));
 #define BLD_SET_SX2C(P) BLD_SET((k_sgs_x<R, 1, 0, P, 2>)); BLD_SET((k_sgs_x<R, 2, 0, P, 2>));
         BLD_SET_SX2C(256)
         BLD_SET_SX2C(288)
@@ -1445,6 +1492,7 @@ void copy_tuning(Space& dst, const Space& src) {
     dst.xr = src.xr;
     dst.x2 = src.x2;
     dst.sx2 = src.sx2;
+    dst.sxk = src.sxk;
     dst.inv = src.inv;
     dst.fwd = src.fwd;
 }
@@ -1499,6 +1547,7 @@ int autotune_impl(bld_handle* h) {
     const bool sx2_staged_only = sk && !strcmp(sk, "twopass_staged") && h->sgs.on && sx2_ok(h, h->sgs);
     const bool only_sx2 = sk && (!strcmp(sk, "twopass") || sx2_capped_only || sx2_staged_only) && h->sgs.on &&
                           sx2_ok(h, h->sgs);
+    const bool only_sxk = sk && !strcmp(sk, "rows") && h->sgs.on && sxk_ok(h, h->sgs);
     const bool adv_bw_ok = h->adv.on && xb_radix(h->adv.P1, h->fp32) > 0;
     if (only_bw && !adv_bw_ok && h->adv.on) return fail(BLD_ERR_INVALID_CONFIG, "no block-of-warps x kernel for P1=%d", h->adv.P1);
     const bool adv_warp_ok = h->adv.on && (h->fp32 ? warpx_radix<float>(h->adv.P1) : warpx_radix<double>(h->adv.P1)) > 0;
@@ -1607,9 +1656,9 @@ int autotune_impl(bld_handle* h) {
         // its best z-chunk count (and, for the warp-per-row kernel, register
         // cap: more resident warps want more chunks)
         struct XPick {
-            int YT, PPT, xr, xw, xwmb, xb, zmult, x2, sx2;
+            int YT, PPT, xr, xw, xwmb, xb, zmult, x2, sx2, sxk;
         };
-        auto get_pick = [&]() { return XPick{s.YT, s.PPT, s.xr, s.xw, s.xwmb, s.xb, s.zmult, s.x2, s.sx2}; };
+        auto get_pick = [&]() { return XPick{s.YT, s.PPT, s.xr, s.xw, s.xwmb, s.xb, s.zmult, s.x2, s.sx2, s.sxk}; };
         auto set_pick = [&](const XPick& p) {
             s.YT = p.YT;
             s.PPT = p.PPT;
@@ -1620,6 +1669,7 @@ int autotune_impl(bld_handle* h) {
             s.zmult = p.zmult;
             s.x2 = p.x2;
             s.sx2 = p.sx2;
+            s.sxk = p.sxk;
             x_chunks(h, s);
         };
         const char* mbe = getenv("BLD_XW_MINB");   // force one register cap (1, 3, 4)
@@ -1650,20 +1700,23 @@ int autotune_impl(bld_handle* h) {
             return BLD_OK;
         };
         const bool block_ok = best < 1e30f;   // a block kernel was timed above
-        if (block_ok && (sp == 1 || !only_x2)) BLD_TRY(tune_chunks(XPick{byt, bppt, bxr, 0, 1, 0, 2, 0, bsx2}));
+        if (block_ok && (sp == 1 || !only_x2) && !(sp == 1 && only_sxk))
+            BLD_TRY(tune_chunks(XPick{byt, bppt, bxr, 0, 1, 0, 2, 0, bsx2, 0}));
+        // the SGS kernel with staged rows and two-pass lines (BLD_SGS_X_KERNEL=rows keeps it)
+        if (sp == 1 && sxk_ok(h, s) && (!sk || only_sxk)) BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 0, 0, 1}));
         const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw && !only_lines && !only_x2;
-        for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) BLD_TRY(tune_chunks(XPick{1, 1, 0, wpb, 1, 0, 2, 0, 0}));
+        for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) BLD_TRY(tune_chunks(XPick{1, 1, 0, wpb, 1, 0, 2, 0, 0, 0}));
         for (int xbk = 1; xbk <= 2; ++xbk) {
             if (!(sp == 0 && adv_bw_ok && !only_block && !only_warp && !only_lines && !only_x2)) break;
             if ((xbk == 1 && only_pipe) || (xbk == 2 && only_bw3)) continue;
-            BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2, 0, 0}));
+            BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2, 0, 0, 0}));
         }
         // the two-pass kernel's variants (BLD_X2_VARIANT = 0, 1, 2 forces one)
         const char* x2v = getenv("BLD_X2_VARIANT");
         const int x2_only = x2v && x2v[0] ? atoi(x2v) : -1;
         for (int v = 0; v <= 2; ++v)
             if (sp == 0 && x2_ok(h, s, v) && (only_x2 || !xk || x2_asked) && (x2_only < 0 || x2_only == v))
-                BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1 + v, 0}));
+                BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1 + v, 0, 0}));
         if (bx >= 1e30f) return fail(BLD_ERR_INVALID_CONFIG, "no x kernel could be timed");
         set_pick(bp);
         x_chunks(h, s);
@@ -1680,9 +1733,9 @@ int autotune_impl(bld_handle* h) {
         s.fwd = bf;
         const char* v = getenv("BLD_VERBOSE");
         if (v && v[0] && v[0] != '0')
-            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d wfft=%d tp=%d | x YT=%d PPT=%d xr=%d warps=%d bw=%d x2=%d sx2=%d chunks=%d | fwd all=%d NL=%d thr=%d wfft=%d tp=%d\n",
+            fprintf(stderr, "bld autotune %s P=%dx%d: inv all=%d NL=%d thr=%d wfft=%d tp=%d | x YT=%d PPT=%d xr=%d warps=%d bw=%d x2=%d sx2=%d sxk=%d chunks=%d | fwd all=%d NL=%d thr=%d wfft=%d tp=%d\n",
                     sp == 0 ? "advection" : "sgs", s.P1, s.P2, s.inv.all, s.inv.NL, s.inv.thr, s.inv.wfft, s.inv.tp, s.YT, s.PPT, s.xr, s.xw, (int)s.xb,
-                    s.x2, s.sx2, s.nchunks, s.fwd.all, s.fwd.NL, s.fwd.thr, s.fwd.wfft, s.fwd.tp);
+                    s.x2, s.sx2, s.sxk, s.nchunks, s.fwd.all, s.fwd.NL, s.fwd.thr, s.fwd.wfft, s.fwd.tp);
     }
     if (h->cfg.pressure && h->g.n3 <= 256) {
         float best = 1e30f, t = 0;
@@ -2810,6 +2863,8 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
             snprintf(xname, sizeof xname, "k_adv_xwc<%s, %d, %d>", R, s.P1 / 32, s.xwmb);
         else if (sp == 0 && s.xw)
             snprintf(xname, sizeof xname, "k_adv_xw<%s, %d>", R, s.P1 / 32);
+        else if (sp == 1 && s.sxk)
+            snprintf(xname, sizeof xname, "k_sgs_x2<%s, %d, %d>", R, y2_radix_a(s.P1), y2_radix_b(s.P1));
         else if (sp == 1 && s.sx2)
             snprintf(xname, sizeof xname, "%s<%s, %d, 0, %d%s>", xk, R, s.PPT, s.P1, s.sx2 % 2 == 0 ? ", 2" : "");
         else

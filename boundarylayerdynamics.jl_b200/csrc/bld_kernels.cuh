@@ -667,6 +667,118 @@ __device__ __forceinline__ void twopass_inplace(cplx<R>* buf, int nlines, int LP
     __syncthreads();
 }
 
+// Values the Smagorinsky x pass carries from one layer to the next at one
+// (x, y) point: the previous C layer's velocities, strain and |S|^2 terms, and
+// the previous I layer's S13, S23, tau13, tau23, tau33.
+template <typename R>
+struct SgsCarry {
+    R u, v, w, w1, w2, s11, s22, s33, s12, sc, s13, s23, t13, t23, t33;
+};
+
+// The Smagorinsky model at one (x, y) point of the x pass when C layer j enters
+// (src/processes/static_smagorinsky.jl:129-249): strain on C layer j, S13, S23,
+// eddy viscosity and tau13, tau23 on I layer j - 1, |S| and the stresses of C
+// layer c = j - 1 with the wall model at the boundary layers, d3 tau_i3 by
+// stencil; o[0..7] are the packed outputs (tau11, tau12, tau22, d3 tau13,
+// d3 tau23, d3 tau33 on I layer c - 1, tau13, tau23 on I layer c), all negated as
+// the rates add them.  Updates the carried values.
+template <typename R>
+__device__ __forceinline__ void sgs_point(const XArgs& a, int j, int n3, bool hasC, const double* lcm,
+                                          const double* lim, R fs_lo, R fs_hi, R ft_lo, R ft_hi, R wlo, R u, R v,
+                                          R u1, R u2, R v1, R v2, R w, R w1, R w2, SgsCarry<R>& cy, R (&o)[8]) {
+    const int c = j - 1;
+    // (a) strain on C layer j (vel3_3 by dx3_i2c with Dirichlet w, :202-216)
+    R s11 = 0, s22 = 0, s33 = 0, s12 = 0, sc = 0;
+    if (hasC) {
+        const R ac = (R)a.alpha_c[j];
+        const R wb = (j == 0) ? wlo : cy.w;
+        s33 = -ac * wb + ac * w;
+        s11 = u1;
+        s22 = v2;
+        s12 = (u2 + v1) / R(2);
+        sc = s11 * s11 + s22 * s22 + s33 * s33 + R(2) * (s12 * s12);
+    }
+    // (b) I layer j-1: S13, S23, eddy viscosity, tau13, tau23
+    R s13 = 0, s23 = 0, sg13 = 0, sg23 = 0;
+    if (j >= 1 && j <= n3 - 1) {
+        const R ai = (R)a.alpha_i[j - 1];
+        s13 = ((-ai * cy.u + ai * u) + cy.w1) / R(2);
+        s23 = ((-ai * cy.v + ai * v) + cy.w2) / R(2);
+        R si = R(2) * (s13 * s13) + R(2) * (s23 * s23);
+        R t;
+        t = cy.s11 + s11; si += t * t / R(4);
+        t = cy.s22 + s22; si += t * t / R(4);
+        t = cy.s33 + s33; si += t * t / R(4);
+        t = cy.s12 + s12; si += R(2) * (t * t) / R(4);
+        const R l2 = (R)lim[j - 1];
+        const R evi = sqrt(R(2) * si) * l2;
+        sg13 = R(-2) * evi * s13;
+        sg23 = R(-2) * evi * s23;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) o[q] = 0;
+    R sg33 = 0;
+    if (j >= 1) {
+        // (c) C layer c = j-1
+        R scc = cy.sc;
+        // S13 (:232-233); dynamic values are not interpolated (:245-249)
+        if (c == 0) {
+            if (a.dyn_lo) { const R d = cy.u * fs_lo; scc += R(2) * (d * d); }
+            else { const R d = R(0) + s13; scc += R(2) * (d * d) / R(4); }
+        } else if (c == n3 - 1) {
+            if (a.dyn_hi) { const R d = cy.u * fs_hi; scc += R(2) * (d * d); }
+            else { const R d = cy.s13 + R(0); scc += R(2) * (d * d) / R(4); }
+        } else {
+            const R d = cy.s13 + s13; scc += R(2) * (d * d) / R(4);
+        }
+        if (c == 0) {
+            if (a.dyn_lo) { const R d = cy.v * fs_lo; scc += R(2) * (d * d); }
+            else { const R d = R(0) + s23; scc += R(2) * (d * d) / R(4); }
+        } else if (c == n3 - 1) {
+            if (a.dyn_hi) { const R d = cy.v * fs_hi; scc += R(2) * (d * d); }
+            else { const R d = cy.s23 + R(0); scc += R(2) * (d * d) / R(4); }
+        } else {
+            const R d = cy.s23 + s23; scc += R(2) * (d * d) / R(4);
+        }
+        const R evc = sqrt(R(2) * scc) * (R)lcm[c];
+        o[0] = -(R(-2) * evc * cy.s11);
+        o[2] = -(R(-2) * evc * cy.s22);
+        sg33 = R(-2) * evc * cy.s33;
+        o[1] = -(R(-2) * evc * cy.s12);
+        // wall stress (stress_bc, :195-200) from the wall-adjacent C layer
+        const R uh = sqrt(cy.u * cy.u + cy.v * cy.v);
+        const R b13lo = a.dyn_lo ? ft_lo * cy.u * uh : R(0);
+        const R b23lo = a.dyn_lo ? ft_lo * cy.v * uh : R(0);
+        const R b13hi = a.dyn_hi ? ft_hi * cy.u * uh : R(0);
+        const R b23hi = a.dyn_hi ? ft_hi * cy.v * uh : R(0);
+        const R below13 = (c == 0) ? b13lo : cy.t13;
+        const R below23 = (c == 0) ? b23lo : cy.t23;
+        const R above13 = (c == n3 - 1) ? b13hi : sg13;
+        const R above23 = (c == n3 - 1) ? b23hi : sg23;
+        const R ac = (R)a.alpha_c[c];
+        o[3] = -(-ac * below13 + ac * above13);
+        o[4] = -(-ac * below23 + ac * above23);
+        if (c >= 1) {  // d3 tau33 on I layer c-1 (dx3_c2i!, :363)
+            const R ai = (R)a.alpha_i[c - 1];
+            o[5] = -(-ai * cy.t33 + ai * sg33);
+        }
+        o[6] = -sg13;
+        o[7] = -sg23;
+    }
+    // (d) carry
+    if (j >= 1 && j <= n3 - 1) {
+        cy.s13 = s13;
+        cy.s23 = s23;
+        cy.t13 = sg13;
+        cy.t23 = sg23;
+    }
+    if (j >= 1) cy.t33 = sg33;
+    if (hasC) {
+        cy.s11 = s11; cy.s22 = s22; cy.s33 = s33; cy.s12 = s12; cy.sc = sc;
+        cy.u = u; cy.v = v; cy.w = w; cy.w1 = w1; cy.w2 = w2;
+    }
+}
+
 // byte offset of the staging area of the two-pass SGS x kernel: after the
 // twiddles and the two line buffers, rounded up to 128 bytes; the area holds
 // the two barriers (128 bytes) and 2 x 9 staged rows of YT K1 values
@@ -736,15 +848,9 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
     const R ft_lo = (R)a.wall[4 * m + 2], ft_hi = (R)a.wall[4 * m + 3];
     const R wlo = (R)a.w_lo, whi = (R)a.w_hi;
 
-    R pu[PPT], pv[PPT], pw[PPT], pw1[PPT], pw2[PPT];
-    R ps11[PPT], ps22[PPT], ps33[PPT], ps12[PPT], psc[PPT];
-    R s13pp[PPT], s23pp[PPT], t13pp[PPT], t23pp[PPT], t33pp[PPT];
+    SgsCarry<R> cy[PPT];
 #pragma unroll
-    for (int i = 0; i < PPT; ++i) {
-        pu[i] = pv[i] = pw[i] = pw1[i] = pw2[i] = R(0);
-        ps11[i] = ps22[i] = ps33[i] = ps12[i] = psc[i] = R(0);
-        s13pp[i] = s23pp[i] = t13pp[i] = t23pp[i] = t33pp[i] = R(0);
-    }
+    for (int i = 0; i < PPT; ++i) cy[i] = SgsCarry<R>{};
 
     const int jend = min(n3, z1 + 1);
     for (int j = jb; j <= jend; ++j) {
@@ -838,100 +944,12 @@ __global__ void __launch_bounds__(256, MINB) k_sgs_x(XArgs a) {
                     w = c3.x; w1 = c3.y; w2 = c4.x;
                 }
             }
-            // (a) strain on C layer j (vel3_3 by dx3_i2c with Dirichlet w, :202-216)
-            R s11 = 0, s22 = 0, s33 = 0, s12 = 0, sc = 0;
-            if (hasC) {
-                const R ac = (R)a.alpha_c[j];
-                const R wb = (j == 0) ? wlo : pw[i];
-                s33 = -ac * wb + ac * w;
-                s11 = u1;
-                s22 = v2;
-                s12 = (u2 + v1) / R(2);
-                sc = s11 * s11 + s22 * s22 + s33 * s33 + R(2) * (s12 * s12);
-            }
-            // (b) I layer j-1: S13, S23, eddy viscosity, tau13, tau23
-            R s13 = 0, s23 = 0, sg13 = 0, sg23 = 0;
-            if (j >= 1 && j <= n3 - 1) {
-                const R ai = (R)a.alpha_i[j - 1];
-                s13 = ((-ai * pu[i] + ai * u) + pw1[i]) / R(2);
-                s23 = ((-ai * pv[i] + ai * v) + pw2[i]) / R(2);
-                R si = R(2) * (s13 * s13) + R(2) * (s23 * s23);
-                R t;
-                t = ps11[i] + s11; si += t * t / R(4);
-                t = ps22[i] + s22; si += t * t / R(4);
-                t = ps33[i] + s33; si += t * t / R(4);
-                t = ps12[i] + s12; si += R(2) * (t * t) / R(4);
-                const R l2 = (R)lim[j - 1];
-                const R evi = sqrt(R(2) * si) * l2;
-                sg13 = R(-2) * evi * s13;
-                sg23 = R(-2) * evi * s23;
-            }
             R o[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) o[q] = 0;
-            R sg33 = 0;
-            if (j >= 1) {
-                // (c) C layer c = j-1
-                R scc = psc[i];
-                // S13 (:232-233); dynamic values are not interpolated (:245-249)
-                if (c == 0) {
-                    if (a.dyn_lo) { const R d = pu[i] * fs_lo; scc += R(2) * (d * d); }
-                    else { const R d = R(0) + s13; scc += R(2) * (d * d) / R(4); }
-                } else if (c == n3 - 1) {
-                    if (a.dyn_hi) { const R d = pu[i] * fs_hi; scc += R(2) * (d * d); }
-                    else { const R d = s13pp[i] + R(0); scc += R(2) * (d * d) / R(4); }
-                } else {
-                    const R d = s13pp[i] + s13; scc += R(2) * (d * d) / R(4);
-                }
-                if (c == 0) {
-                    if (a.dyn_lo) { const R d = pv[i] * fs_lo; scc += R(2) * (d * d); }
-                    else { const R d = R(0) + s23; scc += R(2) * (d * d) / R(4); }
-                } else if (c == n3 - 1) {
-                    if (a.dyn_hi) { const R d = pv[i] * fs_hi; scc += R(2) * (d * d); }
-                    else { const R d = s23pp[i] + R(0); scc += R(2) * (d * d) / R(4); }
-                } else {
-                    const R d = s23pp[i] + s23; scc += R(2) * (d * d) / R(4);
-                }
-                const R evc = sqrt(R(2) * scc) * (R)lcm[c];
-                o[0] = -(R(-2) * evc * ps11[i]);
-                o[2] = -(R(-2) * evc * ps22[i]);
-                sg33 = R(-2) * evc * ps33[i];
-                o[1] = -(R(-2) * evc * ps12[i]);
-                // wall stress (stress_bc, :195-200) from the wall-adjacent C layer
-                const R uh = sqrt(pu[i] * pu[i] + pv[i] * pv[i]);
-                const R b13lo = a.dyn_lo ? ft_lo * pu[i] * uh : R(0);
-                const R b23lo = a.dyn_lo ? ft_lo * pv[i] * uh : R(0);
-                const R b13hi = a.dyn_hi ? ft_hi * pu[i] * uh : R(0);
-                const R b23hi = a.dyn_hi ? ft_hi * pv[i] * uh : R(0);
-                const R below13 = (c == 0) ? b13lo : t13pp[i];
-                const R below23 = (c == 0) ? b23lo : t23pp[i];
-                const R above13 = (c == n3 - 1) ? b13hi : sg13;
-                const R above23 = (c == n3 - 1) ? b23hi : sg23;
-                const R ac = (R)a.alpha_c[c];
-                o[3] = -(-ac * below13 + ac * above13);
-                o[4] = -(-ac * below23 + ac * above23);
-                if (c >= 1) {  // d3 tau33 on I layer c-1 (dx3_c2i!, :363)
-                    const R ai = (R)a.alpha_i[c - 1];
-                    o[5] = -(-ai * t33pp[i] + ai * sg33);
-                }
-                o[6] = -sg13;
-                o[7] = -sg23;
-            }
+            sgs_point<R>(a, j, n3, hasC, lcm, lim, fs_lo, fs_hi, ft_lo, ft_hi, wlo, u, v, u1, u2, v1, v2, w, w1, w2,
+                         cy[i], o);
             if (doC || do5) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) outb[(yl * 4 + q) * LP + xs] = mk<R>(o[2 * q], o[2 * q + 1]);
-            }
-            // (d) carry
-            if (j >= 1 && j <= n3 - 1) {
-                s13pp[i] = s13;
-                s23pp[i] = s23;
-                t13pp[i] = sg13;
-                t23pp[i] = sg23;
-            }
-            if (j >= 1) t33pp[i] = sg33;
-            if (hasC) {
-                ps11[i] = s11; ps22[i] = s22; ps33[i] = s33; ps12[i] = s12; psc[i] = sc;
-                pu[i] = u; pv[i] = v; pw[i] = w; pw1[i] = w1; pw2[i] = w2;
             }
         }
         if (doC || do5) {

@@ -521,3 +521,55 @@ def test_sgs_twopass_staged(oracle, BLD, res, precision, tol, sgs_sizes):
     for f in om.fields:
         e = rel_l2(got[f], ref[f])
         assert e < tol, (res, precision, f, e)
+
+
+@pytest.mark.parametrize("res,precision,tol", [((64, 12, 6), "fp64", 1e-12), ((64, 12, 6), "mixed", 1e-5),
+                                               ((96, 8, 5), "mixed", 1e-5), ((128, 8, 5), "mixed", 1e-5),
+                                               ((128, 8, 5), "fp64", 1e-12), ((256, 6, 4), "fp64", 1e-12),
+                                               ((512, 4, 4), "mixed", 1e-5)])
+def test_sgs_rows_kernel(oracle, BLD, res, precision, tol):
+    """k_sgs_x2 (rows staged by 1-d TMA bulk copies, two-pass line transforms, one
+    thread per pass-1 task) forced with BLD_SGS_X_KERNEL=rows, against the oracle."""
+    om = _build(oracle, res, les=True)
+    old = os.environ.get("BLD_SGS_X_KERNEL")
+    os.environ["BLD_SGS_X_KERNEL"] = "rows"
+    try:
+        gm = _build(BLD, res, precision, les=True)
+    finally:
+        if old is None:
+            del os.environ["BLD_SGS_X_KERNEL"]
+        else:
+            os.environ["BLD_SGS_X_KERNEL"] = old
+    assert gm.kernels()["sgs"]["x"].startswith("k_sgs_x2<"), gm.kernels()
+    st = _state(om, seed=sum(res) + 13)
+    ref = om.compute_rates(st)
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < tol, (res, precision, f, e)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
+def test_sgs_rows_kernel_trajectory(oracle, BLD, precision, tol):
+    """20 SSP-RK33 steps of a 64 x 64 x 8 LES with k_sgs_x2 forced (z chunks,
+    the carried values and the wall model across layers), against the oracle."""
+    res = (64, 64, 8)
+    om = _build(oracle, res, les=True)
+    old = os.environ.get("BLD_SGS_X_KERNEL")
+    os.environ["BLD_SGS_X_KERNEL"] = "rows"
+    try:
+        gm = _build(BLD, res, precision, les=True)
+    finally:
+        if old is None:
+            del os.environ["BLD_SGS_X_KERNEL"]
+        else:
+            os.environ["BLD_SGS_X_KERNEL"] = old
+    assert gm.kernels()["sgs"]["x"].startswith("k_sgs_x2<"), gm.kernels()
+    st = _state(om, seed=21)
+    gm.set_state(st)
+    om.state.update({f: v.copy() for f, v in st.items()})
+    gm.evolve(20 * 1e-4, 1e-4)
+    om.evolve(20 * 1e-4, 1e-4)
+    for f in om.fields:
+        e = rel_l2(gm.state[f], om.state[f])
+        assert e < tol, (precision, f, e)
