@@ -2640,40 +2640,62 @@ int32_t bld_ensemble_step(bld_handle* const* hs, int32_t n, int64_t nsteps, doub
     }
     if (nsteps <= 0) return BLD_OK;
     CUDA_TRY(cudaSetDevice(lead->device));
-    std::vector<const void*> key;
-    for (int i = 0; i < n; ++i) {
-        key.push_back(hs[i]);
-        key.push_back((const void*)(intptr_t)gkey(hs[i], method));
-    }
-    double dtk = dt;
-    const void* dtp;
-    memcpy(&dtp, &dtk, sizeof(dtp) < sizeof(dtk) ? sizeof(dtp) : sizeof(dtk));
-    key.push_back(dtp);
-    auto it = lead->ens_graphs.find(key);
-    if (it == lead->ens_graphs.end()) {
-        cudaGraph_t parent;
-        CUDA_TRY(cudaGraphCreate(&parent, 0));
+    // chained steps as in bld_step (every class must allow it): the first leaves
+    // the next step's first stage value, the middle ones enter and leave, the
+    // last enters and ends with f(u)
+    bool chain = nsteps >= 2;
+    for (int i = 0; i < n; ++i) chain = chain && chain_ok(hs[i], method);
+    // the parent graph of one step variant `c`: the classes' step graphs as
+    // independent children
+    auto parent_for = [&](int c, cudaGraphExec_t* out) -> int {
+        std::vector<const void*> key;
         for (int i = 0; i < n; ++i) {
-            int st = step_graph(hs[i], method, dt);
-            if (st != BLD_OK) {
-                cudaGraphDestroy(parent);
-                return st;
-            }
-            cudaGraphNode_t node;
-            cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0,
-                                                       hs[i]->graph_src.at(std::make_pair(gkey(hs[i], method), dt)));
-            if (e != cudaSuccess) {
-                cudaGraphDestroy(parent);
-                CUDA_TRY(e);
-            }
+            key.push_back(hs[i]);
+            key.push_back((const void*)(intptr_t)(gkey(hs[i], method) + 32 * c));
         }
-        cudaGraphExec_t exec;
-        cudaError_t ie = cudaGraphInstantiate(&exec, parent, 0);
-        cudaGraphDestroy(parent);
-        CUDA_TRY(ie);
-        it = lead->ens_graphs.emplace(key, exec).first;
+        double dtk = dt;
+        const void* dtp;
+        memcpy(&dtp, &dtk, sizeof(dtp) < sizeof(dtk) ? sizeof(dtp) : sizeof(dtk));
+        key.push_back(dtp);
+        auto it = lead->ens_graphs.find(key);
+        if (it == lead->ens_graphs.end()) {
+            cudaGraph_t parent;
+            CUDA_TRY(cudaGraphCreate(&parent, 0));
+            for (int i = 0; i < n; ++i) {
+                int st = step_graph(hs[i], method, dt, c);
+                if (st != BLD_OK) {
+                    cudaGraphDestroy(parent);
+                    return st;
+                }
+                cudaGraphNode_t node;
+                cudaError_t e = cudaGraphAddChildGraphNode(
+                    &node, parent, nullptr, 0, hs[i]->graph_src.at(std::make_pair(gkey(hs[i], method) + 32 * c, dt)));
+                if (e != cudaSuccess) {
+                    cudaGraphDestroy(parent);
+                    CUDA_TRY(e);
+                }
+            }
+            cudaGraphExec_t exec;
+            cudaError_t ie = cudaGraphInstantiate(&exec, parent, 0);
+            cudaGraphDestroy(parent);
+            CUDA_TRY(ie);
+            it = lead->ens_graphs.emplace(key, exec).first;
+        }
+        *out = it->second;
+        return BLD_OK;
+    };
+    if (!chain) {
+        cudaGraphExec_t g;
+        BLD_TRY(parent_for(0, &g));
+        for (int64_t s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(g, lead->stream));
+    } else {
+        cudaGraphExec_t gfirst, gmid, glast;
+        BLD_TRY(parent_for(CHAIN_LEAVE, &gfirst));
+        BLD_TRY(parent_for(CHAIN_ENTER | CHAIN_LEAVE, &gmid));
+        BLD_TRY(parent_for(CHAIN_ENTER, &glast));
+        for (int64_t s = 0; s < nsteps; ++s)
+            CUDA_TRY(cudaGraphLaunch(s == 0 ? gfirst : (s == nsteps - 1 ? glast : gmid), lead->stream));
     }
-    for (int64_t s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(it->second, lead->stream));
     CUDA_TRY(cudaStreamSynchronize(lead->stream));
     int status = BLD_OK;
     for (int i = 0; i < n; ++i) {
