@@ -33,8 +33,9 @@ METRIC = "grid-pt updates/s (plain FP64 vs mixed) @192^2x96"
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the x-pass
 # kernel the autotuner picks at 192^2x96, from one ncu capture of a step
 # (profiles/step_kernels_dns192_fp64.md, profiles/step_kernels_dns192_mixed.md)
-TRAFFIC = {("dns192", "k_adv_x2<double, 16, 18>"): (254.1 + 95.65) * 1e6,
-           ("dns192", "k_adv_x2<float, 16, 18>"): (127.4 + 36.42) * 1e6}
+TRAFFIC = {("dns192", "k_adv_x2<double, 16, 18, wide>"): (254.4 + 95.5) * 1e6,
+           ("dns192", "k_adv_x2<double, 16, 18>"): (254.1 + 95.65) * 1e6,
+           ("dns192", "k_adv_x2<float, 16, 18>"): (128.6 + 34.7) * 1e6}
 TRAFFIC_SOURCE = "ncu capture of one step in profiles/ (a fixed figure, not measured in this run)"
 UNIT = "grid-pt updates/s"
 # the workload both arms report under "config" (identical dicts); how the engine
