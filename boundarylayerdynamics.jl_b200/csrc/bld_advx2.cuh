@@ -19,15 +19,15 @@
 // Pass-1 outputs sit at q (B + 1) + j in their line, so that both passes read
 // and write consecutive addresses across a warp.
 //
-// Variants (V): 0 as above; 1 (lean) trades barriers for shared memory (65 KB
-// instead of 113 KB per block in double precision, for three blocks per SM):
-// one staging buffer, refilled with layer j + 1 as soon as pass 1 of layer j has
-// read it (the copy still overlaps the rest of the layer), and the second passes
-// in place in the pass-1 buffer (every task reads its line segment into
-// registers, a barrier, then the outputs go back), so the physical / spectral
-// lines need no buffer of their own; 2 (wide) runs V = 0 with 1.5x the threads
-// (fewer product points, hence fewer registers, per thread: two blocks of six
-// warps per SM in double precision instead of two of four).
+// The layers are software-pipelined by one phase: the unpack of layer j - 1
+// (which reads the spectra) and pass 1 of layer j (which writes the pass-1
+// buffer) touch different buffers, so they share one barrier interval, five
+// barriers per layer in all, and the unpack's many small tasks fill the threads
+// that pass 1 leaves idle.
+//
+// Variants (V): 0 as above; 2 (wide) runs it with 1.5x the threads (fewer
+// product points, hence fewer registers, per thread: two blocks of six warps
+// per SM in double precision instead of two of four).
 #pragma once
 
 #include "bld_tma.cuh"
@@ -48,26 +48,14 @@ __host__ __device__ constexpr int x2_smem(int A, int B, int K1, int csz) {
            x2_al(3 * x2_rows(csz, A * B) * A * B * csz) +
            x2_al((x2_rows(csz, A * B) + x2_rows(csz, A * B) / 2) * A * B * csz);
 }
-
-// the lean form: barriers, twiddles, 1 stage x 6 terms x NR rows, the pass-1
-// buffer (which also holds the physical / spectral lines), forward inputs
-__host__ __device__ constexpr int x2_smem_lean(int A, int B, int K1, int csz) {
-    return 128 + x2_al(A * B * csz) + x2_al(6 * x2_rows(csz, A * B) * K1 * csz) +
-           x2_al(3 * x2_rows(csz, A * B) * (A * (B + 1) + 128 / csz) * csz) +
-           x2_al((x2_rows(csz, A * B) + x2_rows(csz, A * B) / 2) * A * B * csz);
-}
 // blocks per SM a variant is compiled for (its register cap; 0: the compiler's choice)
-__host__ __device__ constexpr int x2_minb(int csz, int V) { return V == 1 ? (csz == 16 ? 3 : 2) : (V == 2 ? 2 : 0); }
-__host__ __device__ constexpr int x2_smem_v(int A, int B, int K1, int csz, int V) {
-    return V == 1 ? x2_smem_lean(A, B, K1, csz) : x2_smem(A, B, K1, csz);
-}
+__host__ __device__ constexpr int x2_minb(int csz, int V) { return V == 2 ? 2 : 0; }
 
 // grid (P2 / NR, nchunks, members), block x2_threads(B, NR, V); NR = x2_rows(sizeof(C), P)
 template <typename R, int A, int B, int V = 0>
 __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B), V), x2_minb(sizeof(cplx<R>), V))
     k_adv_x2(XArgs a, int* flag) {
     using C = cplx<R>;
-    constexpr bool LEAN = (V == 1);
     constexpr int P = A * B, NR = x2_rows(sizeof(C), P), NLI = 3 * NR, NLF = NR + NR / 2;
     constexpr int T = x2_threads(B, NR, V);
     constexpr int PPT = (NR * P + T - 1) / T;   // product points per thread
@@ -76,11 +64,7 @@ __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B),
     // line stride of the pass-1 buffer: line L + 1 starts where line L's task
     // B would, modulo a bank row, so warps spanning two lines stay conflict-free
     constexpr int X1L = A * X1S + ((B - A * X1S) % E + E) % E;
-    constexpr int NST = LEAN ? 1 : 2;           // staging buffers
-    constexpr int PHL = LEAN ? X1L : P;         // line stride of the physical / spectral lines
     static_assert(NR % 2 == 0, "adv3 lines pair two rows");
-    // the in-place second passes hold one task per thread across a barrier
-    static_assert(!LEAN || NLI * A <= T, "one pass-2 task per thread");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int n3 = a.g.n3, k1max = a.g.k1max, K1 = a.g.K1;
     const int m = a.m0 + blockIdx.z;
@@ -94,14 +78,11 @@ __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B),
     C* tw = reinterpret_cast<C*>(p);
     p += x2_al(P * csz);
     C* stage = reinterpret_cast<C*>(p);
-    p += x2_al(NST * 6 * NR * K1 * csz);
+    p += x2_al(2 * 6 * NR * K1 * csz);
     C* X1 = reinterpret_cast<C*>(p);
     p += x2_al(NLI * X1L * csz);
-    C* Ph = X1;                         // physical lines; later the forward spectra
-    if constexpr (!LEAN) {
-        Ph = reinterpret_cast<C*>(p);
-        p += x2_al(NLI * P * csz);
-    }
+    C* Ph = reinterpret_cast<C*>(p);    // physical lines; later the forward spectra
+    p += x2_al(NLI * P * csz);
     C* Fw = reinterpret_cast<C*>(p);    // forward inputs: NR (adv1, adv2) lines, NR / 2 adv3 pairs
     const C* Min = reinterpret_cast<const C*>(a.min) + (long long)m * a.min_mstride;
     C* Mout = reinterpret_cast<C*>(a.mout) + (long long)m * a.mout_mstride;
@@ -133,16 +114,37 @@ __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B),
 #pragma unroll
     for (int i = 0; i < PPT; ++i) pu[i] = pv[i] = pw[i] = po1[i] = po2[i] = R(0);
 
-    for (int j = jb; j < z1; ++j) {
-        const int s = LEAN ? 0 : (j - jb) & 1;
-        const unsigned parity = LEAN ? (unsigned)((j - jb) & 1) : (unsigned)(((j - jb) >> 1) & 1);
-        const bool hasI = (j < n3 - 1);
-        // stage s ^ 1 was last read by layer j - 1's pass 1, several barriers ago
-        if (!LEAN && threadIdx.x == 0 && j + 1 < z1) {
+    int plf0 = 0, plf1 = 0;   // forward lines of the previous layer
+    // layer j sits in stage slot (j - jb) & 1 and completes that slot's phase
+    // ((j - jb) >> 1) & 1; the last pass (j = z1) only unpacks layer z1 - 1
+    for (int j = jb; j <= z1; ++j) {
+        const int s = (j - jb) & 1;
+        // stage slot s ^ 1 was last read by layer j - 1's pass 1, several barriers ago
+        if (threadIdx.x == 0 && j + 1 < z1) {
             fence_async_shared();
             issue(j + 1, s ^ 1);
         }
-        const bool arrived = mbar_wait_bounded(&bar[s], parity, wait_limit);
+        // the unpack of layer j - 1 and the pass 1 of layer j share one barrier
+        // interval: they touch different buffers (Ph, X1)
+        if (j > jb) {
+            for (int task = threadIdx.x; task < (plf1 - plf0) * K1; task += T) {
+                const int Lr = fdiv(task, a.k1_magic), L = plf0 + Lr, f = task - Lr * K1;
+                const C Zk = Ph[L * P + f], Zr = Ph[L * P + (P - f) % P];
+                const C va = mk<R>((Zk.x + Zr.x) * R(0.5), (Zk.y - Zr.y) * R(0.5));
+                const C vb = mk<R>((Zk.y + Zr.y) * R(0.5), -(Zk.x - Zr.x) * R(0.5));
+                if (L < NR) {
+                    mrow_w(Mout, a, 0, j - 1, y0 + L)[f] = va;
+                    mrow_w(Mout, a, 1, j - 1, y0 + L)[f] = vb;
+                } else {
+                    const int r = 2 * (L - NR);
+                    mrow_w(Mout, a, 2, j - 2, y0 + r)[f] = va;
+                    mrow_w(Mout, a, 2, j - 2, y0 + r + 1)[f] = vb;
+                }
+            }
+        }
+        if (j == z1) break;
+        const bool hasI = (j < n3 - 1);
+        const bool arrived = mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1, wait_limit);
         const C* cur = stage + (size_t)s * 6 * NR * K1;
         // ---- inverse pass 1: lines L = 3 r + p (pairs (u, v), (vort3, w), (vort1, vort2))
         for (int task = threadIdx.x; task < NLI * B; task += T) {
@@ -178,46 +180,23 @@ __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B),
         if (__syncthreads_or(!arrived)) {
             if (threadIdx.x == 0) {
                 atomicOr(flag + m, BLD_FLAG_TIMEOUT);
-                mbar_wait_bounded(&bar[s], parity);
-                if (!LEAN && j + 1 < z1) mbar_wait_bounded(&bar[s ^ 1], ((j + 1 - jb) >> 1) & 1);
+                mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1);
+                if (j + 1 < z1) mbar_wait_bounded(&bar[s ^ 1], ((j + 1 - jb) >> 1) & 1);
             }
             return;
         }
-        // the single staging buffer has been read: refill it with layer j + 1
-        if (LEAN && threadIdx.x == 0 && j + 1 < z1) {
-            fence_async_shared();
-            issue(j + 1, 0);
-        }
         // ---- inverse pass 2 -> physical lines Ph[L][x]
-        if constexpr (LEAN) {
-            const int L = threadIdx.x / A, j2 = threadIdx.x - L * A;
-            const bool act = threadIdx.x < NLI * A && !(L % 3 == 2 && !hasI);
+        for (int task = threadIdx.x; task < NLI * A; task += T) {
+            const int L = task / A, j2 = task - L * A;
+            if (L % 3 == 2 && !hasI) continue;
             C x[B];
-            if (act) {
 #pragma unroll
-                for (int t = 0; t < B; ++t) x[t] = X1[L * X1L + j2 * X1S + t];
+            for (int t = 0; t < B; ++t) x[t] = X1[L * X1L + j2 * X1S + t];
 #pragma unroll
-                for (int t = 1; t < B; ++t) x[t] = c_tw<+1>(x[t], tw[t * A + j2]);
-                dft<R, B, +1>(x);
-            }
-            __syncthreads();
-            if (act) {
+            for (int t = 1; t < B; ++t) x[t] = c_tw<+1>(x[t], tw[t * A + j2]);
+            dft<R, B, +1>(x);
 #pragma unroll
-                for (int q = 0; q < B; ++q) Ph[L * PHL + j2 + A * q] = x[q];
-            }
-        } else {
-            for (int task = threadIdx.x; task < NLI * A; task += T) {
-                const int L = task / A, j2 = task - L * A;
-                if (L % 3 == 2 && !hasI) continue;
-                C x[B];
-#pragma unroll
-                for (int t = 0; t < B; ++t) x[t] = X1[L * X1L + j2 * X1S + t];
-#pragma unroll
-                for (int t = 1; t < B; ++t) x[t] = c_tw<+1>(x[t], tw[t * A + j2]);
-                dft<R, B, +1>(x);
-#pragma unroll
-                for (int q = 0; q < B; ++q) Ph[L * PHL + j2 + A * q] = x[q];
-            }
+            for (int q = 0; q < B; ++q) Ph[L * P + j2 + A * q] = x[q];
         }
         __syncthreads();
         // ---- products at (x, row); outputs into Fw
@@ -228,8 +207,8 @@ __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B),
             const int idx = threadIdx.x + T * i;
             if (idx < NR * P) {
                 const int r = idx / P, x = idx - r * P;
-                const C c0 = Ph[(3 * r) * PHL + x], c1 = Ph[(3 * r + 1) * PHL + x];
-                const C c2 = hasI ? Ph[(3 * r + 2) * PHL + x] : mk<R>(R(0), R(0));
+                const C c0 = Ph[(3 * r) * P + x], c1 = Ph[(3 * r + 1) * P + x];
+                const C c2 = hasI ? Ph[(3 * r + 2) * P + x] : mk<R>(R(0), R(0));
                 const R u = c0.x, v = c0.y, o3 = c1.x;
                 const R w = hasI ? c1.y : R(0);
                 const R q1 = c2.x, q2 = c2.y;
@@ -270,52 +249,19 @@ __global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B),
         }
         __syncthreads();
         // ---- forward pass 2 -> spectra in Ph
-        if constexpr (LEAN) {
-            const int task = threadIdx.x;
+        for (int task = threadIdx.x; task < (lf1 - lf0) * A; task += T) {
             const int L = lf0 + task / A, j2 = task % A;
-            const bool act = task < (lf1 - lf0) * A;
             C x[B];
-            if (act) {
 #pragma unroll
-                for (int t = 0; t < B; ++t) x[t] = X1[L * X1L + j2 * X1S + t];
+            for (int t = 0; t < B; ++t) x[t] = X1[L * X1L + j2 * X1S + t];
 #pragma unroll
-                for (int t = 1; t < B; ++t) x[t] = c_tw<-1>(x[t], tw[t * A + j2]);
-                dft<R, B, -1>(x);
-            }
-            __syncthreads();
-            if (act) {
+            for (int t = 1; t < B; ++t) x[t] = c_tw<-1>(x[t], tw[t * A + j2]);
+            dft<R, B, -1>(x);
 #pragma unroll
-                for (int q = 0; q < B; ++q) Ph[L * PHL + j2 + A * q] = x[q];
-            }
-        } else {
-            for (int task = threadIdx.x; task < (lf1 - lf0) * A; task += T) {
-                const int L = lf0 + task / A, j2 = task % A;
-                C x[B];
-#pragma unroll
-                for (int t = 0; t < B; ++t) x[t] = X1[L * X1L + j2 * X1S + t];
-#pragma unroll
-                for (int t = 1; t < B; ++t) x[t] = c_tw<-1>(x[t], tw[t * A + j2]);
-                dft<R, B, -1>(x);
-#pragma unroll
-                for (int q = 0; q < B; ++q) Ph[L * PHL + j2 + A * q] = x[q];
-            }
+            for (int q = 0; q < B; ++q) Ph[L * P + j2 + A * q] = x[q];
         }
         __syncthreads();
-        // ---- unpack the two real lines of each spectrum and write the modes
-        for (int task = threadIdx.x; task < (lf1 - lf0) * K1; task += T) {
-            const int Lr = fdiv(task, a.k1_magic), L = lf0 + Lr, f = task - Lr * K1;
-            const C Zk = Ph[L * PHL + f], Zr = Ph[L * PHL + (P - f) % P];
-            const C va = mk<R>((Zk.x + Zr.x) * R(0.5), (Zk.y - Zr.y) * R(0.5));
-            const C vb = mk<R>((Zk.y + Zr.y) * R(0.5), -(Zk.x - Zr.x) * R(0.5));
-            if (L < NR) {
-                mrow_w(Mout, a, 0, j, y0 + L)[f] = va;
-                mrow_w(Mout, a, 1, j, y0 + L)[f] = vb;
-            } else {
-                const int r = 2 * (L - NR);
-                mrow_w(Mout, a, 2, j - 1, y0 + r)[f] = va;
-                mrow_w(Mout, a, 2, j - 1, y0 + r + 1)[f] = vb;
-            }
-        }
-        __syncthreads();
+        plf0 = lf0;
+        plf1 = lf1;
     }
 }

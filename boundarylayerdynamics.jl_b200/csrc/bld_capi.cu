@@ -623,10 +623,10 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
 
 // two-pass advection x kernel: compiled for P1 with a two-pass factorisation
 // (single precision up to 768, double up to 288), whole row pairs per block;
-// variants V = 1 (lean) and 2 (wide) in double precision only
+// variant V = 2 (wide) in double precision only
 bool x2_ok(const bld_handle* h, const Space& s, int V = 0) {
-    return y2_ok(s.P1, h->fp32) && s.P2 % x2_rows((int)csize(h->fp32), s.P1) == 0 && (V == 0 || !h->fp32) &&
-           x2_smem_v(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, (int)csize(h->fp32), V) <= 227 * 1024;
+    return y2_ok(s.P1, h->fp32) && s.P2 % x2_rows((int)csize(h->fp32), s.P1) == 0 && (V == 0 || (V == 2 && !h->fp32)) &&
+           x2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, (int)csize(h->fp32)) <= 227 * 1024;
 }
 
 template <typename R, int P, int V>
@@ -634,14 +634,13 @@ void launch_x2_pv(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
     constexpr int NR = x2_rows((int)sizeof(cplx<R>), P);
     dim3 grid(s.P2 / NR, s.nchunks, nm);
-    const size_t sm = x2_smem_v(A, B, h->g.K1, (int)sizeof(cplx<R>), V);
+    const size_t sm = x2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>));
     k_adv_x2<R, A, B, V><<<grid, x2_threads(B, NR, V), sm, h->stream>>>(a, h->flag);
 }
 
 template <typename R, int P>
 int launch_x2_p(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     if constexpr (sizeof(R) == 8) {
-        if (s.x2 == 2) return launch_x2_pv<R, P, 1>(h, s, a, nm), BLD_OK;
         if (s.x2 == 3) return launch_x2_pv<R, P, 2>(h, s, a, nm), BLD_OK;
     }
     launch_x2_pv<R, P, 0>(h, s, a, nm);
@@ -1002,7 +1001,6 @@ int set_smem_limits_R() {
 #define BLD_SET_X2(P)                                                   \
     BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P), 0>));            \
     if constexpr (sizeof(R) == 8) {                                     \
-        BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P), 1>));        \
         BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P), 2>));        \
     }
     BLD_SET_X2(64)
@@ -1711,7 +1709,7 @@ int autotune_impl(bld_handle* h) {
             if ((xbk == 1 && only_pipe) || (xbk == 2 && only_bw3)) continue;
             BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2, 0, 0, 0}));
         }
-        // the two-pass kernel's variants (BLD_X2_VARIANT = 0, 1, 2 forces one)
+        // the two-pass kernel's variants (BLD_X2_VARIANT = 0, 2 forces one)
         const char* x2v = getenv("BLD_X2_VARIANT");
         const int x2_only = x2v && x2v[0] ? atoi(x2v) : -1;
         for (int v = 0; v <= 2; ++v)
@@ -2878,7 +2876,7 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         char xname[96];
         if (sp == 0 && s.x2)
             snprintf(xname, sizeof xname, "k_adv_x2<%s, %d, %d%s>", R, y2_radix_a(s.P1), y2_radix_b(s.P1),
-                     s.x2 == 2 ? ", lean" : (s.x2 == 3 ? ", wide" : ""));
+                     s.x2 == 3 ? ", wide" : "");
         else if (sp == 0 && s.xb)
             snprintf(xname, sizeof xname, "%s<%s, %d>", s.xb == 2 ? "k_adv_xp" : "k_adv_xb", R, s.P1 / 32);
         else if (sp == 0 && s.xw && s.xwmb > 1)
