@@ -461,7 +461,7 @@ int state_tmap(const bld_handle* h, const void* base, int nl, CUtensorMap* out) 
 // of modes per layer (gamma rows are 16-byte multiples for the TMA map) and
 // LN columns x all layers within a block's shared memory
 bool project_tile_ok(const bld_handle* h, int ln) {
-    return h->cfg.pressure && h->g.n3 <= 256 && h->g.F % 2 == 0 && (ln == 8 || ln == 16) &&
+    return h->cfg.pressure && h->g.n3 <= 256 && h->g.F % 2 == 0 && (ln == 4 || ln == 8 || ln == 16) &&
            project_tile_smem(h->g.n3, ln) <= 200 * 1024 && encode_tiled() != nullptr;
 }
 
@@ -1135,6 +1135,8 @@ int set_smem_limits() {
     CUDA_TRY(cudaFuncSetAttribute(k_project_tile<8, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CUDA_TRY(cudaFuncSetAttribute(k_project_tile<16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CUDA_TRY(cudaFuncSetAttribute(k_project_tile<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_tile<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_tile<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CUDA_TRY(cudaFuncSetAttribute(k_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     done = 1;
     return BLD_OK;
@@ -1766,12 +1768,12 @@ int autotune_impl(bld_handle* h) {
         h->proj_variant = bv;
         // projections of stored stage values (the step's in-place projections):
         // the chosen kernel against k_project_tile with 8 or 16 columns per block
-        // (BLD_PROJ_TILE = 0, 8, 16 keeps one)
+        // (BLD_PROJ_TILE = 0, 4, 8, 16 keeps one)
         const char* pt = getenv("BLD_PROJ_TILE");
         const int only_t = (pt && pt[0]) ? atoi(pt) : -1;
         float bt = 1e30f;
         int btile = 0;
-        for (int ln : {0, 8, 16}) {
+        for (int ln : {0, 4, 8, 16}) {
             if (ln && !project_tile_ok(h, ln)) continue;
             if (only_t >= 0 && ln != only_t) continue;
             h->proj_tile = ln;
@@ -1875,8 +1877,10 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
         dim3 grid((unsigned)((h->g.F + ln - 1) / ln), nm);
         dim3 block(ln, std::max(1, std::min(16, (n3 + lmax - 1) / lmax)));
         const size_t sm = project_tile_smem(n3, ln);
-        if (lmax == 8 && ln == 8) k_project_tile<8, 8><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
+        if (lmax == 8 && ln == 4) k_project_tile<8, 4><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
+        else if (lmax == 8 && ln == 8) k_project_tile<8, 8><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
         else if (lmax == 8) k_project_tile<8, 16><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
+        else if (ln == 4) k_project_tile<16, 4><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
         else if (ln == 8) k_project_tile<16, 8><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
         else k_project_tile<16, 16><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
         CUDA_TRY(cudaGetLastError());

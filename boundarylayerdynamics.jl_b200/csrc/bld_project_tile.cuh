@@ -11,14 +11,19 @@
 // shared memory; the block writes u + grad p once.
 //
 // block (LN, NS) with NS segments of <= LMAX layers; grid (ceil(F / LN), members);
-// dynamic shared memory project_tile_smem(n3, LN).
+// dynamic shared memory project_tile_smem(n3, LN).  A tensor copy's shared-memory
+// destination starts on a 128-byte boundary: the component tiles are padded to
+// project_tile_stride values.
 #pragma once
 
 #include "bld_tma.cuh"
 
+// values per component tile: n3 LN rounded up to 8 (128 bytes), so that every
+// TMA destination starts on a 128-byte boundary whatever n3 and LN are
+__host__ __device__ constexpr int project_tile_stride(int n3, int LN) { return (n3 * LN + 7) / 8 * 8; }
 // bytes: alignment slack, the barrier, the three components, gamma
 __host__ __device__ constexpr int project_tile_smem(int n3, int LN) {
-    return 128 + 128 + 3 * n3 * LN * 16 + n3 * LN * 8;
+    return 128 + 128 + 3 * project_tile_stride(n3, LN) * 16 + n3 * LN * 8;
 }
 
 template <int LMAX, int LN>
@@ -33,8 +38,9 @@ __global__ void __launch_bounds__(LN * 32) k_project_tile(ProjArgs a, const __gr
     const Geo& g = a.g;
     const int n = g.n3;
     const long long F = g.F;
-    double2* tile = reinterpret_cast<double2*>(base + 128);   // [3][n][LN]
-    const double* gt = reinterpret_cast<const double*>(tile + 3 * n * LN);   // [n][LN]
+    const int FS = project_tile_stride(n, LN);
+    double2* tile = reinterpret_cast<double2*>(base + 128);   // [3][FS >= n LN]
+    const double* gt = reinterpret_cast<const double*>(tile + 3 * FS);   // [n][LN]
     const int NS = blockDim.y, s = threadIdx.y, lane = threadIdx.x;
     const int tid = s * LN + lane;
     const int c0 = blockIdx.x * LN, c = c0 + lane;
@@ -51,7 +57,7 @@ __global__ void __launch_bounds__(LN * 32) k_project_tile(ProjArgs a, const __gr
         mbar_arrive_expect_tx(bar, (unsigned)(3 * n * LN * 16 + n * LN * 8));
         // components at rows 0, n3, 2 n3 of the member's (3 n3 - 1)-row state; the
         // last row of the third box lies past the state and is filled with zeros
-        for (int f = 0; f < 3; ++f) tma_load_3d(tile + (size_t)f * n * LN, &umap, 2 * c0, f * n, m, bar);
+        for (int f = 0; f < 3; ++f) tma_load_3d(tile + (size_t)f * FS, &umap, 2 * c0, f * n, m, bar);
         tma_load_2d(const_cast<double*>(gt), &gmap, c0, 0, bar);
     }
     const long long wait_limit = g_bld_wait_limit;
@@ -73,7 +79,7 @@ __global__ void __launch_bounds__(LN * 32) k_project_tile(ProjArgs a, const __gr
     const int j = cc / g.K1, k1 = cc - j * g.K1;
     const bool mean_mode = (c == 0);
     const double e1 = a.d1[k1], e2 = a.d2[j];
-    auto U = [&](int f, int z) -> double2 { return tile[(f * n + z) * LN + lane]; };
+    auto U = [&](int f, int z) -> double2 { return tile[f * FS + z * LN + lane]; };
     double2 wprev = make_double2(0.0, 0.0);
     if (z0 > 0 && len > 0) wprev = U(2, z0 - 1);
     double2 X[LMAX];

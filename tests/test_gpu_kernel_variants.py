@@ -413,12 +413,12 @@ def test_twopass_x_variants_fp64(oracle, BLD, res, variant, name):
         assert e < 1e-12, (res, variant, f, e)
 
 
-@pytest.mark.parametrize("tile", ["8", "16"])
+@pytest.mark.parametrize("tile", ["4", "8", "16"])
 @pytest.mark.parametrize("res,flux", [((16, 12, 7), False), ((24, 20, 40), True), ((16, 16, 200), False),
                                       ((64, 64, 96), True), ((17, 12, 9), False)])
 def test_projection_tile(oracle, BLD, tile, res, flux):
     """k_project_tile (each block's columns brought into shared memory by TMA
-    tensor copies, 8 or 16 columns per block) forced for the projections of
+    tensor copies, 4, 8 or 16 columns per block) forced for the projections of
     stored stage values: apply_projections and 10 chained SSP-RK33 steps against
     the oracle, with and without ConstantMean.  An odd number of modes per layer
     (17 x 12: F = 9 x 11) keeps the z-segmented kernel."""
