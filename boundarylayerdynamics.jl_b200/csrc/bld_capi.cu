@@ -2513,7 +2513,9 @@ int32_t bld_apply_projections(bld_handle* h, int32_t m, double* v1, double* v2, 
     CUDA_TRY(cudaSetDevice(h->device));
     BLD_TRY(copy_fields_h2d(h, h->io, m, v1, v2, v3));
     BLD_TRY(enqueue_project(h, S_NONE, 0.0, h->io, nullptr, nullptr, nullptr, h->io, m, 1));
-    return copy_fields_d2h(h, h->io, m, v1, v2, v3);
+    BLD_TRY(copy_fields_d2h(h, h->io, m, v1, v2, v3));
+    // the tile projection's bounded wait reports through the flags
+    return check_flag(h);
 }
 
 int32_t bld_prepare(bld_handle* h) {

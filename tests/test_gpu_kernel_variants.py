@@ -572,3 +572,56 @@ def test_sgs_rows_kernel_trajectory(oracle, BLD, precision, tol):
     for f in om.fields:
         e = rel_l2(gm.state[f], om.state[f])
         assert e < tol, (precision, f, e)
+
+
+def _with_env(env, fn):
+    saved = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        return fn()
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+@pytest.mark.parametrize("kind", ["projection_tile", "sgs_rows", "sgs_staged"])
+def test_bounded_wait_timeout_exit_other_kernels(oracle, BLD, kind):
+    """The timeout exit of the other kernels that wait for their own TMA copies
+    (the tile projection, the SGS x kernel with staged row groups, the two-pass
+    SGS x kernel with staged rows), each forced, with the device's wait limit at
+    0: the call reports BLD_ERR_TIMEOUT; with the limit restored the same handle
+    gives the oracle's result again."""
+    from BoundaryLayerDynamics import _capi
+    if kind == "projection_tile":
+        res, les, env = (64, 64, 6), False, {"BLD_PROJ_TILE": "8"}
+    elif kind == "sgs_rows":
+        res, les, env = (64, 12, 6), True, {"BLD_SGS_X_KERNEL": "rows"}
+    else:
+        res, les, env = (64, 12, 6), True, {"BLD_SGS_X_KERNEL": "twopass_staged"}
+    gm = _with_env(env, lambda: _build(BLD, res, "fp64", les=les))
+    om = _build(oracle, res, les=les)
+    if kind == "projection_tile":
+        assert gm.kernels()["projection_stored"].startswith("k_project_tile<"), gm.kernels()
+        rng = np.random.default_rng(5)
+        st = {f: rng.standard_normal(om.state[f].shape) + 1j * rng.standard_normal(om.state[f].shape)
+              for f in om.fields}
+        call = lambda g: g.apply_projections({f: v.copy() for f, v in st.items()})
+    else:
+        st = _state(om, seed=17)
+        call = lambda g: g.compute_rates(st)
+    ref = call(om)
+    lib = _capi.load()
+    _capi.check(lib.bld_set_wait_limit(0, 0))
+    try:
+        with pytest.raises(_capi.BldError) as err:
+            call(gm)
+        assert err.value.status == _capi.BLD_ERR_TIMEOUT, err.value
+    finally:
+        _capi.check(lib.bld_set_wait_limit(0, -1))
+    got = call(gm)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < 1e-12, (kind, f, e)
