@@ -97,17 +97,46 @@ __global__ void __launch_bounds__(sx2_threads(B, sx2_rows(sizeof(cplx<R>), A * B
 #pragma unroll
     for (int i = 0; i < PPT; ++i) cy[i] = SgsCarry<R>{};
 
-    for (int j = jb; j <= jend; ++j) {
+    // forward lines of the previous layer, and which of its outputs it writes
+    bool pfw = false, pdoC = false, pdo67 = false, pdo5 = false;
+    // the last pass (j = jend + 1) only unpacks layer jend
+    for (int j = jb; j <= jend + 1; ++j) {
         const bool hasC = (j <= n3 - 1), hasI = (j <= n3 - 2);
         const int s = (j - jb) & 1;
-        if (hasC) {
-            // stage s ^ 1 was last read by layer j - 1's pass 1, several barriers ago
-            const bool more = j + 1 <= min(jend, n3 - 1);
-            if (threadIdx.x == 0 && more) {
-                fence_async_shared();
-                issue(j + 1, s ^ 1);
+        // stage s ^ 1 was last read by layer j - 1's pass 1, several barriers ago
+        const bool more = hasC && j + 1 <= min(jend, n3 - 1);
+        if (threadIdx.x == 0 && more) {
+            fence_async_shared();
+            issue(j + 1, s ^ 1);
+        }
+        // the unpack of layer j - 1 shares a barrier interval with the pass 1 of
+        // layer j: they touch different buffers (Ph, X1)
+        if (pfw) {
+            // ---- unpack layer j - 1's spectra: pairs (0,1) (2,3) (4,5) (6,7)
+            for (int task = threadIdx.x; task < NLF * K1; task += T) {
+                const int line = fdiv(task, a.k1_magic), k = task - line * K1;
+                const int r = line / 4, q = line - 4 * r, y = y0 + r;
+                C Av, Bv;
+                unpack_pair<R, 0>(Ph + line * P, k, P, Av, Bv);
+                const int ta = 2 * q, tb = 2 * q + 1;
+                if (ta <= 4) {
+                    if (pdoC) mrow_w(Mout, a, ta, j - 2, y)[k] = Av;
+                } else if (pdo67) {
+                    mrow_w(Mout, a, ta, j - 2, y)[k] = Av;
+                }
+                if (tb <= 4) {
+                    if (pdoC) mrow_w(Mout, a, tb, j - 2, y)[k] = Bv;
+                } else if (tb == 5) {
+                    if (pdo5) mrow_w(Mout, a, 5, j - 3, y)[k] = Bv;
+                } else if (pdo67) {
+                    mrow_w(Mout, a, tb, j - 2, y)[k] = Bv;
+                }
             }
-            const bool arrived = mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1, wait_limit);
+        }
+        if (j == jend + 1) break;
+        bool arrived = true;
+        if (hasC) {
+            arrived = mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1, wait_limit);
             const C* cur = stage + (size_t)s * 9 * NR * K1;
             // ---- inverse pass 1: lines L = 5 r + qq, packed pairs of terms
             // (0,1) (3,4) (5,6) (2,7) (8,-), the last two only below the top layer
@@ -140,16 +169,18 @@ __global__ void __launch_bounds__(sx2_threads(B, sx2_rows(sizeof(cplx<R>), A * B
 #pragma unroll
                 for (int q = 0; q < A; ++q) X1[L * X1L + q * X1S + jt] = x[q];
             }
-            // a block whose wait expired stops here (uniformly), after the copies
-            // it issued have landed
-            if (__syncthreads_or(!arrived)) {
-                if (threadIdx.x == 0) {
-                    atomicOr(a.flag + m, BLD_FLAG_TIMEOUT);
-                    mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1);
-                    if (more) mbar_wait_bounded(&bar[s ^ 1], ((j + 1 - jb) >> 1) & 1);
-                }
-                return;
+        }
+        // a block whose wait expired stops here (uniformly), after the copies it
+        // issued have landed
+        if (__syncthreads_or(!arrived)) {
+            if (threadIdx.x == 0) {
+                atomicOr(a.flag + m, BLD_FLAG_TIMEOUT);
+                mbar_wait_bounded(&bar[s], ((j - jb) >> 1) & 1);
+                if (more) mbar_wait_bounded(&bar[s ^ 1], ((j + 1 - jb) >> 1) & 1);
             }
+            return;
+        }
+        if (hasC) {
             // ---- inverse pass 2 -> physical lines Ph[L][x]
             for (int task = threadIdx.x; task < NLI * A; task += T) {
                 const int L = task / A, j2 = task - L * A;
@@ -219,27 +250,10 @@ __global__ void __launch_bounds__(sx2_threads(B, sx2_rows(sizeof(cplx<R>), A * B
                 for (int q = 0; q < B; ++q) Ph[L * P + j2 + A * q] = x[q];
             }
             __syncthreads();
-            // ---- unpack the two real lines of each spectrum: pairs (0,1) (2,3) (4,5) (6,7)
-            for (int task = threadIdx.x; task < NLF * K1; task += T) {
-                const int line = fdiv(task, a.k1_magic), k = task - line * K1;
-                const int r = line / 4, q = line - 4 * r, y = y0 + r;
-                C Av, Bv;
-                unpack_pair<R, 0>(Ph + line * P, k, P, Av, Bv);
-                const int ta = 2 * q, tb = 2 * q + 1;
-                if (ta <= 4) {
-                    if (doC) mrow_w(Mout, a, ta, c, y)[k] = Av;
-                } else if (do67) {
-                    mrow_w(Mout, a, ta, c, y)[k] = Av;
-                }
-                if (tb <= 4) {
-                    if (doC) mrow_w(Mout, a, tb, c, y)[k] = Bv;
-                } else if (tb == 5) {
-                    if (do5) mrow_w(Mout, a, 5, j - 2, y)[k] = Bv;
-                } else if (do67) {
-                    mrow_w(Mout, a, tb, c, y)[k] = Bv;
-                }
-            }
         }
-        __syncthreads();
+        pfw = doC || do5;
+        pdoC = doC;
+        pdo67 = do67;
+        pdo5 = do5;
     }
 }
