@@ -127,7 +127,8 @@ struct YCfg {
     int wfft = 0;  // per-term kernels: radix of the warp transform (P2 = 32 wfft), 0 = block stages
     int tp = 0;    // 1: two-pass kernels (k_inv_y2 / k_fwd_y2), BLD_Y2_NL lines, P2 = A * B;
                    // 2: inverse pass with TMA-staged tiles (k_inv_y3), BLD_Y3_NL lines;
-                   // 3: forward two-pass kernel on 8 lines, 3 blocks per SM, 4 outputs in flight
+                   // 3: forward two-pass kernel on 8 lines, 3 blocks per SM, 4 outputs in flight;
+                   // 4: forward two-pass kernel, single precision, 2 outputs in flight
     int zc = 1;    // tp 2: layer chunks (blocks along z)
 };
 
@@ -391,6 +392,9 @@ int launch_y2_p(bld_handle* h, bool inverse, const void* args, dim3 grid, size_t
     constexpr int MINBI = y2_min_blocks_inv<R>(B * BLD_Y2_NL);
     if (!inverse && tp == 3)
         k_fwd_y2<R, A, B, 3, 8, 4><<<grid, B * 8, sm, h->stream>>>(*static_cast<const FwdYArgs*>(args));
+    else if (!inverse && tp == 4 && sizeof(R) == 4)
+        k_fwd_y2<R, A, B, MINB, BLD_Y2_NL, 2><<<grid, B * BLD_Y2_NL, sm, h->stream>>>(
+            *static_cast<const FwdYArgs*>(args));
     else if (inverse)
         k_inv_y2<R, A, B, MINBI><<<grid, B * BLD_Y2_NL, sm, h->stream>>>(*static_cast<const InvYArgs*>(args));
     else
@@ -585,7 +589,7 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
     a.NL = c.NL;
     const size_t cs = csize(sizeof(R) == 4);
     if (c.tp) {
-        const int nl = c.tp == 3 ? 8 : BLD_Y2_NL;
+        const int nl = c.tp == 3 ? 8 : BLD_Y2_NL;   // tp 1, 2, 4: BLD_Y2_NL lines
         a.NL = nl;
         dim3 grid(a.fields * nm, (h->g.K1 + nl - 1) / nl, h->g.n3);
         BLD_TRY(launch_y2<R>(h, s.P2, false, &a, grid, smem_y2(s.P2, s.fsets * nl, sizeof(R) == 4), c.tp));
@@ -970,7 +974,9 @@ int set_smem_limits_R() {
 #define BLD_SET_Y2(P)                                                                                  \
     BLD_SET((k_inv_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks_inv<R>(y2_radix_b(P) * BLD_Y2_NL)>)); \
     BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks<R>(y2_radix_b(P) * BLD_Y2_NL)>)); \
-    BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), 3, 8, 4>));
+    BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), 3, 8, 4>));                                                                   \
+    if constexpr (sizeof(R) == 4)                                                                    \
+        BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks<R>(y2_radix_b(P) * BLD_Y2_NL), BLD_Y2_NL, 2>));
     BLD_SET_Y2(64)
     BLD_SET_Y2(96)
     BLD_SET_Y2(128)
@@ -1351,6 +1357,12 @@ bool yforce_twopass8() {
     const char* e = getenv("BLD_Y_KERNEL");
     return e && !strcmp(e, "twopass8");
 }
+// BLD_Y_KERNEL=twopass2: the two-pass kernels with two outputs of the forward
+// epilogue in flight (single precision; double keeps one)
+bool yforce_twopass2() {
+    const char* e = getenv("BLD_Y_KERNEL");
+    return e && !strcmp(e, "twopass2");
+}
 
 // y-pass candidates: per-term blocks (two-buffer FFT) with several line counts
 // and block sizes, and all-terms blocks (in-place FFT); lines * element size of
@@ -1382,6 +1394,10 @@ std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_pe
         c.thr = y2_radix_b(s.P2) * BLD_Y2_NL;
         c.tp = 1;
         out.push_back(c);
+        if (!inverse && h->fp32) {   // single precision: two outputs of the epilogue in flight
+            c.tp = 4;
+            out.push_back(c);
+        }
         if (!inverse) {   // eight lines, more blocks per SM
             c.NL = 8;
             c.thr = y2_radix_b(s.P2) * 8;
@@ -1389,11 +1405,11 @@ std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_pe
             out.push_back(c);
         }
     }
-    if (tp_ok && (yforce_twopass() || yforce_twopass8() || (yforce_tma() && !inverse))) {
+    if (tp_ok && (yforce_twopass() || yforce_twopass8() || yforce_twopass2() || (yforce_tma() && !inverse))) {
         YCfg c{};
         c.NL = BLD_Y2_NL;
         c.thr = y2_radix_b(s.P2) * BLD_Y2_NL;
-        c.tp = 1;
+        c.tp = (yforce_twopass2() && !inverse && h->fp32) ? 4 : 1;
         if (yforce_twopass8() && !inverse) {
             c.NL = 8;
             c.thr = y2_radix_b(s.P2) * 8;
@@ -2901,7 +2917,7 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         else if (s.inv.all) snprintf(iname, sizeof iname, "k_inv_y_all<%s>", R);
         else snprintf(iname, sizeof iname, "k_inv_y<%s, %d>", R, s.inv.wfft);
         if (s.fwd.tp) snprintf(fname, sizeof fname, "k_fwd_y2<%s, %d, %d%s>", R, y2_radix_a(s.P2), y2_radix_b(s.P2),
-                               s.fwd.tp == 3 ? ", 8 lines" : "");
+                               s.fwd.tp == 3 ? ", 8 lines" : (s.fwd.tp == 4 ? ", 2 outputs" : ""));
         else if (s.fwd.all) snprintf(fname, sizeof fname, "k_fwd_y_all<%s>", R);
         else snprintf(fname, sizeof fname, "k_fwd_y<%s, %d>", R, s.fwd.wfft);
         snprintf(tmp, sizeof tmp,

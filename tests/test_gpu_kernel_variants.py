@@ -212,11 +212,11 @@ Y2_SIZES_FP32 = {384, 512, 768}
 
 
 @pytest.mark.parametrize("res,precision,les,tol", Y_CASES)
-@pytest.mark.parametrize("family", ["warp", "block", "twopass", "twopass8", "tma"])
+@pytest.mark.parametrize("family", ["warp", "block", "twopass", "twopass8", "twopass2", "tma"])
 def test_y_kernel_family(oracle, BLD, res, precision, les, tol, family):
     om = _build(oracle, res, les=les)
     gm = _forced_y(BLD, family, res, precision, les)
-    if family in ("twopass", "twopass8", "tma"):   # the forced family is the one that runs where it is compiled
+    if family in ("twopass", "twopass8", "twopass2", "tma"):   # the forced family is the one that runs where it is compiled
         inv = "k_inv_y3<" if family == "tma" else "k_inv_y2<"
         for space in gm.kernels().values():
             if not isinstance(space, dict):
@@ -227,6 +227,7 @@ def test_y_kernel_family(oracle, BLD, res, precision, les, tol, family):
             if p2 in Y2_SIZES or (precision == "mixed" and p2 in Y2_SIZES_FP32):
                 assert space["inv_y"].startswith(inv) and space["fwd_y"].startswith("k_fwd_y2<"), space
                 assert (family == "twopass8") == space["fwd_y"].endswith(", 8 lines>"), space
+                assert (family == "twopass2" and precision == "mixed") == space["fwd_y"].endswith(", 2 outputs>"), space
     st = _state(om, seed=sum(res) + 1)
     ref = om.compute_rates(st)
     got = gm.compute_rates(st)
