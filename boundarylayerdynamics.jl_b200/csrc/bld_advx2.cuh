@@ -27,14 +27,18 @@
 //
 // Variants (V): 0 as above; 2 (wide) runs it with 1.5x the threads (fewer
 // product points, hence fewer registers, per thread: two blocks of six warps
-// per SM in double precision instead of two of four).
+// per SM in double precision instead of two of four); 3 (single precision up
+// to P1 = 384) takes two rows per block instead of four: blocks of four warps,
+// four per SM.
 #pragma once
 
 #include "bld_tma.cuh"
 
 // y rows per block: 2 in double precision, 4 in single up to P1 = 384 (shared
-// memory per block)
-__host__ __device__ constexpr int x2_rows(int csz, int P) { return csz == 16 || P > 384 ? 2 : 4; }
+// memory per block); variant 3 takes 2 in single precision too
+__host__ __device__ constexpr int x2_rows(int csz, int P, int V = 0) {
+    return V == 3 || csz == 16 || P > 384 ? 2 : 4;
+}
 __host__ __device__ constexpr int x2_threads(int B, int NR, int V = 0) {
     return (V == 2 ? (9 * NR * B / 2 + 31) : (3 * NR * B + 31)) / 32 * 32;
 }
@@ -42,21 +46,21 @@ __host__ __device__ constexpr int x2_al(int b) { return (b + 127) / 128 * 128; }
 // dynamic shared memory: barriers, twiddles, 2 stages x 6 terms x NR rows,
 // pass-1 buffer (3 NR lines of A (B + 1)), physical / spectral lines (3 NR x P),
 // forward inputs (NR + NR / 2 lines of P)
-__host__ __device__ constexpr int x2_smem(int A, int B, int K1, int csz) {
-    return 128 + x2_al(A * B * csz) + x2_al(2 * 6 * x2_rows(csz, A * B) * K1 * csz) +
-           x2_al(3 * x2_rows(csz, A * B) * (A * (B + 1) + 128 / csz) * csz) +
-           x2_al(3 * x2_rows(csz, A * B) * A * B * csz) +
-           x2_al((x2_rows(csz, A * B) + x2_rows(csz, A * B) / 2) * A * B * csz);
+__host__ __device__ constexpr int x2_smem(int A, int B, int K1, int csz, int V = 0) {
+    return 128 + x2_al(A * B * csz) + x2_al(2 * 6 * x2_rows(csz, A * B, V) * K1 * csz) +
+           x2_al(3 * x2_rows(csz, A * B, V) * (A * (B + 1) + 128 / csz) * csz) +
+           x2_al(3 * x2_rows(csz, A * B, V) * A * B * csz) +
+           x2_al((x2_rows(csz, A * B, V) + x2_rows(csz, A * B, V) / 2) * A * B * csz);
 }
 // blocks per SM a variant is compiled for (its register cap; 0: the compiler's choice)
-__host__ __device__ constexpr int x2_minb(int csz, int V) { return V == 2 ? 2 : 0; }
+__host__ __device__ constexpr int x2_minb(int csz, int V) { return V == 2 ? 2 : (V == 3 ? 4 : 0); }
 
-// grid (P2 / NR, nchunks, members), block x2_threads(B, NR, V); NR = x2_rows(sizeof(C), P)
+// grid (P2 / NR, nchunks, members), block x2_threads(B, NR, V); NR = x2_rows(sizeof(C), P, V)
 template <typename R, int A, int B, int V = 0>
-__global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B), V), x2_minb(sizeof(cplx<R>), V))
+__global__ void __launch_bounds__(x2_threads(B, x2_rows(sizeof(cplx<R>), A * B, V), V), x2_minb(sizeof(cplx<R>), V))
     k_adv_x2(XArgs a, int* flag) {
     using C = cplx<R>;
-    constexpr int P = A * B, NR = x2_rows(sizeof(C), P), NLI = 3 * NR, NLF = NR + NR / 2;
+    constexpr int P = A * B, NR = x2_rows(sizeof(C), P, V), NLI = 3 * NR, NLF = NR + NR / 2;
     constexpr int T = x2_threads(B, NR, V);
     constexpr int PPT = (NR * P + T - 1) / T;   // product points per thread
     constexpr int X1S = B + 1;                  // pass-1 stride of a task's outputs

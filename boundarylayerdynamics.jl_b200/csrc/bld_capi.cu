@@ -278,7 +278,7 @@ int pick_y(int P2, bool fp32, int sets) {
 // fill the GPU a few times over, at least 8 layers per chunk
 void x_chunks(const bld_handle* h, Space& s) {
     const int n3 = h->g.n3;
-    const int rows = s.x2 ? x2_rows((int)csize(h->fp32), s.P1)
+    const int rows = s.x2 ? x2_rows((int)csize(h->fp32), s.P1, s.x2 - 1)
                            : (s.sxk ? sx2_rows((int)csize(h->fp32), s.P1) : (s.xb ? 1 : (s.xw ? s.xw : s.YT)));
     const long long blocks_per_chunk = (long long)((s.P2 + rows - 1) / rows) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
@@ -627,18 +627,20 @@ int launch_fwd_y(bld_handle* h, const Space& s, FwdYArgs a, int nm) {
 
 // two-pass advection x kernel: compiled for P1 with a two-pass factorisation
 // (single precision up to 768, double up to 288), whole row pairs per block;
-// variant V = 2 (wide) in double precision only
+// variants V = 2 (wide) in double precision, V = 3 (two rows) in single precision up to 384
 bool x2_ok(const bld_handle* h, const Space& s, int V = 0) {
-    return y2_ok(s.P1, h->fp32) && s.P2 % x2_rows((int)csize(h->fp32), s.P1) == 0 && (V == 0 || (V == 2 && !h->fp32)) &&
-           x2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, (int)csize(h->fp32)) <= 227 * 1024;
+    const int cs = (int)csize(h->fp32);
+    return y2_ok(s.P1, h->fp32) && s.P2 % x2_rows(cs, s.P1, V) == 0 &&
+           (V == 0 || (V == 2 && !h->fp32) || (V == 3 && h->fp32 && s.P1 <= 384)) &&
+           x2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, cs, V) <= 227 * 1024;
 }
 
 template <typename R, int P, int V>
 void launch_x2_pv(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
-    constexpr int NR = x2_rows((int)sizeof(cplx<R>), P);
+    constexpr int NR = x2_rows((int)sizeof(cplx<R>), P, V);
     dim3 grid(s.P2 / NR, s.nchunks, nm);
-    const size_t sm = x2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>));
+    const size_t sm = x2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>), V);
     k_adv_x2<R, A, B, V><<<grid, x2_threads(B, NR, V), sm, h->stream>>>(a, h->flag);
 }
 
@@ -646,6 +648,9 @@ template <typename R, int P>
 int launch_x2_p(bld_handle* h, const Space& s, const XArgs& a, int nm) {
     if constexpr (sizeof(R) == 8) {
         if (s.x2 == 3) return launch_x2_pv<R, P, 2>(h, s, a, nm), BLD_OK;
+    }
+    if constexpr (sizeof(R) == 4 && P <= 384) {
+        if (s.x2 == 4) return launch_x2_pv<R, P, 3>(h, s, a, nm), BLD_OK;
     }
     launch_x2_pv<R, P, 0>(h, s, a, nm);
     return BLD_OK;
@@ -1008,6 +1013,9 @@ int set_smem_limits_R() {
     BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P), 0>));            \
     if constexpr (sizeof(R) == 8) {                                     \
         BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P), 2>));        \
+    }                                                                   \
+    if constexpr (sizeof(R) == 4 && P <= 384) {                         \
+        BLD_SET((k_adv_x2<R, y2_radix_a(P), y2_radix_b(P), 3>));        \
     }
     BLD_SET_X2(64)
     BLD_SET_X2(96)
@@ -1727,10 +1735,10 @@ int autotune_impl(bld_handle* h) {
             if ((xbk == 1 && only_pipe) || (xbk == 2 && only_bw3)) continue;
             BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, xbk, 2, 0, 0, 0}));
         }
-        // the two-pass kernel's variants (BLD_X2_VARIANT = 0, 2 forces one)
+        // the two-pass kernel's variants (BLD_X2_VARIANT = 0, 2, 3 forces one)
         const char* x2v = getenv("BLD_X2_VARIANT");
         const int x2_only = x2v && x2v[0] ? atoi(x2v) : -1;
-        for (int v = 0; v <= 2; ++v)
+        for (int v = 0; v <= 3; ++v)
             if (sp == 0 && x2_ok(h, s, v) && (only_x2 || !xk || x2_asked) && (x2_only < 0 || x2_only == v))
                 BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 1 + v, 0, 0}));
         if (bx >= 1e30f) return fail(BLD_ERR_INVALID_CONFIG, "no x kernel could be timed");
@@ -2898,7 +2906,7 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         char xname[96];
         if (sp == 0 && s.x2)
             snprintf(xname, sizeof xname, "k_adv_x2<%s, %d, %d%s>", R, y2_radix_a(s.P1), y2_radix_b(s.P1),
-                     s.x2 == 3 ? ", wide" : "");
+                     s.x2 == 3 ? ", wide" : (s.x2 == 4 ? ", 2 rows" : ""));
         else if (sp == 0 && s.xb)
             snprintf(xname, sizeof xname, "%s<%s, %d>", s.xb == 2 ? "k_adv_xp" : "k_adv_xb", R, s.P1 / 32);
         else if (sp == 0 && s.xw && s.xwmb > 1)

@@ -626,3 +626,20 @@ def test_bounded_wait_timeout_exit_other_kernels(oracle, BLD, kind):
     for f in om.fields:
         e = rel_l2(got[f], ref[f])
         assert e < 1e-12, (kind, f, e)
+
+
+@pytest.mark.parametrize("res", [(192, 8, 5), (64, 12, 6), (256, 6, 4)])
+def test_twopass_x_two_rows_mixed(oracle, BLD, res):
+    """The single-precision two-pass x kernel with two rows per block (four blocks
+    of four warps per SM instead of two of seven), forced, against the oracle at
+    the mixed form's 1e-5."""
+    gm = _with_env({"BLD_X_KERNEL": "twopass", "BLD_X2_VARIANT": "3"}, lambda: _build(BLD, res, "mixed"))
+    xk = gm.kernels()["advection"]["x"]
+    assert xk.startswith("k_adv_x2<float") and xk.endswith(", 2 rows>"), xk
+    om = _build(oracle, res)
+    st = _state(om, seed=sum(res) + 31)
+    ref = om.compute_rates(st)
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < 1e-5, (res, f, e)
