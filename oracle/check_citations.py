@@ -20,18 +20,25 @@ import sys
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DEFAULT_REF = "/root/reference"
 CITE = re.compile(r"\b((?:src|test|docs|benchmark)/[A-Za-z0-9_./-]+\.(?:jl|md|toml)):(\d+(?:-\d+)?(?:,\d+(?:-\d+)?)*)")
-SKIP_DIRS = {".git", "_work", "gpurun_out", "__pycache__", ".pytest_cache", "baseline", "lib", "golden"}
-# files written by others (the survey, the reviews) are not this code's citations
-SKIP_FILES = {"SURVEY.md", "VERDICT.md", "ADVICE.md", "BASELINE.json", "PROGRESS.jsonl"}
-EXTS = (".py", ".cu", ".cuh", ".h", ".md", ".jl", ".c", ".cpp")
+# this repository's own sources: the package, the kernels, the header, the
+# oracle, the tests, the bench and entry points, and the design and integration notes
+SOURCE_DIRS = ("boundarylayerdynamics.jl_b200/BoundaryLayerDynamics", "boundarylayerdynamics.jl_b200/csrc",
+               "include", "oracle", "tests")
+SOURCE_FILES = ("bench.py", "__graft_entry__.py", "DESIGN.md", "INTEGRATION.md", "README.md")
+EXTS = (".py", ".cu", ".cuh", ".h", ".md", ".c", ".cpp")
 
 
 def repo_files(root):
-    for d, dirs, files in os.walk(root):
-        dirs[:] = [x for x in dirs if x not in SKIP_DIRS and not x.startswith(".")]
-        for f in files:
-            if f.endswith(EXTS) and f not in SKIP_FILES:
-                yield os.path.join(d, f)
+    for d in SOURCE_DIRS:
+        base = os.path.join(root, d)
+        for f in sorted(os.listdir(base)) if os.path.isdir(base) else ():
+            p = os.path.join(base, f)
+            if os.path.isfile(p) and f.endswith(EXTS):
+                yield p
+    for f in SOURCE_FILES:
+        p = os.path.join(root, f)
+        if os.path.isfile(p):
+            yield p
 
 
 def line_counts(ref):
