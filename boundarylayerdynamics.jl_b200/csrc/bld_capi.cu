@@ -155,7 +155,7 @@ struct Space {
     int sx2 = 0;                                    // SGS block x kernel with two-pass line transforms: 1 plain,
                                                     // 2 registers capped for two blocks of 256 threads per SM,
                                                     // 3 / 4 as 1 / 2 with the input rows staged by bulk copies
-    int sxk = 0;                                    // 1: SGS x kernel k_sgs_x2 (rows staged by bulk copies, two-pass lines)
+    int sxk = 0;                                    // 1 + V: SGS x kernel k_sgs_x2<.., V> (rows staged by bulk copies, two-pass lines)
     int xr = 0;                                     // block x kernels: warp-transform radix (P1 = 32 xr), 0 = Stockham
     int fsets = 1;                                  // forward line sets (2 when a D2 contribution exists)
     YCfg inv, fwd;                                  // y-pass variants (chosen by the autotuner)
@@ -279,7 +279,7 @@ int pick_y(int P2, bool fp32, int sets) {
 void x_chunks(const bld_handle* h, Space& s) {
     const int n3 = h->g.n3;
     const int rows = s.x2 ? x2_rows((int)csize(h->fp32), s.P1, s.x2 - 1)
-                           : (s.sxk ? sx2_rows((int)csize(h->fp32), s.P1) : (s.xb ? 1 : (s.xw ? s.xw : s.YT)));
+                           : (s.sxk ? sx2_rows((int)csize(h->fp32), s.P1, s.sxk - 1) : (s.xb ? 1 : (s.xw ? s.xw : s.YT)));
     const long long blocks_per_chunk = (long long)((s.P2 + rows - 1) / rows) * h->B;
     int want = (int)std::max<long long>(1, (900 + blocks_per_chunk - 1) / blocks_per_chunk);
     want = std::min(want, std::max(1, n3 / 8));
@@ -860,19 +860,28 @@ bool sx2_ok(const bld_handle* h, const Space& s, int v = 1) {
 }
 
 // k_sgs_x2: compiled for the two-pass sizes; whole row groups per block
-bool sxk_ok(const bld_handle* h, const Space& s) {
+// V = 1 (two rows per block) in single precision up to P1 = 384
+bool sxk_ok(const bld_handle* h, const Space& s, int V = 0) {
     const int cs = (int)csize(h->fp32);
-    return y2_ok(s.P1, h->fp32) && s.P2 % sx2_rows(cs, s.P1) == 0 &&
-           sx2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, cs) <= 227 * 1024;
+    return y2_ok(s.P1, h->fp32) && (V == 0 || (h->fp32 && s.P1 <= 384)) && s.P2 % sx2_rows(cs, s.P1, V) == 0 &&
+           sx2_smem(y2_radix_a(s.P1), y2_radix_b(s.P1), h->g.K1, cs, V) <= 227 * 1024;
+}
+
+template <typename R, int P, int V>
+void launch_sgs_xk_pv(bld_handle* h, const Space& s, const XArgs& a, int nm) {
+    constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
+    constexpr int NR = sx2_rows((int)sizeof(cplx<R>), P, V);
+    dim3 grid(s.P2 / NR, s.nchunks, nm);
+    const size_t sm = sx2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>), V);
+    k_sgs_x2<R, A, B, V><<<grid, sx2_threads(B, NR), sm, h->stream>>>(a);
 }
 
 template <typename R, int P>
 int launch_sgs_xk_p(bld_handle* h, const Space& s, const XArgs& a, int nm) {
-    constexpr int A = y2_radix_a(P), B = y2_radix_b(P);
-    constexpr int NR = sx2_rows((int)sizeof(cplx<R>), P);
-    dim3 grid(s.P2 / NR, s.nchunks, nm);
-    const size_t sm = sx2_smem(A, B, h->g.K1, (int)sizeof(cplx<R>));
-    k_sgs_x2<R, A, B><<<grid, sx2_threads(B, NR), sm, h->stream>>>(a);
+    if constexpr (sizeof(R) == 4 && P <= 384) {
+        if (s.sxk == 2) return launch_sgs_xk_pv<R, P, 1>(h, s, a, nm), BLD_OK;
+    }
+    launch_sgs_xk_pv<R, P, 0>(h, s, a, nm);
     return BLD_OK;
 }
 
@@ -1031,7 +1040,8 @@ int set_smem_limits_R() {
     }
 #undef BLD_SET_X2
 #define BLD_SET_SX2(P) BLD_SET((k_sgs_x<R, 1, 0, P>)); BLD_SET((k_sgs_x<R, 2, 0, P>));   \
-    if constexpr (P <= 288) BLD_SET((k_sgs_x2<R, y2_radix_a(P), y2_radix_b(P)>));
+    if constexpr (P <= 288) BLD_SET((k_sgs_x2<R, y2_radix_a(P), y2_radix_b(P)>));          \
+    if constexpr (sizeof(R) == 4 && P <= 384) BLD_SET((k_sgs_x2<R, y2_radix_a(P), y2_radix_b(P), 1>));
     BLD_SET_SX2(64)
     BLD_SET_SX2(96)
     BLD_SET_SX2(128)
@@ -1497,7 +1507,7 @@ TuneKey tune_key(const bld_handle* h) {
     // any kernel-family switch in the environment makes its own entry
     int env = 0;
     for (const char* v : {"BLD_X_KERNEL", "BLD_Y_KERNEL", "BLD_XW_MINB", "BLD_PROJ_VARIANT", "BLD_X_LINES",
-                          "BLD_SGS_X_KERNEL", "BLD_X2_VARIANT", "BLD_PROJ_TILE"}) {
+                          "BLD_SGS_X_KERNEL", "BLD_X2_VARIANT", "BLD_PROJ_TILE", "BLD_SGS_X2_VARIANT"}) {
         const char* e = getenv(v);
         env = env * 31 + (e ? (int)(std::hash<std::string>{}(e) % 1000003) + 1 : 0);
     }
@@ -1727,7 +1737,12 @@ int autotune_impl(bld_handle* h) {
         if (block_ok && (sp == 1 || !only_x2) && !(sp == 1 && only_sxk))
             BLD_TRY(tune_chunks(XPick{byt, bppt, bxr, 0, 1, 0, 2, 0, bsx2, 0}));
         // the SGS kernel with staged rows and two-pass lines (BLD_SGS_X_KERNEL=rows keeps it)
-        if (sp == 1 && sxk_ok(h, s) && (!sk || only_sxk)) BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 0, 0, 1}));
+        // (BLD_SGS_X2_VARIANT = 0, 1 keeps one of its variants)
+        const char* sxv = getenv("BLD_SGS_X2_VARIANT");
+        const int sxv_only = sxv && sxv[0] ? atoi(sxv) : -1;
+        for (int v = 0; v <= 1; ++v)
+            if (sp == 1 && sxk_ok(h, s, v) && (!sk || only_sxk) && (sxv_only < 0 || sxv_only == v))
+                BLD_TRY(tune_chunks(XPick{1, 1, 0, 0, 1, 0, 2, 0, 0, 1 + v}));
         const bool warp_ok = sp == 0 && adv_warp_ok && !only_block && !only_bw && !only_lines && !only_x2;
         for (int wpb = 1; warp_ok && wpb <= 4; wpb *= 2) BLD_TRY(tune_chunks(XPick{1, 1, 0, wpb, 1, 0, 2, 0, 0, 0}));
         for (int xbk = 1; xbk <= 2; ++xbk) {
@@ -2914,7 +2929,8 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         else if (sp == 0 && s.xw)
             snprintf(xname, sizeof xname, "k_adv_xw<%s, %d>", R, s.P1 / 32);
         else if (sp == 1 && s.sxk)
-            snprintf(xname, sizeof xname, "k_sgs_x2<%s, %d, %d>", R, y2_radix_a(s.P1), y2_radix_b(s.P1));
+            snprintf(xname, sizeof xname, "k_sgs_x2<%s, %d, %d%s>", R, y2_radix_a(s.P1), y2_radix_b(s.P1),
+                     s.sxk == 2 ? ", 2 rows" : "");
         else if (sp == 1 && s.sx2)
             snprintf(xname, sizeof xname, "%s<%s, %d, 0, %d%s>", xk, R, s.PPT, s.P1, s.sx2 % 2 == 0 ? ", 2" : "");
         else

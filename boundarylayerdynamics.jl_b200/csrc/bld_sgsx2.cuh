@@ -22,23 +22,24 @@
 
 #include "bld_tma.cuh"
 
-// y rows per block: 2 in double precision and above P1 = 384 in single, else 4
-__host__ __device__ constexpr int sx2_rows(int csz, int P) { return csz == 16 || P > 384 ? 2 : 4; }
+// y rows per block: 2 in double precision and above P1 = 384 in single, else 4;
+// variant 1 takes 2 in single precision too (smaller blocks, more of them per SM)
+__host__ __device__ constexpr int sx2_rows(int csz, int P, int V = 0) { return V == 1 || csz == 16 || P > 384 ? 2 : 4; }
 __host__ __device__ constexpr int sx2_threads(int B, int NR) { return (5 * NR * B + 31) / 32 * 32; }
 // dynamic shared memory: barriers, twiddles, 2 stages x 9 terms x NR rows, the
 // pass-1 buffer (5 NR lines of A (B + 1) plus padding), physical / spectral
 // lines (5 NR x P), forward inputs (4 NR x P)
-__host__ __device__ constexpr int sx2_smem(int A, int B, int K1, int csz) {
-    return 128 + x2_al(A * B * csz) + x2_al(2 * 9 * sx2_rows(csz, A * B) * K1 * csz) +
-           x2_al(5 * sx2_rows(csz, A * B) * (A * (B + 1) + 128 / csz) * csz) +
-           x2_al(5 * sx2_rows(csz, A * B) * A * B * csz) + x2_al(4 * sx2_rows(csz, A * B) * A * B * csz);
+__host__ __device__ constexpr int sx2_smem(int A, int B, int K1, int csz, int V = 0) {
+    return 128 + x2_al(A * B * csz) + x2_al(2 * 9 * sx2_rows(csz, A * B, V) * K1 * csz) +
+           x2_al(5 * sx2_rows(csz, A * B, V) * (A * (B + 1) + 128 / csz) * csz) +
+           x2_al(5 * sx2_rows(csz, A * B, V) * A * B * csz) + x2_al(4 * sx2_rows(csz, A * B, V) * A * B * csz);
 }
 
-// grid (P2 / NR, nchunks, members), block sx2_threads(B, NR); NR = sx2_rows(sizeof(C), P)
-template <typename R, int A, int B>
-__global__ void __launch_bounds__(sx2_threads(B, sx2_rows(sizeof(cplx<R>), A * B))) k_sgs_x2(XArgs a) {
+// grid (P2 / NR, nchunks, members), block sx2_threads(B, NR); NR = sx2_rows(sizeof(C), P, V)
+template <typename R, int A, int B, int V = 0>
+__global__ void __launch_bounds__(sx2_threads(B, sx2_rows(sizeof(cplx<R>), A * B, V))) k_sgs_x2(XArgs a) {
     using C = cplx<R>;
-    constexpr int P = A * B, NR = sx2_rows(sizeof(C), P), NLI = 5 * NR, NLF = 4 * NR;
+    constexpr int P = A * B, NR = sx2_rows(sizeof(C), P, V), NLI = 5 * NR, NLF = 4 * NR;
     constexpr int T = sx2_threads(B, NR);
     constexpr int PPT = (NR * P + T - 1) / T;   // model points per thread
     constexpr int X1S = B + 1;                  // pass-1 stride of a task's outputs

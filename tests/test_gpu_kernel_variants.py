@@ -643,3 +643,20 @@ def test_twopass_x_two_rows_mixed(oracle, BLD, res):
     for f in om.fields:
         e = rel_l2(got[f], ref[f])
         assert e < 1e-5, (res, f, e)
+
+
+@pytest.mark.parametrize("res", [(64, 12, 6), (128, 8, 5), (96, 8, 5)])
+def test_sgs_rows_kernel_two_rows_mixed(oracle, BLD, res):
+    """k_sgs_x2 with two rows per block in single precision (smaller blocks, more
+    per SM), forced, against the oracle at the mixed form's 1e-5."""
+    gm = _with_env({"BLD_SGS_X_KERNEL": "rows", "BLD_SGS_X2_VARIANT": "1"},
+                   lambda: _build(BLD, res, "mixed", les=True))
+    xk = gm.kernels()["sgs"]["x"]
+    assert xk.startswith("k_sgs_x2<float") and xk.endswith(", 2 rows>"), xk
+    om = _build(oracle, res, les=True)
+    st = _state(om, seed=sum(res) + 41)
+    ref = om.compute_rates(st)
+    got = gm.compute_rates(st)
+    for f in om.fields:
+        e = rel_l2(got[f], ref[f])
+        assert e < 1e-5, (res, f, e)
