@@ -127,7 +127,8 @@ struct YCfg {
     int wfft = 0;  // per-term kernels: radix of the warp transform (P2 = 32 wfft), 0 = block stages
     int tp = 0;    // 1: two-pass kernels (k_inv_y2 / k_fwd_y2), BLD_Y2_NL lines, P2 = A * B;
                    // 2: inverse pass with TMA-staged tiles (k_inv_y3), BLD_Y3_NL lines;
-                   // 3: forward two-pass kernel on 8 lines, 3 blocks per SM, 4 outputs in flight;
+                   // 3: two-pass kernels on 8 lines (forward: 3 blocks per SM, 4 outputs in flight;
+                   //    inverse: 3 blocks per SM in double, 4 in single precision);
                    // 4: forward two-pass kernel, single precision, 2 outputs in flight
     int zc = 1;    // tp 2: layer chunks (blocks along z)
 };
@@ -392,6 +393,9 @@ int launch_y2_p(bld_handle* h, bool inverse, const void* args, dim3 grid, size_t
     constexpr int MINBI = y2_min_blocks_inv<R>(B * BLD_Y2_NL);
     if (!inverse && tp == 3)
         k_fwd_y2<R, A, B, 3, 8, 4><<<grid, B * 8, sm, h->stream>>>(*static_cast<const FwdYArgs*>(args));
+    else if (inverse && tp == 3)   // eight lines: three (double) or four (single precision) blocks per SM
+        k_inv_y2<R, A, B, sizeof(R) == 8 ? 3 : 4, 8><<<grid, B * 8, sm, h->stream>>>(
+            *static_cast<const InvYArgs*>(args));
     else if (!inverse && tp == 4 && sizeof(R) == 4)
         k_fwd_y2<R, A, B, MINB, BLD_Y2_NL, 2><<<grid, B * BLD_Y2_NL, sm, h->stream>>>(
             *static_cast<const FwdYArgs*>(args));
@@ -548,9 +552,10 @@ int launch_inv_y(bld_handle* h, const Space& s, InvYArgs a, int nm) {
         return BLD_OK;
     }
     if (c.tp) {
-        a.NL = BLD_Y2_NL;
-        dim3 grid(a.nterms * nm, (h->g.K1 + BLD_Y2_NL - 1) / BLD_Y2_NL, h->g.n3);
-        BLD_TRY(launch_y2<R>(h, s.P2, true, &a, grid, smem_y2(s.P2, BLD_Y2_NL, sizeof(R) == 4)));
+        const int nl = c.tp == 3 ? 8 : BLD_Y2_NL;
+        a.NL = nl;
+        dim3 grid(a.nterms * nm, (h->g.K1 + nl - 1) / nl, h->g.n3);
+        BLD_TRY(launch_y2<R>(h, s.P2, true, &a, grid, smem_y2(s.P2, nl, sizeof(R) == 4), c.tp));
         CUDA_TRY(cudaGetLastError());
         return BLD_OK;
     }
@@ -989,6 +994,7 @@ int set_smem_limits_R() {
     BLD_SET((k_inv_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks_inv<R>(y2_radix_b(P) * BLD_Y2_NL)>)); \
     BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks<R>(y2_radix_b(P) * BLD_Y2_NL)>)); \
     BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), 3, 8, 4>));                                                                   \
+    BLD_SET((k_inv_y2<R, y2_radix_a(P), y2_radix_b(P), sizeof(R) == 8 ? 3 : 4, 8>));                                                \
     if constexpr (sizeof(R) == 4)                                                                    \
         BLD_SET((k_fwd_y2<R, y2_radix_a(P), y2_radix_b(P), y2_min_blocks<R>(y2_radix_b(P) * BLD_Y2_NL), BLD_Y2_NL, 2>));
     BLD_SET_Y2(64)
@@ -1416,7 +1422,7 @@ std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_pe
             c.tp = 4;
             out.push_back(c);
         }
-        if (!inverse) {   // eight lines, more blocks per SM
+        {   // eight lines, more blocks per SM
             c.NL = 8;
             c.thr = y2_radix_b(s.P2) * 8;
             c.tp = 3;
@@ -1428,7 +1434,7 @@ std::vector<YCfg> y_candidates(const bld_handle* h, const Space& s, int lines_pe
         c.NL = BLD_Y2_NL;
         c.thr = y2_radix_b(s.P2) * BLD_Y2_NL;
         c.tp = (yforce_twopass2() && !inverse && h->fp32) ? 4 : 1;
-        if (yforce_twopass8() && !inverse) {
+        if (yforce_twopass8()) {
             c.NL = 8;
             c.thr = y2_radix_b(s.P2) * 8;
             c.tp = 3;
@@ -2937,7 +2943,8 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
             snprintf(xname, sizeof xname, "%s<%s, %d, %d>", xk, R, s.PPT, s.xr);
         char iname[64], fname[64];
         if (s.inv.tp == 2) snprintf(iname, sizeof iname, "k_inv_y3<%s, %d, %d>", R, y2_radix_a(s.P2), y2_radix_b(s.P2));
-        else if (s.inv.tp) snprintf(iname, sizeof iname, "k_inv_y2<%s, %d, %d>", R, y2_radix_a(s.P2), y2_radix_b(s.P2));
+        else if (s.inv.tp) snprintf(iname, sizeof iname, "k_inv_y2<%s, %d, %d%s>", R, y2_radix_a(s.P2), y2_radix_b(s.P2),
+                                    s.inv.tp == 3 ? ", 8 lines" : "");
         else if (s.inv.all) snprintf(iname, sizeof iname, "k_inv_y_all<%s>", R);
         else snprintf(iname, sizeof iname, "k_inv_y<%s, %d>", R, s.inv.wfft);
         if (s.fwd.tp) snprintf(fname, sizeof fname, "k_fwd_y2<%s, %d, %d%s>", R, y2_radix_a(s.P2), y2_radix_b(s.P2),

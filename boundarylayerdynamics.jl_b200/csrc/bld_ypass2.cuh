@@ -65,11 +65,11 @@ __device__ __forceinline__ double2 y2_term(const double2* __restrict__ Sf, const
 }
 
 // pass 1 of the inverse transform for term kind OP: gather, radix-A DFT, store X1
-template <typename R, int A, int B, int OP>
+template <typename R, int A, int B, int OP, int NL = BLD_Y2_NL>
 __device__ __forceinline__ void inv_y2_pass1(const InvYArgs& a, const double2* __restrict__ S, int f, int z, int k1,
                                              bool ok, int j, int l, cplx<R>* buf) {
     using C = cplx<R>;
-    constexpr int P = A * B, NL = BLD_Y2_NL;
+    constexpr int P = A * B;
     const Geo& g = a.g;
     const int F = g.F, n3 = g.n3, k2max = g.k2max, shift = P - g.K2;
     const double2* Su = S + (long long)z * F;
@@ -96,11 +96,11 @@ __device__ __forceinline__ void inv_y2_pass1(const InvYArgs& a, const double2* _
 }
 
 // grid (nterms * members, ceil(K1 / NL), n3), block B * NL threads;
-// smem tw[P] + P * NL complex
-template <typename R, int A, int B, int MINB>
-__global__ void __launch_bounds__(B * BLD_Y2_NL, MINB) k_inv_y2(InvYArgs a) {
+// smem tw[P] + P * NL complex; NL = 16 lines per block, or 8 with more blocks per SM
+template <typename R, int A, int B, int MINB, int NL = BLD_Y2_NL>
+__global__ void __launch_bounds__(B * NL, MINB) k_inv_y2(InvYArgs a) {
     using C = cplx<R>;
-    constexpr int P = A * B, NL = BLD_Y2_NL;
+    constexpr int P = A * B;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + P;
@@ -118,12 +118,12 @@ __global__ void __launch_bounds__(B * BLD_Y2_NL, MINB) k_inv_y2(InvYArgs a) {
     for (int i = threadIdx.x; i < P; i += blockDim.x) tw[i] = twg[i];
     const double2* S = a.state + (long long)m * a.g.mstride;
     switch (op) {
-        case T_DIRECT: inv_y2_pass1<R, A, B, T_DIRECT>(a, S, f, z, k1, ok, j, l, buf); break;
-        case T_D1: inv_y2_pass1<R, A, B, T_D1>(a, S, f, z, k1, ok, j, l, buf); break;
-        case T_D2: inv_y2_pass1<R, A, B, T_D2>(a, S, f, z, k1, ok, j, l, buf); break;
-        case T_VORT1: inv_y2_pass1<R, A, B, T_VORT1>(a, S, f, z, k1, ok, j, l, buf); break;
-        case T_VORT2: inv_y2_pass1<R, A, B, T_VORT2>(a, S, f, z, k1, ok, j, l, buf); break;
-        default: inv_y2_pass1<R, A, B, T_VORT3>(a, S, f, z, k1, ok, j, l, buf); break;
+        case T_DIRECT: inv_y2_pass1<R, A, B, T_DIRECT, NL>(a, S, f, z, k1, ok, j, l, buf); break;
+        case T_D1: inv_y2_pass1<R, A, B, T_D1, NL>(a, S, f, z, k1, ok, j, l, buf); break;
+        case T_D2: inv_y2_pass1<R, A, B, T_D2, NL>(a, S, f, z, k1, ok, j, l, buf); break;
+        case T_VORT1: inv_y2_pass1<R, A, B, T_VORT1, NL>(a, S, f, z, k1, ok, j, l, buf); break;
+        case T_VORT2: inv_y2_pass1<R, A, B, T_VORT2, NL>(a, S, f, z, k1, ok, j, l, buf); break;
+        default: inv_y2_pass1<R, A, B, T_VORT3, NL>(a, S, f, z, k1, ok, j, l, buf); break;
     }
     __syncthreads();
     if (j >= A) return;
