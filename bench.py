@@ -607,6 +607,21 @@ def run_profile(args):
     import torch
     import BoundaryLayerDynamics as BLD
     from BoundaryLayerDynamics import workloads
+    if args.config == "ensemble":
+        # the 64-member uneven LES ensemble (mixed form), one parent-graph step per step
+        from BoundaryLayerDynamics.ensemble import Ensemble
+        groups = workloads.ensemble_members()
+        ens = Ensemble.from_groups(groups, precision="mixed")
+        ens.initialize(groups, seed=100)
+        ens.prepare()
+        ens.step(max(3, args.warmup), 1e-4)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        ens.step(args.profile_steps, 1e-4)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        return {"profile": "ensemble", "precision": "mixed", "steps": args.profile_steps,
+                "kernels": [m.kernels() for m in ens.models]}
     spec = workloads.CONFIGS[args.config]
     m = workloads.build(spec, BLD, precision=args.precision)
     u0, v0, w0 = workloads.initial_fields(spec)
