@@ -193,6 +193,7 @@ struct bld_handle {
     bool mask_on = false;        // the active mask applies to whole-ensemble steps only
     int proj_variant = 1;        // 0: column kernel, 1/2: z-segmented kernel, 3: with a shared tile (autotuned)
     int proj_tile = 0;           // LN > 0: projections of stored stage values by k_project_tile<.., LN> (autotuned)
+    int proj_pipe = 0;           // 1: ... by its persistent two-stage form k_project_pipe<.., LN> (autotuned)
     double* prof_acc = nullptr;  // [members][3][n3+1] time integral of the mean profiles
     double* prof_prev = nullptr; // [members][3][n3+1] last sample
     bool prof_on = false;        // step graphs sample the profiles after every step
@@ -471,6 +472,43 @@ int state_tmap(const bld_handle* h, const void* base, int nl, CUtensorMap* out) 
 bool project_tile_ok(const bld_handle* h, int ln) {
     return h->cfg.pressure && h->g.n3 <= 256 && h->g.F % 2 == 0 && (ln == 4 || ln == 8 || ln == 16) &&
            project_tile_smem(h->g.n3, ln) <= 200 * 1024 && encode_tiled() != nullptr;
+}
+
+// k_project_pipe applies where k_project_tile does and two stages fit in 200 KB
+bool project_pipe_ok(const bld_handle* h, int ln) {
+    return project_tile_ok(h, ln) && project_pipe_smem(h->g.n3, ln) <= 200 * 1024;
+}
+
+// launches k_project_pipe<LMAX, LN>: as many blocks as are resident at once on
+// the device (at most one per item)
+template <int LMAX, int LN>
+int launch_project_pipe(bld_handle* h, const ProjArgs& a, int nm, const CUtensorMap& umap, const CUtensorMap& gmap) {
+    const int n3 = h->g.n3;
+    dim3 block(LN, std::max(1, std::min(16, (n3 + LMAX - 1) / LMAX)));
+    const size_t sm = project_pipe_smem(n3, LN);
+    // resident blocks per SM at this block shape and shared memory, found once
+    // per (kernel, n3) (the autotuner's first launch, outside any capture)
+    static std::mutex mu;
+    static std::map<int, int> per_sm_of_n3;
+    int dev = 0, nsm = 0, per_sm = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = per_sm_of_n3.find(n3);
+        if (it != per_sm_of_n3.end()) {
+            per_sm = it->second;
+        } else {
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_project_pipe<LMAX, LN>,
+                                                                   (int)(block.x * block.y), sm));
+            per_sm_of_n3[n3] = per_sm;
+        }
+    }
+    const long long items = (h->g.F + LN - 1) / LN * (long long)nm;
+    const int blocks = (int)std::min<long long>(items, (long long)std::max(1, per_sm) * nsm);
+    k_project_pipe<LMAX, LN><<<blocks, block, sm, h->stream>>>(a, nm, umap, gmap, h->flag);
+    CUDA_TRY(cudaGetLastError());
+    return BLD_OK;
 }
 
 // tensor maps of k_project_tile: the members' states from `u` as float64
@@ -1167,6 +1205,13 @@ int set_smem_limits() {
     CUDA_TRY(cudaFuncSetAttribute(k_project_tile<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CUDA_TRY(cudaFuncSetAttribute(k_project_tile<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CUDA_TRY(cudaFuncSetAttribute(k_project_tile<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    // k_project_pipe: at most 200 KB as well (project_pipe_ok)
+    CUDA_TRY(cudaFuncSetAttribute(k_project_pipe<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_pipe<8, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_pipe<8, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_pipe<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_pipe<16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_project_pipe<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CUDA_TRY(cudaFuncSetAttribute(k_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     done = 1;
     return BLD_OK;
@@ -1504,7 +1549,7 @@ struct TuneKey {
 };
 struct TuneVal {
     Space adv, sgs;
-    int proj_variant, proj_tile;
+    int proj_variant, proj_tile, proj_pipe;
 };
 std::mutex g_tune_mutex;
 std::map<TuneKey, TuneVal> g_tune_cache;
@@ -1513,7 +1558,7 @@ TuneKey tune_key(const bld_handle* h) {
     // any kernel-family switch in the environment makes its own entry
     int env = 0;
     for (const char* v : {"BLD_X_KERNEL", "BLD_Y_KERNEL", "BLD_XW_MINB", "BLD_PROJ_VARIANT", "BLD_X_LINES",
-                          "BLD_SGS_X_KERNEL", "BLD_X2_VARIANT", "BLD_PROJ_TILE", "BLD_SGS_X2_VARIANT"}) {
+                          "BLD_SGS_X_KERNEL", "BLD_X2_VARIANT", "BLD_PROJ_TILE", "BLD_PROJ_PIPE", "BLD_SGS_X2_VARIANT"}) {
         const char* e = getenv(v);
         env = env * 31 + (e ? (int)(std::hash<std::string>{}(e) % 1000003) + 1 : 0);
     }
@@ -1553,6 +1598,7 @@ int autotune(bld_handle* h) {
             if (h->sgs.on) x_chunks(h, h->sgs);
             h->proj_variant = it->second.proj_variant;
             h->proj_tile = it->second.proj_tile;
+            h->proj_pipe = it->second.proj_pipe;
             return BLD_OK;
         }
     }
@@ -1564,6 +1610,7 @@ int autotune(bld_handle* h) {
         copy_tuning(v.sgs, h->sgs);
         v.proj_variant = h->proj_variant;
         v.proj_tile = h->proj_tile;
+        v.proj_pipe = h->proj_pipe;
         g_tune_cache[key] = v;
     }
     return BLD_OK;
@@ -1813,28 +1860,38 @@ int autotune_impl(bld_handle* h) {
         h->proj_variant = bv;
         // projections of stored stage values (the step's in-place projections):
         // the chosen kernel against k_project_tile with 8 or 16 columns per block
-        // (BLD_PROJ_TILE = 0, 4, 8, 16 keeps one)
+        // (BLD_PROJ_TILE = 0, 4, 8, 16 keeps one), each also in its persistent
+        // two-stage form (BLD_PROJ_PIPE = 0 or 1 keeps one form)
         const char* pt = getenv("BLD_PROJ_TILE");
         const int only_t = (pt && pt[0]) ? atoi(pt) : -1;
+        const char* pp = getenv("BLD_PROJ_PIPE");
+        const int only_p = (pp && pp[0]) ? atoi(pp) : -1;
         float bt = 1e30f;
-        int btile = 0;
-        for (int ln : {0, 4, 8, 16}) {
-            if (ln && !project_tile_ok(h, ln)) continue;
-            if (only_t >= 0 && ln != only_t) continue;
-            h->proj_tile = ln;
-            BLD_TRY(time_launches(h, [&] {
-                for (int k = 0; k < 3; ++k)
-                    BLD_TRY(enqueue_project(h, S_NONE, 1e-4, h->io, nullptr, nullptr, nullptr, h->io, 0, B));
-                return (int)BLD_OK;
-            }, 3, &t));
-            if (t < bt) {
-                bt = t;
-                btile = ln;
+        int btile = 0, bpipe = 0;
+        for (int ln : {0, 4, 8, 16})
+            for (int pipe = 0; pipe < 2; ++pipe) {
+                if (ln && !project_tile_ok(h, ln)) continue;
+                if (pipe && (!ln || !project_pipe_ok(h, ln))) continue;
+                if (only_t >= 0 && ln != only_t) continue;
+                // a forced persistent form that does not fit keeps the plain one
+                if (ln && only_p >= 0 && pipe != only_p && !(only_p == 1 && !project_pipe_ok(h, ln))) continue;
+                h->proj_tile = ln;
+                h->proj_pipe = pipe;
+                BLD_TRY(time_launches(h, [&] {
+                    for (int k = 0; k < 3; ++k)
+                        BLD_TRY(enqueue_project(h, S_NONE, 1e-4, h->io, nullptr, nullptr, nullptr, h->io, 0, B));
+                    return (int)BLD_OK;
+                }, 3, &t));
+                if (t < bt) {
+                    bt = t;
+                    btile = ln;
+                    bpipe = pipe;
+                }
             }
-        }
         h->proj_tile = btile;
+        h->proj_pipe = bpipe;
         const char* v = getenv("BLD_VERBOSE");
-        if (v && v[0] && v[0] != '0') fprintf(stderr, "bld autotune projection: variant %d, tile %d\n", bv, btile);
+        if (v && v[0] && v[0] != '0') fprintf(stderr, "bld autotune projection: variant %d, tile %d, persistent %d\n", bv, btile, bpipe);
     }
     CUDA_TRY(cudaMemsetAsync(h->flag, 0, h->B * sizeof(int), h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1921,6 +1978,14 @@ int enqueue_project(bld_handle* h, int kind, double dt, const double2* u, const 
         BLD_TRY(project_tmaps(h, u, ln, &umap, &gmap));
         dim3 grid((unsigned)((h->g.F + ln - 1) / ln), nm);
         dim3 block(ln, std::max(1, std::min(16, (n3 + lmax - 1) / lmax)));
+        if (h->proj_pipe && project_pipe_ok(h, ln)) {
+            if (lmax == 8 && ln == 4) return launch_project_pipe<8, 4>(h, a, nm, umap, gmap);
+            if (lmax == 8 && ln == 8) return launch_project_pipe<8, 8>(h, a, nm, umap, gmap);
+            if (lmax == 8) return launch_project_pipe<8, 16>(h, a, nm, umap, gmap);
+            if (ln == 4) return launch_project_pipe<16, 4>(h, a, nm, umap, gmap);
+            if (ln == 8) return launch_project_pipe<16, 8>(h, a, nm, umap, gmap);
+            return launch_project_pipe<16, 16>(h, a, nm, umap, gmap);
+        }
         const size_t sm = project_tile_smem(n3, ln);
         if (lmax == 8 && ln == 4) k_project_tile<8, 4><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
         else if (lmax == 8 && ln == 8) k_project_tile<8, 8><<<grid, block, sm, h->stream>>>(a, umap, gmap, h->flag);
@@ -2967,8 +3032,8 @@ int32_t bld_describe(bld_handle* h, char* buf, size_t len) {
         snprintf(tmp, sizeof tmp, "%s\"projection\": \"k_project\"", out.size() > 1 ? ", " : "");
     out += tmp;
     if (h->proj_tile)
-        snprintf(tmp, sizeof tmp, ", \"projection_stored\": \"k_project_tile<%d, %d>\"}", h->g.n3 <= 128 ? 8 : 16,
-                 h->proj_tile);
+        snprintf(tmp, sizeof tmp, ", \"projection_stored\": \"%s<%d, %d>\"}",
+                 h->proj_pipe ? "k_project_pipe" : "k_project_tile", h->g.n3 <= 128 ? 8 : 16, h->proj_tile);
     else
         snprintf(tmp, sizeof tmp, "}");
     out += tmp;

@@ -14,6 +14,11 @@
 // dynamic shared memory project_tile_smem(n3, LN).  A tensor copy's shared-memory
 // destination starts on a 128-byte boundary: the component tiles are padded to
 // project_tile_stride values.
+//
+// k_project_pipe runs the same solve as a persistent kernel: each block walks the
+// (member, LN-column tile) items i = blockIdx.x + k gridDim.x with two stages of
+// shared memory, and the copies of item k + 1 are in flight while item k is
+// solved and written, so a block's loads never wait behind its own arithmetic.
 #pragma once
 
 #include "bld_tma.cuh"
@@ -26,49 +31,41 @@ __host__ __device__ constexpr int project_tile_smem(int n3, int LN) {
     return 128 + 128 + 3 * project_tile_stride(n3, LN) * 16 + n3 * LN * 8;
 }
 
+// bytes of one stage of k_project_pipe (the three component tiles and gamma),
+// rounded to 128; dynamic shared memory of k_project_pipe: slack, the two
+// barriers, two stages
+__host__ __device__ constexpr int project_stage_bytes(int n3, int LN) {
+    return (3 * project_tile_stride(n3, LN) * 16 + n3 * LN * 8 + 127) / 128 * 128;
+}
+__host__ __device__ constexpr int project_pipe_smem(int n3, int LN) {
+    return 128 + 128 + 2 * project_stage_bytes(n3, LN);
+}
+
+// Issues the TMA copies of the LN columns from c0 of member m into one stage
+// (`tile` [3][FS], then gamma [n3][LN]), completing on `bar`.  The components
+// sit at rows 0, n3, 2 n3 of the member's (3 n3 - 1)-row state; the last row of
+// the third box lies past the state and is filled with zeros, as are columns
+// past F.
+template <int LN>
+__device__ __forceinline__ void project_tile_issue(const CUtensorMap* umap, const CUtensorMap* gmap, double2* tile,
+                                                   int FS, int n, int c0, int m, uint64_t* bar) {
+    mbar_arrive_expect_tx(bar, (unsigned)(3 * n * LN * 16 + n * LN * 8));
+    for (int f = 0; f < 3; ++f) tma_load_3d(tile + (size_t)f * FS, umap, 2 * c0, f * n, m, bar);
+    tma_load_2d(reinterpret_cast<double*>(tile + 3 * FS), gmap, c0, 0, bar);
+}
+
+// The solve of one staged tile (columns c0 .. c0 + LN - 1 of member m), writing
+// u + grad p to a.out; every thread of the block calls it, and it ends after a
+// barrier that follows the block's last read of the tile.
 template <int LMAX, int LN>
-__global__ void __launch_bounds__(LN * 32) k_project_tile(ProjArgs a, const __grid_constant__ CUtensorMap umap,
-                                                        const __grid_constant__ CUtensorMap gmap, int* flag) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double2 sP[32][LN];
-    __shared__ double sQ[32][LN];
-    // the TMA destinations start on 128-byte boundaries
-    unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(base);
+__device__ __forceinline__ void project_tile_solve(const ProjArgs& a, const double2* tile, int FS, int c0, int m,
+                                                   double2 (*sP)[LN], double (*sQ)[LN]) {
     const Geo& g = a.g;
     const int n = g.n3;
     const long long F = g.F;
-    const int FS = project_tile_stride(n, LN);
-    double2* tile = reinterpret_cast<double2*>(base + 128);   // [3][FS >= n LN]
     const double* gt = reinterpret_cast<const double*>(tile + 3 * FS);   // [n][LN]
     const int NS = blockDim.y, s = threadIdx.y, lane = threadIdx.x;
-    const int tid = s * LN + lane;
-    const int c0 = blockIdx.x * LN, c = c0 + lane;
-    const int m = a.m0 + blockIdx.y;
-    BLD_SKIP_INACTIVE(a, m);
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        fence_async_shared();
-    }
-    __syncthreads();
-    if (tid == 0) {
-        prefetch_tmap(&umap);
-        prefetch_tmap(&gmap);
-        mbar_arrive_expect_tx(bar, (unsigned)(3 * n * LN * 16 + n * LN * 8));
-        // components at rows 0, n3, 2 n3 of the member's (3 n3 - 1)-row state; the
-        // last row of the third box lies past the state and is filled with zeros
-        for (int f = 0; f < 3; ++f) tma_load_3d(tile + (size_t)f * FS, &umap, 2 * c0, f * n, m, bar);
-        tma_load_2d(const_cast<double*>(gt), &gmap, c0, 0, bar);
-    }
-    const long long wait_limit = g_bld_wait_limit;
-    const bool arrived = mbar_wait_bounded(bar, 0, wait_limit);
-    if (__syncthreads_or(!arrived)) {
-        if (tid == 0) {
-            atomicOr(flag + m, BLD_FLAG_TIMEOUT);
-            mbar_wait_bounded(bar, 0);
-        }
-        return;
-    }
+    const int c = c0 + lane;
     const bool valid = c < F;
     const int L = (n + NS - 1) / NS;
     const int z0 = min(n, s * L), z1 = min(n, z0 + L);
@@ -224,5 +221,105 @@ __global__ void __launch_bounds__(LN * 32) k_project_tile(ProjArgs a, const __gr
             const double add = a.mean_val[3 * m + f] - sum;
             for (int z = 0; z < n; ++z) a.out[of + z * F].x += add;
         }
+    }
+}
+
+template <int LMAX, int LN>
+__global__ void __launch_bounds__(LN * 32) k_project_tile(ProjArgs a, const __grid_constant__ CUtensorMap umap,
+                                                        const __grid_constant__ CUtensorMap gmap, int* flag) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double2 sP[32][LN];
+    __shared__ double sQ[32][LN];
+    // the TMA destinations start on 128-byte boundaries
+    unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base);
+    const int n = a.g.n3;
+    const int FS = project_tile_stride(n, LN);
+    double2* tile = reinterpret_cast<double2*>(base + 128);   // [3][FS >= n LN], then gamma
+    const int tid = threadIdx.y * LN + threadIdx.x;
+    const int c0 = blockIdx.x * LN;
+    const int m = a.m0 + blockIdx.y;
+    BLD_SKIP_INACTIVE(a, m);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_async_shared();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        prefetch_tmap(&umap);
+        prefetch_tmap(&gmap);
+        project_tile_issue<LN>(&umap, &gmap, tile, FS, n, c0, m, bar);
+    }
+    const long long wait_limit = g_bld_wait_limit;
+    const bool arrived = mbar_wait_bounded(bar, 0, wait_limit);
+    if (__syncthreads_or(!arrived)) {
+        if (tid == 0) {
+            atomicOr(flag + m, BLD_FLAG_TIMEOUT);
+            mbar_wait_bounded(bar, 0);
+        }
+        return;
+    }
+    project_tile_solve<LMAX, LN>(a, tile, FS, c0, m, sP, sQ);
+}
+
+// persistent form: grid (blocks, 1), block (LN, NS), dynamic shared memory
+// project_pipe_smem(n3, LN); the items are the ceil(F / LN) tiles of each of the
+// nm members from a.m0 (inactive members skipped)
+template <int LMAX, int LN>
+__global__ void __launch_bounds__(LN * 32) k_project_pipe(ProjArgs a, int nm, const __grid_constant__ CUtensorMap umap,
+                                                        const __grid_constant__ CUtensorMap gmap, int* flag) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double2 sP[32][LN];
+    __shared__ double sQ[32][LN];
+    unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base);   // [2]
+    const int n = a.g.n3;
+    const int FS = project_tile_stride(n, LN);
+    const int SB = project_stage_bytes(n, LN);
+    const int tid = threadIdx.y * LN + threadIdx.x;
+    const int ntiles = (int)((a.g.F + LN - 1) / LN);
+    const int total = ntiles * nm;
+    const int step = (int)gridDim.x;
+    // this block's first active item
+    int it = blockIdx.x;
+    while (it < total && a.active && !a.active[a.m0 + it / ntiles]) it += step;
+    if (it >= total) return;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_async_shared();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        prefetch_tmap(&umap);
+        prefetch_tmap(&gmap);
+        project_tile_issue<LN>(&umap, &gmap, reinterpret_cast<double2*>(base + 128), FS, n, (it % ntiles) * LN,
+                               a.m0 + it / ntiles, &bar[0]);
+    }
+    const long long wait_limit = g_bld_wait_limit;
+    for (int k = 0; it < total; ++k) {
+        const int s = k & 1;
+        int nx = it + step;
+        while (nx < total && a.active && !a.active[a.m0 + nx / ntiles]) nx += step;
+        // stage s ^ 1 was last read by item k - 1, whose solve ended in a barrier
+        if (tid == 0 && nx < total) {
+            fence_async_shared();
+            project_tile_issue<LN>(&umap, &gmap, reinterpret_cast<double2*>(base + 128 + (s ^ 1) * SB), FS, n,
+                                   (nx % ntiles) * LN, a.m0 + nx / ntiles, &bar[s ^ 1]);
+        }
+        const int m = a.m0 + it / ntiles, c0 = (it % ntiles) * LN;
+        const bool arrived = mbar_wait_bounded(&bar[s], (k >> 1) & 1, wait_limit);
+        // a block whose wait expired stops here (uniformly), after the copies it
+        // issued have landed
+        if (__syncthreads_or(!arrived)) {
+            if (tid == 0) {
+                atomicOr(flag + m, BLD_FLAG_TIMEOUT);
+                mbar_wait_bounded(&bar[s], (k >> 1) & 1);
+                if (nx < total) mbar_wait_bounded(&bar[s ^ 1], ((k + 1) >> 1) & 1);
+            }
+            return;
+        }
+        project_tile_solve<LMAX, LN>(a, reinterpret_cast<const double2*>(base + 128 + s * SB), FS, c0, m, sP, sQ);
+        it = nx;
     }
 }

@@ -183,8 +183,8 @@ int32_t bld_stream_idle(bld_handle* h, int32_t* idle);
    default.  cycles = 0 is a diagnostic setting: every such wait gives up at once,
    the kernels take their timeout exit (after their copies have landed) and the
    next call that checks the flags returns BLD_ERR_TIMEOUT.  Affects only the
-   TMA-staged kernels (k_adv_x2, k_inv_y3, k_project_tile, k_sgs_x2 and the
-   staged k_sgs_x); the setting is device-wide. */
+   TMA-staged kernels (k_adv_x2, k_inv_y3, k_project_tile, k_project_pipe,
+   k_sgs_x2 and the staged k_sgs_x); the setting is device-wide. */
 int32_t bld_set_wait_limit(int32_t device, int64_t cycles);
 
 /* Average device time of each launch kind of one right-hand side, measured with

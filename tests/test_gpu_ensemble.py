@@ -69,11 +69,20 @@ def test_member_params_after_creation(BLD):
         _close(a.get_state(m), b.get_state(m), 0.0)
 
 
-def test_active_mask_and_prepare_member(BLD):
-    """Inactive members keep their state; active ones equal a model of their own."""
+@pytest.mark.parametrize("proj", ["auto", "pipe", "tile"])
+def test_active_mask_and_prepare_member(BLD, proj, monkeypatch):
+    """Inactive members keep their state; active ones equal a model of their own.
+    `pipe` and `tile` force the projections of stored stage values onto the
+    persistent k_project_pipe (whose blocks walk the items of active members
+    only) or onto k_project_tile, 8 columns per block."""
     from BoundaryLayerDynamics import workloads
+    if proj != "auto":
+        monkeypatch.setenv("BLD_PROJ_TILE", "8")
+        monkeypatch.setenv("BLD_PROJ_PIPE", "1" if proj == "pipe" else "0")
     spec = _spec()
     ens = workloads.build(spec, BLD, members=3)
+    if proj != "auto":
+        assert ens.kernels()["projection_stored"].startswith("k_project_" + proj), ens.kernels()
     for m in range(3):
         _load(ens, _ic(spec, 20 + m), member=m)
     ens.prepare()

@@ -414,17 +414,29 @@ def test_twopass_x_variants_fp64(oracle, BLD, res, variant, name):
         assert e < 1e-12, (res, variant, f, e)
 
 
+def _project_pipe_smem(n3, ln):
+    """Dynamic shared memory of k_project_pipe: slack and barriers, two stages of
+    three component tiles (n3 ln values rounded up to 8) and gamma."""
+    stride = (n3 * ln + 7) // 8 * 8
+    stage = (3 * stride * 16 + n3 * ln * 8 + 127) // 128 * 128
+    return 256 + 2 * stage
+
+
+@pytest.mark.parametrize("pipe", ["0", "1"])
 @pytest.mark.parametrize("tile", ["4", "8", "16"])
 @pytest.mark.parametrize("res,flux", [((16, 12, 7), False), ((24, 20, 40), True), ((16, 16, 200), False),
                                       ((64, 64, 96), True), ((17, 12, 9), False)])
-def test_projection_tile(oracle, BLD, tile, res, flux):
+def test_projection_tile(oracle, BLD, tile, pipe, res, flux):
     """k_project_tile (each block's columns brought into shared memory by TMA
-    tensor copies, 4, 8 or 16 columns per block) forced for the projections of
-    stored stage values: apply_projections and 10 chained SSP-RK33 steps against
-    the oracle, with and without ConstantMean.  An odd number of modes per layer
-    (17 x 12: F = 9 x 11) keeps the z-segmented kernel."""
-    saved = os.environ.get("BLD_PROJ_TILE")
+    tensor copies, 4, 8 or 16 columns per block), and its persistent two-stage
+    form k_project_pipe where two stages fit in 200 KB, forced for the
+    projections of stored stage values: apply_projections and 10 chained
+    SSP-RK33 steps against the oracle, with and without ConstantMean.  An odd
+    number of modes per layer (17 x 12: F = 9 x 11) keeps the z-segmented
+    kernel."""
+    saved = {k: os.environ.get(k) for k in ("BLD_PROJ_TILE", "BLD_PROJ_PIPE")}
     os.environ["BLD_PROJ_TILE"] = tile
+    os.environ["BLD_PROJ_PIPE"] = pipe
 
     def build(api):
         dom = api.Domain((4 * math.pi, 2 * math.pi, 2.0), api.SmoothWall(), api.SmoothWall())
@@ -434,15 +446,18 @@ def test_projection_tile(oracle, BLD, tile, res, flux):
     try:
         gm = build(BLD)
     finally:
-        if saved is None:
-            del os.environ["BLD_PROJ_TILE"]
-        else:
-            os.environ["BLD_PROJ_TILE"] = saved
+        for k, v in saved.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
     om = build(oracle)
     F = om.state["vel1"].shape[1] * om.state["vel1"].shape[2]
     stored = gm.kernels().get("projection_stored", "")
     if F % 2 == 0:
-        assert stored == "k_project_tile<%d, %s>" % (8 if res[2] <= 128 else 16, tile), gm.kernels()
+        persistent = pipe == "1" and _project_pipe_smem(res[2], int(tile)) <= 200 * 1024
+        name = "k_project_pipe" if persistent else "k_project_tile"
+        assert stored == "%s<%d, %s>" % (name, 8 if res[2] <= 128 else 16, tile), gm.kernels()
     else:
         assert stored == "", gm.kernels()
     rng = np.random.default_rng(int(tile) + sum(res))
@@ -588,24 +603,26 @@ def _with_env(env, fn):
                 os.environ[k] = v
 
 
-@pytest.mark.parametrize("kind", ["projection_tile", "sgs_rows", "sgs_staged"])
+@pytest.mark.parametrize("kind", ["projection_tile", "projection_pipe", "sgs_rows", "sgs_staged"])
 def test_bounded_wait_timeout_exit_other_kernels(oracle, BLD, kind):
     """The timeout exit of the other kernels that wait for their own TMA copies
-    (the tile projection, the SGS x kernel with staged row groups, the two-pass
+    (the tile projection and its persistent form, the SGS x kernel with staged row groups, the two-pass
     SGS x kernel with staged rows), each forced, with the device's wait limit at
     0: the call reports BLD_ERR_TIMEOUT; with the limit restored the same handle
     gives the oracle's result again."""
     from BoundaryLayerDynamics import _capi
-    if kind == "projection_tile":
-        res, les, env = (64, 64, 6), False, {"BLD_PROJ_TILE": "8"}
+    if kind.startswith("projection"):
+        res, les = (64, 64, 6), False
+        env = {"BLD_PROJ_TILE": "8", "BLD_PROJ_PIPE": "1" if kind == "projection_pipe" else "0"}
     elif kind == "sgs_rows":
         res, les, env = (64, 12, 6), True, {"BLD_SGS_X_KERNEL": "rows"}
     else:
         res, les, env = (64, 12, 6), True, {"BLD_SGS_X_KERNEL": "twopass_staged"}
     gm = _with_env(env, lambda: _build(BLD, res, "fp64", les=les))
     om = _build(oracle, res, les=les)
-    if kind == "projection_tile":
-        assert gm.kernels()["projection_stored"].startswith("k_project_tile<"), gm.kernels()
+    if kind.startswith("projection"):
+        name = "k_project_pipe<" if kind == "projection_pipe" else "k_project_tile<"
+        assert gm.kernels()["projection_stored"].startswith(name), gm.kernels()
         rng = np.random.default_rng(5)
         st = {f: rng.standard_normal(om.state[f].shape) + 1j * rng.standard_normal(om.state[f].shape)
               for f in om.fields}
